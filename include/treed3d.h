@@ -1,0 +1,161 @@
+/*
+ * treed3d.h -- C ABI of libtreed3d.so, the sm_100a field solver of charges in a plane
+ * (B200-native implementation of tree-d-3d's FlatQuadtree, Barnes-Hut walk, FMM and
+ * direct sums).
+ *
+ * Conventions (those of the reference's kernel boundary, src/tree_d_3d/kernels/
+ * __init__.py:99-114, where every kernel takes contiguous float64 / int64 arrays and
+ * writes caller-allocated outputs in place):
+ *   - every pointer is a DEVICE pointer to caller-owned memory, unless marked "host";
+ *   - points are component-major (2, n) float64 arrays (x row, then y row);
+ *   - node arrays are node-major: center (nodes, 2), moments (nodes, order + 1);
+ *   - indices are int64;
+ *   - `stream` is a cudaStream_t (0: the legacy default stream); work is enqueued on it;
+ *   - `status` is an int64 device word the caller zeroes: a kernel that meets an
+ *     unsoftened coincident charged pair writes 1 + an index there (the first thread
+ *     to report wins, as tree_d_3d_report, src/tree_d_3d/kernels/barnes_hut.cuh:15-20);
+ *   - scratch memory is a caller-provided `workspace` of at least the size returned
+ *     by the matching *_workspace_size query; the library allocates nothing;
+ *   - return value: TD3_OK, or an error code below (launch errors are TD3_ECUDA with
+ *     the CUDA error kept for td3_last_error).
+ * Entry points are re-entrant and keep no state between calls.
+ */
+#ifndef TREED3D_H
+#define TREED3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TD3_OK 0
+#define TD3_EINVAL 1      /* an argument is out of range */
+#define TD3_ECUDA 2       /* a CUDA call failed (td3_last_error) */
+#define TD3_ENEEDMORE 3   /* an output buffer is too small; the needed size is reported */
+#define TD3_EWORKSPACE 4  /* the workspace is smaller than its size query */
+
+#define TD3_KERNEL_COULOMB 0
+#define TD3_KERNEL_LOG 1
+
+/* Highest expansion order (MAX_ORDER, src/tree_d_3d/flat_tree.py:46). */
+#define TD3_MAX_ORDER 64
+
+/* Library version (major * 10000 + minor * 100 + patch). */
+int td3_version(void);
+
+/* The last CUDA error seen by this thread, as a string ("" when none). */
+const char* td3_last_error(void);
+
+/* ------------------------------------------------------------------ direct sums */
+
+/* Exact all-pairs potential (n_targets) and field (2, n_targets) at `targets` of the
+ * sources `pos` (2, n_sources) with `charge`, without k_e.  kernel: TD3_KERNEL_COULOMB
+ * (phi = sum q / sqrt(r^2 + eps^2)) or TD3_KERNEL_LOG (phi = -sum q ln(r^2 + eps^2),
+ * E = 2 sum q d / (r^2 + eps^2)).  exclude[i] is a source index skipped for target i
+ * (-1: none); zero charges are skipped.  with_potential = 0 writes phi = 0 and, for
+ * the log kernel, skips the logarithms.
+ * Replaces the reference kernels direct_sum (src/tree_d_3d/kernels/direct_sum/
+ * direct_sum_cuda.cu:7-44) and direct_log_sum (kernels/direct_log_sum/
+ * direct_log_sum_cuda.cu:7-42), called by direct_field (src/tree_d_3d/flat_tree.py:157-158). */
+size_t td3_direct_sum_workspace_size(int64_t n_targets, int64_t n_sources);
+int td3_direct_sum(int kernel, const double* targets, int64_t n_targets, const int64_t* exclude,
+                   const double* pos, const double* charge, int64_t n_sources, double softening,
+                   int with_potential, double* phi, double* field, int64_t* status,
+                   void* workspace, size_t workspace_bytes, void* stream);
+
+/* Exact pair energy sum_{i<j} q_i q_j / sqrt(r^2 + eps^2) of the Coulomb kernel, added
+ * to energy[0] (device).  Replaces pair_energy (src/tree_d_3d/kernels/pair_energy/
+ * pair_energy_cuda.cu:11-38), used by ElectrostaticSimulation.get_potential_energy
+ * (src/tree_d_3d/simulation.py:905-915). */
+size_t td3_pair_energy_workspace_size(int64_t n);
+int td3_pair_energy(const double* pos, const double* charge, int64_t n, double softening,
+                    double* energy, int64_t* status, void* workspace, size_t workspace_bytes,
+                    void* stream);
+
+/* ------------------------------------------------------------------ tree build */
+
+/* Build the quadtree of the n particles at `pos` (2, n) in the root cell (xmid, ymid,
+ * half): nodes with more than leaf_capacity particles above max_depth split into four
+ * children (upper left, upper right, lower left, lower right), numbered breadth first
+ * in the order of their parents; a particle on a dividing line goes left or up; the
+ * particles of a cell keep their input order.  Writes the node arrays (capacity rows:
+ * node_center (capacity, 2), node_half, node_start, node_end, node_child (-1 for
+ * leaves), node_depth), perm (n; the particles in tree order) and sorted_pos (2, n;
+ * pos[:, perm]).  levels (HOST, capacity + 1) receives the first node of each depth;
+ * sizes (HOST, 3) receives node count, number of levels and 1 if capacity was too
+ * small (then TD3_ENEEDMORE is returned and the tree is unfinished: retry with a
+ * larger capacity, as the reference doubles it).  Synchronises `stream` once per level.
+ * Replaces quadtree_build (src/tree_d_3d/kernels/quadtree_build/quadtree_build_pyccel.py:
+ * 12-137) and the GPU level kernels quadtree_quadrants / quadtree_scatter
+ * (kernels/quadtree_quadrants/quadtree_quadrants_cuda.cu:7-26, kernels/quadtree_scatter/
+ * quadtree_scatter_cuda.cu:8-34) driven by FlatQuadtree._build (src/tree_d_3d/flat_tree.py:
+ * 483-625); identical node arrays, perm and levels. */
+size_t td3_quadtree_build_workspace_size(int64_t n, int64_t capacity);
+int td3_quadtree_build(const double* pos, int64_t n, double xmid, double ymid, double half,
+                       int64_t leaf_capacity, int64_t max_depth, int64_t capacity,
+                       double* node_center, double* node_half, int64_t* node_start,
+                       int64_t* node_end, int64_t* node_child, int64_t* node_depth,
+                       int64_t* perm, double* sorted_pos, int64_t* levels, int64_t* sizes,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+/* ------------------------------------------------------------------ moments */
+
+/* Coulomb cell moments about each node centre: node_q, node_qabs (sum |q|), node_p
+ * (nodes, 2) and the raw second moment node_s (nodes, 3: xx, xy, yy); leaves from their
+ * particles (sorted_pos (2, n), sorted_charge in tree order), parents by M2M, deepest
+ * level first.  levels (HOST, n_levels + 1).  Replaces quadtree_moments_upward
+ * (src/tree_d_3d/kernels/quadtree_moments_upward/quadtree_moments_upward_pyccel.py:13-83)
+ * and quadtree_moments (kernels/quadtree_moments/quadtree_moments_cuda.cu:7-46), called
+ * by FlatQuadtree._moments (src/tree_d_3d/flat_tree.py:720-743). */
+int td3_quadtree_moments(const int64_t* levels, int64_t n_levels, const double* sorted_pos,
+                         const double* sorted_charge, int64_t n, const double* node_center,
+                         const int64_t* node_start, const int64_t* node_end,
+                         const int64_t* node_child, double* node_q, double* node_qabs,
+                         double* node_p, double* node_s, void* stream);
+
+/* Complex multipole moments a_n = sum q (z - c)^n, n = 0..order, of every node
+ * (moment_re / moment_im (nodes, order + 1)) and node_qabs; binomial is the
+ * (binomial_size, binomial_size) table C(n, m) of the reference (_binomial_table,
+ * src/tree_d_3d/flat_tree.py:224-231).  Replaces log_moments_upward
+ * (src/tree_d_3d/kernels/log_moments_upward/log_moments_upward_pyccel.py:14-93) and
+ * log_quadtree_moments (kernels/log_quadtree_moments/log_quadtree_moments_cuda.cu:7-46),
+ * called at src/tree_d_3d/flat_tree.py:689-713. */
+int td3_log_moments(const int64_t* levels, int64_t n_levels, int order,
+                    const double* sorted_pos, const double* sorted_charge, int64_t n,
+                    const double* node_center, const int64_t* node_start,
+                    const int64_t* node_end, const int64_t* node_child,
+                    const double* binomial, int binomial_size, double* node_qabs,
+                    double* moment_re, double* moment_im, void* stream);
+
+/* Cartesian multipole moments m_g = sum q (r - c)^g, |g| <= order, of every node
+ * (moments (nodes, n_coef)), with the index tables of the reference's _cartesian.tables
+ * (src/tree_d_3d/_cartesian.py:40-107): ex, ey (n_coef), shift (n_shift, 3) rows
+ * (g, b, g - b) sorted by g with shift_coef, and shift_start (n_coef + 1) the first
+ * row of each g.  Replaces cart_moments_upward (src/tree_d_3d/kernels/
+ * cart_moments_upward/cart_moments_upward_pyccel.py:14-82), called by
+ * FlatQuadtree._cartesian_moments (src/tree_d_3d/flat_tree.py:1063-1084). */
+int td3_cart_moments(const int64_t* levels, int64_t n_levels, const double* sorted_pos,
+                     const double* sorted_charge, int64_t n, const double* node_center,
+                     const int64_t* node_start, const int64_t* node_end,
+                     const int64_t* node_child, const int64_t* ex, const int64_t* ey,
+                     const int64_t* shift, const double* shift_coef, const int64_t* shift_start,
+                     int n_coef, double* moments, void* stream);
+
+/* ------------------------------------------------------------------ utilities */
+
+/* Stable radix sort of (key, value) uint32 pairs by the low `bits` bits of the key.
+ * The buffers ping-pong; *result_in_alt (host) tells whether the sorted pairs ended in
+ * the *_alt buffers.  No reference counterpart (the reference sorts Morton keys on
+ * the host with numpy.argsort, src/tree_d_3d/flat_tree.py:891-912). */
+size_t td3_radix_sort_workspace_size(int64_t n);
+int td3_radix_sort_pairs(uint32_t* keys, uint32_t* keys_alt, uint32_t* values,
+                         uint32_t* values_alt, int64_t n, int bits, int* result_in_alt,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TREED3D_H */

@@ -1,0 +1,161 @@
+"""The GPU tree build and moments against the reference's golden vectors.
+
+Trees are integer work plus exactly replicated floating-point centres: every node
+array, the permutation, the levels and the sorted positions must be identical.  The
+moments sum in the reference's order without FMA contraction, so they are compared
+for equality as well.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+TREE_ARRAYS = ("perm", "node_center", "node_half", "node_start", "node_end", "node_child",
+               "node_depth")
+
+
+def _np(t):
+    return t.cpu().numpy() if isinstance(t, torch.Tensor) else np.asarray(t)
+
+
+def assert_tree(tree, data, prefix):
+    assert tree.node_count == int(data[f"{prefix}/node_count"])
+    for name in TREE_ARRAYS:
+        np.testing.assert_array_equal(_np(getattr(tree, name)), data[f"{prefix}/{name}"],
+                                      err_msg=name)
+    np.testing.assert_array_equal(tree.levels, data[f"{prefix}/levels"])
+
+
+@pytest.mark.parametrize("cloud", ["uniform", "circle", "clustered", "lattice", "coincident"])
+def test_build_is_identical(cloud):
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    data = golden("build")
+    pos = data[f"{cloud}/pos"]
+    tree = FlatQuadtree(pos, np.ones(pos.shape[1]), Quad(0, 0, 1), leaf_capacity=6)
+    assert_tree(tree, data, cloud)
+    perm = _np(tree.perm)
+    assert np.array_equal(np.sort(perm), np.arange(pos.shape[1]))
+    np.testing.assert_array_equal(_np(tree._sorted_pos), pos[:, perm])
+
+
+def test_build_deep_chain_depths_and_offset_root():
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    data = golden("build")
+    tree = FlatQuadtree(data["chain/pos"], [1, 1, -1], Quad(0, 0, 1), leaf_capacity=1)
+    assert_tree(tree, data, "chain")
+    assert tree.node_count == 1 + 4 * 48 and int(tree.node_depth.max()) == 48
+    assert tree.root.count == 3
+    for leaf, depth in ((1, 10), (8, 48)):
+        key = f"cloud300_l{leaf}_d{depth}"
+        tree = FlatQuadtree(data[f"{key}/pos"], np.ones(300), Quad(0, 0, 1),
+                            leaf_capacity=leaf, max_depth=depth)
+        assert_tree(tree, data, key)
+    root = data["offroot/root"]
+    pos = data["offroot/pos"]
+    tree = FlatQuadtree(pos, np.zeros(pos.shape[1]), Quad(*root), leaf_capacity=16)
+    assert_tree(tree, data, "offroot")
+
+
+def test_too_small_node_buffer_restarts_the_build():
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    data = golden("build")
+    pos = data["clustered/pos"]
+    tree = FlatQuadtree.__new__(FlatQuadtree)
+    # the constructor with a capacity of 8 nodes: must restart and give the same tree
+    original = FlatQuadtree._build
+    FlatQuadtree._build = lambda self, capacity=None: original(self, 8)
+    try:
+        tree = FlatQuadtree(pos, np.ones(pos.shape[1]), Quad(0, 0, 1), leaf_capacity=6)
+    finally:
+        FlatQuadtree._build = original
+    assert tree.build_restarts > 0
+    assert_tree(tree, data, "clustered")
+
+
+def test_moments_are_identical():
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    data = golden("moments")
+    pos, charge = data["pos"], data["charge"]
+    tree = FlatQuadtree(pos, charge, Quad(0, 0, 1), leaf_capacity=8)
+    assert_tree(tree, data, "coulomb")
+    for name in ("node_q", "node_qabs", "node_p", "node_s"):
+        np.testing.assert_array_equal(_np(getattr(tree, name)), data[f"coulomb/{name}"],
+                                      err_msg=name)
+    tree = FlatQuadtree(pos, charge, Quad(0, 0, 1), leaf_capacity=8, kernel="log", order=12)
+    for name in ("node_qabs", "moment_re", "moment_im", "node_q", "node_p"):
+        np.testing.assert_array_equal(_np(getattr(tree, name)), data[f"log/{name}"],
+                                      err_msg=name)
+    for order in (4, 12):
+        tree = FlatQuadtree(pos, charge, Quad(0, 0, 1), leaf_capacity=8, order=order)
+        np.testing.assert_array_equal(_np(tree._cartesian_moments()), data[f"cart{order}/moments"])
+
+
+@pytest.mark.parametrize("kernel", ["log", "coulomb"])
+def test_set_charges_equals_a_new_tree(kernel):
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    rng = np.random.default_rng(8)
+    pos = rng.uniform(-1, 1, (2, 3000))
+    first, second = rng.normal(size=3000), rng.normal(size=3000)
+    tree = FlatQuadtree(pos, first, Quad(0, 0, 1), kernel=kernel, leaf_capacity=16)
+    tree.set_charges(second)
+    fresh = FlatQuadtree(pos, second, Quad(0, 0, 1), kernel=kernel, leaf_capacity=16)
+    names = ("moment_re", "moment_im") if kernel == "log" else ("node_q", "node_p", "node_s")
+    for name in names + ("node_qabs",):
+        assert torch.equal(getattr(tree, name), getattr(fresh, name)), name
+    with pytest.raises(ValueError, match="one entry per particle"):
+        tree.set_charges(second[:10])
+
+
+def test_validation_and_empty_tree():
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    with pytest.raises(ValueError, match=r"\(2, N\)"):
+        FlatQuadtree(np.zeros((3, 2)), np.zeros(3), Quad(0, 0, 1))
+    with pytest.raises(ValueError, match="outside tree bounds"):
+        FlatQuadtree([[2.0], [0.0]], [1.0], Quad(0, 0, 1))
+    with pytest.raises(ValueError, match="finite"):
+        FlatQuadtree([[np.nan], [0.0]], [1.0], Quad(0, 0, 1))
+    with pytest.raises(ValueError, match="kernel"):
+        FlatQuadtree([[0.0], [0.0]], [1.0], Quad(0, 0, 1), kernel="yukawa")
+    with pytest.raises(ValueError, match="order"):
+        FlatQuadtree([[0.0], [0.0]], [1.0], Quad(0, 0, 1), order=65)
+    with pytest.raises(ValueError, match="same length"):
+        FlatQuadtree([[0.0], [0.0]], [1.0, 2.0], Quad(0, 0, 1))
+    tree = FlatQuadtree(np.zeros((2, 0)), np.zeros(0), Quad(0, 0, 1))
+    tree.set_charges(np.zeros(0))
+    assert tree.node_count == 1
+
+
+def test_large_build_is_a_valid_tree():
+    """1M clustered points: the permutation is a permutation, every split node's
+    children tile its range, leaves respect the capacity, digits follow the centres."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    rng = np.random.default_rng(3)
+    n = 1_000_000
+    pos = rng.normal(0, 0.2, (2, n)).clip(-0.999, 0.999)
+    tree = FlatQuadtree(torch.tensor(pos, device="cuda"), torch.ones(n, device="cuda",
+                        dtype=torch.float64), Quad(0, 0, 1), leaf_capacity=8)
+    perm = tree.perm
+    assert torch.equal(torch.sort(perm).values, torch.arange(n, device="cuda"))
+    child, start, end = tree.node_child, tree.node_start, tree.node_end
+    split = child >= 0
+    first = child[split]
+    assert torch.equal(start[first], start[split])
+    assert torch.equal(end[first + 3], end[split])
+    for c in range(3):
+        assert torch.equal(end[first + c], start[first + c + 1])
+    leaves = ~split
+    assert int(((end - start)[leaves] > 8).sum()) == 0
+    assert torch.equal(tree._sorted_pos, tree.pos[:, perm])

@@ -1,0 +1,227 @@
+// Cell moments, leaves from their particles and parents by M2M, deepest level first:
+//   Coulomb  Q, sum|q|, p, S (K/quadtree_moments_upward/quadtree_moments_upward_pyccel.py:13-83)
+//   log      a_n = sum q (z - c)^n   (K/log_moments_upward/log_moments_upward_pyccel.py:14-93)
+//   Cartesian m_g = sum q (r - c)^g  (K/cart_moments_upward/cart_moments_upward_pyccel.py:14-82)
+// The particles are read in tree order (sorted positions and charges, contiguous per
+// leaf).  Each output coefficient is summed by one thread in the reference's order,
+// and this file is compiled with --fmad=false, so the moments equal the reference's
+// bit for bit.
+#include "common.cuh"
+
+namespace {
+
+constexpr int MOM_THREADS = 128;
+
+__global__ void k_coulomb_moments(i64 lo, i64 hi, const double* __restrict__ spos,
+                                  const double* __restrict__ scharge, i64 n,
+                                  const double* __restrict__ node_center,
+                                  const i64* __restrict__ node_start,
+                                  const i64* __restrict__ node_end,
+                                  const i64* __restrict__ node_child, double* node_q,
+                                  double* node_qabs, double* node_p, double* node_s) {
+    i64 node = lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= hi) return;
+    double q = 0.0, qabs = 0.0, px = 0.0, py = 0.0, sxx = 0.0, sxy = 0.0, syy = 0.0;
+    double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
+    i64 first = node_child[node];
+    if (first < 0) {
+        for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+            double c = scharge[k];
+            double dx = spos[k] - xmid;
+            double dy = spos[n + k] - ymid;
+            q += c;
+            qabs += fabs(c);
+            px += c * dx;
+            py += c * dy;
+            sxx += c * dx * dx;
+            sxy += c * dx * dy;
+            syy += c * dy * dy;
+        }
+    } else {
+        for (i64 child = first; child < first + 4; ++child) {
+            double dx = node_center[2 * child] - xmid;
+            double dy = node_center[2 * child + 1] - ymid;
+            double cq = node_q[child], cpx = node_p[2 * child], cpy = node_p[2 * child + 1];
+            q += cq;
+            qabs += node_qabs[child];
+            px += cpx + cq * dx;
+            py += cpy + cq * dy;
+            sxx += node_s[3 * child] + 2.0 * cpx * dx + cq * dx * dx;
+            sxy += node_s[3 * child + 1] + cpx * dy + cpy * dx + cq * dx * dy;
+            syy += node_s[3 * child + 2] + 2.0 * cpy * dy + cq * dy * dy;
+        }
+    }
+    node_q[node] = q;
+    node_qabs[node] = qabs;
+    node_p[2 * node] = px;
+    node_p[2 * node + 1] = py;
+    node_s[3 * node] = sxx;
+    node_s[3 * node + 1] = sxy;
+    node_s[3 * node + 2] = syy;
+}
+
+// One thread per (node, n), n = 0..order.
+__global__ void k_log_moments(i64 lo, i64 hi, int order, const double* __restrict__ spos,
+                              const double* __restrict__ scharge, i64 n_particles,
+                              const double* __restrict__ node_center,
+                              const i64* __restrict__ node_start, const i64* __restrict__ node_end,
+                              const i64* __restrict__ node_child,
+                              const double* __restrict__ binomial, int bsize, double* node_qabs,
+                              double* moment_re, double* moment_im) {
+    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    int w = order + 1;
+    i64 node = lo + t / w;
+    int n = (int)(t % w);
+    if (node >= hi) return;
+    double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
+    double acc_re = 0.0, acc_im = 0.0, qabs = 0.0;
+    i64 first = node_child[node];
+    if (first < 0) {
+        for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+            double q = scharge[k];
+            qabs += fabs(q);
+            double dx = spos[k] - xmid, dy = spos[n_particles + k] - ymid;
+            double pr = q, pi = 0.0;
+            for (int m = 0; m < n; ++m) {
+                double next_re = pr * dx - pi * dy;
+                pi = pr * dy + pi * dx;
+                pr = next_re;
+            }
+            acc_re += pr;
+            acc_im += pi;
+        }
+    } else {
+        double sh_re[TD3_MAX_ORDER + 1], sh_im[TD3_MAX_ORDER + 1];
+        for (i64 child = first; child < first + 4; ++child) {
+            qabs += node_qabs[child];
+            if (node_end[child] == node_start[child]) continue;
+            double s_re = node_center[2 * child] - xmid;
+            double s_im = node_center[2 * child + 1] - ymid;
+            sh_re[0] = 1.0;
+            sh_im[0] = 0.0;
+            for (int k = 1; k <= n; ++k) {
+                sh_re[k] = sh_re[k - 1] * s_re - sh_im[k - 1] * s_im;
+                sh_im[k] = sh_re[k - 1] * s_im + sh_im[k - 1] * s_re;
+            }
+            double c_re = 0.0, c_im = 0.0;
+            for (int m = 0; m <= n; ++m) {
+                double c = binomial[n * bsize + m];
+                double a_re = moment_re[child * w + m] * c;
+                double a_im = moment_im[child * w + m] * c;
+                c_re += a_re * sh_re[n - m] - a_im * sh_im[n - m];
+                c_im += a_re * sh_im[n - m] + a_im * sh_re[n - m];
+            }
+            acc_re += c_re;
+            acc_im += c_im;
+        }
+    }
+    moment_re[node * w + n] = acc_re;
+    moment_im[node * w + n] = acc_im;
+    if (n == 0) node_qabs[node] = qabs;
+}
+
+// One thread per (node, coefficient g).  The monomial u^(a,b) is built as the
+// reference's mono recurrence builds it: b factors of u_y, then a factors of u_x.
+__device__ __forceinline__ double monomial(double start, double ux, double uy, int a, int b) {
+    double v = start;
+    for (int t = 0; t < b; ++t) v = v * uy;
+    for (int t = 0; t < a; ++t) v = v * ux;
+    return v;
+}
+
+__global__ void k_cart_moments(i64 lo, i64 hi, int n_coef, const double* __restrict__ spos,
+                               const double* __restrict__ scharge, i64 n_particles,
+                               const double* __restrict__ node_center,
+                               const i64* __restrict__ node_start, const i64* __restrict__ node_end,
+                               const i64* __restrict__ node_child, const i64* __restrict__ ex,
+                               const i64* __restrict__ ey, const i64* __restrict__ shift,
+                               const double* __restrict__ shift_coef,
+                               const i64* __restrict__ shift_start, double* moments) {
+    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    i64 node = lo + t / n_coef;
+    int g = (int)(t % n_coef);
+    if (node >= hi) return;
+    double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
+    int ga = (int)ex[g], gb = (int)ey[g];
+    double acc = 0.0;
+    i64 first = node_child[node];
+    if (first < 0) {
+        for (i64 k = node_start[node]; k < node_end[node]; ++k)
+            acc += monomial(scharge[k], spos[k] - xmid, spos[n_particles + k] - ymid, ga, gb);
+    } else {
+        for (i64 child = first; child < first + 4; ++child) {
+            if (node_end[child] == node_start[child]) continue;
+            double ux = node_center[2 * child] - xmid, uy = node_center[2 * child + 1] - ymid;
+            const double* cm = moments + child * n_coef;
+            for (i64 r = shift_start[g]; r < shift_start[g + 1]; ++r) {
+                int b = (int)shift[3 * r + 1];
+                int d = (int)shift[3 * r + 2];
+                acc += shift_coef[r] * cm[b] * monomial(1.0, ux, uy, (int)ex[d], (int)ey[d]);
+            }
+        }
+    }
+    moments[node * n_coef + g] = acc;
+}
+
+}  // namespace
+
+extern "C" int td3_quadtree_moments(const int64_t* levels, int64_t n_levels,
+                                    const double* sorted_pos, const double* sorted_charge,
+                                    int64_t n, const double* node_center,
+                                    const int64_t* node_start, const int64_t* node_end,
+                                    const int64_t* node_child, double* node_q, double* node_qabs,
+                                    double* node_p, double* node_s, void* stream) {
+    if (n_levels < 1) return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        k_coulomb_moments<<<td3_blocks(hi - lo, MOM_THREADS), MOM_THREADS, 0, s>>>(
+            lo, hi, sorted_pos, sorted_charge, n, node_center, node_start, node_end, node_child,
+            node_q, node_qabs, node_p, node_s);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_log_moments(const int64_t* levels, int64_t n_levels, int order,
+                               const double* sorted_pos, const double* sorted_charge, int64_t n,
+                               const double* node_center, const int64_t* node_start,
+                               const int64_t* node_end, const int64_t* node_child,
+                               const double* binomial, int binomial_size, double* node_qabs,
+                               double* moment_re, double* moment_im, void* stream) {
+    if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER || binomial_size < order + 1)
+        return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        i64 threads = (hi - lo) * (order + 1);
+        k_log_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
+            lo, hi, order, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
+            node_child, binomial, binomial_size, node_qabs, moment_re, moment_im);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_cart_moments(const int64_t* levels, int64_t n_levels, const double* sorted_pos,
+                                const double* sorted_charge, int64_t n, const double* node_center,
+                                const int64_t* node_start, const int64_t* node_end,
+                                const int64_t* node_child, const int64_t* ex, const int64_t* ey,
+                                const int64_t* shift, const double* shift_coef,
+                                const int64_t* shift_start, int n_coef, double* moments,
+                                void* stream) {
+    if (n_levels < 1 || n_coef < 1) return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        i64 threads = (hi - lo) * n_coef;
+        k_cart_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
+            lo, hi, n_coef, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
+            node_child, ex, ey, shift, shift_coef, shift_start, moments);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}

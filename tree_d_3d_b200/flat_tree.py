@@ -1,0 +1,393 @@
+"""The flat quadtree and direct sums on the GPU: a drop-in for tree-d-3d's field solver.
+
+Mirrors src/tree_d_3d/flat_tree.py of the reference (``ft`` below): ``direct_field``,
+``FlatNode`` and ``FlatQuadtree`` keep its signatures, defaults, validation messages
+and semantics, with component-major (2, N) arrays.  The arrays live on the current
+CUDA device as float64 / int64 tensors and every numeric step runs in libtreed3d.so
+(hand-written sm_100a kernels behind the C ABI of include/treed3d.h).  Tensor inputs
+give CUDA tensor results; NumPy or list inputs give NumPy results.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from tree_d_3d_b200 import _lib
+from tree_d_3d_b200._utils import (
+    _check,
+    _device,
+    _finite,
+    _points,
+    device,
+    out,
+    status_word,
+    wants_numpy,
+)
+from tree_d_3d_b200.constants import K_E
+from tree_d_3d_b200.quad import Quad
+
+#: Highest expansion order (ft:46).
+MAX_ORDER = 64
+
+#: Default orders of the log kernel and of the Coulomb FMM (ft:50-51).
+LOG_ORDER = 12
+COULOMB_ORDER = 4
+
+_KERNELS = ("coulomb", "log")
+
+#: targets per group of the reference's CPU walk (ft:70); the GPU walk groups a warp
+GROUP_SIZE = 32
+
+
+def _kernel_code(kernel: str) -> int:
+    return _lib.KERNEL_LOG if kernel == "log" else _lib.KERNEL_COULOMB
+
+
+def _direct(targets, exclude, pos, charge, softening, kernel, potential=True):
+    """Device tensors in, (phi, field) device tensors out; raises on coincidence."""
+    dev = targets.device
+    m, n = targets.shape[1], pos.shape[1]
+    phi = torch.zeros(m, dtype=torch.float64, device=dev)
+    field = torch.zeros((2, m), dtype=torch.float64, device=dev)
+    if not m or not n:
+        return phi, field
+    status = status_word(dev)
+    ws = _lib.workspace(_lib.query("td3_direct_sum_workspace_size", m, n), dev)
+    _lib.call(
+        "td3_direct_sum", _kernel_code(kernel), targets.data_ptr(), m, exclude.data_ptr(),
+        pos.data_ptr(), charge.data_ptr(), n, float(softening), 1 if potential else 0,
+        phi.data_ptr(), field.data_ptr(), status.data_ptr(), ws.data_ptr(), ws.numel(),
+        _lib.stream(dev),
+    )
+    _check(status)
+    return phi, field
+
+
+def direct_field(targets, pos, charge, *, softening=0.0, exclude=None, compiled=True,
+                 kernel="coulomb"):
+    """Exact potential (M,) and field (2, M) at ``targets`` (2, M), without ``k_e``.
+
+    ``pos`` (2, N) and ``charge`` (N,) are the sources; ``exclude[i]`` is the index of a
+    source skipped for target ``i`` (-1 for none); ``kernel`` is ``"coulomb"`` or
+    ``"log"``.  ft:124-160.  ``compiled`` is accepted for compatibility (the GPU path
+    is always the compiled one).
+    """
+    if kernel not in _KERNELS:
+        raise ValueError(f"kernel must be one of {_KERNELS}")
+    as_numpy = wants_numpy(targets)
+    targets = _points(targets, "targets")
+    pos = _points(pos, "pos")
+    charge = _device(charge).reshape(-1)
+    m = targets.shape[1]
+    if exclude is None:
+        exclude = torch.full((m,), -1, dtype=torch.int64, device=targets.device)
+    exclude = _device(exclude, torch.int64).reshape(-1)
+    return out(_direct(targets, exclude, pos, charge, softening, kernel), as_numpy)
+
+
+class FlatNode:
+    """Read-only view of one node of a `FlatQuadtree` (ft:163-211)."""
+
+    def __init__(self, tree: FlatQuadtree, index: int) -> None:
+        self.tree = tree
+        self.index = index
+
+    @property
+    def quad(self) -> Quad:
+        x, y = self.tree.node_center[self.index].tolist()
+        return Quad(float(x), float(y), float(self.tree.node_half[self.index]))
+
+    @property
+    def count(self) -> int:
+        return int(self.tree.node_end[self.index] - self.tree.node_start[self.index])
+
+    @property
+    def total_charge(self) -> float:
+        return float(self.tree.node_q[self.index])
+
+    @property
+    def total_abs_charge(self) -> float:
+        return float(self.tree.node_qabs[self.index])
+
+    @property
+    def dipole(self) -> np.ndarray:
+        return self.tree.node_p[self.index].cpu().numpy().copy()
+
+    @property
+    def second_moment(self) -> np.ndarray:
+        sxx, sxy, syy = self.tree.node_s[self.index].tolist()
+        return np.array([[sxx, sxy], [sxy, syy]])
+
+    @property
+    def particles(self) -> np.ndarray:
+        """Indices of the particles inside this node."""
+        tree = self.tree
+        start, end = int(tree.node_start[self.index]), int(tree.node_end[self.index])
+        return tree.perm[start:end].cpu().numpy()
+
+    def is_external(self) -> bool:
+        return int(self.tree.node_child[self.index]) < 0
+
+    @property
+    def children(self) -> tuple:
+        first = int(self.tree.node_child[self.index])
+        if first < 0:
+            return (None, None, None, None)
+        return tuple(FlatNode(self.tree, first + k) for k in range(4))
+
+
+_NODE_ARRAYS = ("node_center", "node_half", "node_start", "node_end", "node_child", "node_depth")
+
+#: small per-device tables shared by every tree (binomials, M2L matrices, Cartesian tables)
+_TABLES: dict = {}
+
+
+def _binomial_table(size: int) -> np.ndarray:
+    """C(n, k) for 0 <= n, k < size as floats, by Pascal's rule in floating point
+    (the values of the reference's table, ft:224-231)."""
+    table = np.zeros((size, size))
+    table[:, 0] = 1.0
+    for row in range(1, size):
+        table[row, 1 : row + 1] = table[row - 1, : row] + table[row - 1, 1 : row + 1]
+    return table
+
+
+def _m2l_coefficients(order: int, symmetric: bool) -> np.ndarray:
+    """The real M2L matrix coeff[k, l] (ft:234-245): 1/l in row 0, 1/k in column 0,
+    C(k + l - 1, l) / k elsewhere, zero beyond the triangle k <= p - l if symmetric."""
+    binomial = _binomial_table(2 * order + 1)
+    coeff = np.zeros((order + 1, order + 1))
+    ls = np.arange(1, order + 1)
+    coeff[0, 1:] = 1.0 / ls
+    coeff[1:, 0] = 1.0 / ls
+    for k in range(1, order + 1):
+        for m in range(1, order + 1):
+            if k <= (order - m if symmetric else order):
+                coeff[k, m] = binomial[k + m - 1, m] / k
+    return coeff
+
+
+def _device_table(key, make, dev, dtype=torch.float64):
+    full = (key, dev)
+    if full not in _TABLES:
+        _TABLES[full] = torch.as_tensor(np.ascontiguousarray(make()), dtype=dtype, device=dev)
+    return _TABLES[full]
+
+
+class FlatQuadtree:
+    """Array quadtree for point charges in a plane or for line charges, on the GPU.
+
+    The tree and conventions of the reference (ft:437-1676): nodes holding more than
+    ``leaf_capacity`` particles split into four until ``max_depth``; ``positions``
+    (2, N) and ``charges`` (N,) are copied.  ``kernel="coulomb"`` keeps signed moments
+    through the quadrupole, ``kernel="log"`` complex multipole expansions of ``order``
+    terms.  ``comm`` (MPI sharing of the moments) is not supported: one GPU holds the
+    whole tree.  ``precision="mixed"`` selects the mixed-precision FMM.
+    """
+
+    def __init__(self, positions, charges, root_quad: Quad, *, leaf_capacity: int = 8,
+                 max_depth: int = 48, compiled: bool = True, kernel: str = "coulomb",
+                 order: int | None = None, symmetric: bool = False, comm=None,
+                 precision: str = "fp64") -> None:
+        # ft:760-800
+        if kernel not in _KERNELS:
+            raise ValueError(f"kernel must be one of {_KERNELS}")
+        if order is None:
+            order = LOG_ORDER if kernel == "log" else COULOMB_ORDER
+        if isinstance(order, bool) or int(order) != order or order < 1:
+            raise ValueError("order must be a positive integer")
+        if order > MAX_ORDER:
+            raise ValueError(f"order must be at most {MAX_ORDER}, got {order}")
+        if comm is not None:
+            raise NotImplementedError("comm: the GPU tree runs on one device (comm=None)")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.kernel = kernel
+        self.order = int(order)
+        self.comm = None
+        self.symmetric = bool(symmetric)
+        self.precision = precision
+        self._compiled = bool(compiled)
+        _finite("half_size", root_quad.half, positive=True)
+        _finite("xmid", root_quad.xmid)
+        _finite("ymid", root_quad.ymid)
+        for name, value in (("leaf_capacity", leaf_capacity), ("max_depth", max_depth)):
+            if isinstance(value, bool) or int(value) != value or value < 1:
+                raise ValueError(f"{name} must be a positive integer")
+        self._numpy = wants_numpy(positions)
+        self.pos = _points(positions, "positions").clone()
+        self.charge = _device(charges).reshape(-1).clone()
+        self.device = self.pos.device
+        n = self.pos.shape[1]
+        if self.charge.shape[0] != n:
+            raise ValueError("positions and charges must have the same length")
+        if not bool(torch.isfinite(self.pos).all()):
+            raise ValueError("Particle position must be finite")
+        lo = torch.tensor([[root_quad.xmid - root_quad.half], [root_quad.ymid - root_quad.half]],
+                          dtype=torch.float64, device=self.device)
+        hi = torch.tensor([[root_quad.xmid + root_quad.half], [root_quad.ymid + root_quad.half]],
+                          dtype=torch.float64, device=self.device)
+        if bool((self.pos < lo).any()) or bool((self.pos > hi).any()):
+            raise ValueError("Particle lies outside tree bounds")
+        self.leaf_capacity = int(leaf_capacity)
+        self.max_depth = int(max_depth)
+        self.root_quad = Quad(float(root_quad.xmid), float(root_quad.ymid), float(root_quad.half))
+        self._traversals: dict = {}
+        self._cart_moments = None
+        self._plans: dict = {}
+        if not n:
+            self._empty()
+            return
+        count = self._build()
+        self.node_count = int(count)
+        for name in _NODE_ARRAYS:
+            setattr(self, name, getattr(self, name)[:count].clone())
+        self._moments()
+
+    # ------------------------------------------------------------------ build
+    def _empty(self) -> None:
+        """ft:462-481: the lone root of an empty tree."""
+        dev, q = self.device, self.root_quad
+        f64, i64 = torch.float64, torch.int64
+        self.perm = torch.empty(0, dtype=i64, device=dev)
+        self.node_count = 1
+        self.node_center = torch.tensor([[q.xmid, q.ymid]], dtype=f64, device=dev)
+        self.node_half = torch.tensor([q.half], dtype=f64, device=dev)
+        self.node_start = torch.zeros(1, dtype=i64, device=dev)
+        self.node_end = torch.zeros(1, dtype=i64, device=dev)
+        self.node_child = torch.full((1,), -1, dtype=i64, device=dev)
+        self.node_depth = torch.zeros(1, dtype=i64, device=dev)
+        self.levels = np.array([0, 1])
+        self.node_q = torch.zeros(1, dtype=f64, device=dev)
+        self.node_qabs = torch.zeros(1, dtype=f64, device=dev)
+        self.node_p = torch.zeros((1, 2), dtype=f64, device=dev)
+        self.node_s = torch.zeros((1, 3), dtype=f64, device=dev)
+        self.moment_re = torch.zeros((1, self.order + 1), dtype=f64, device=dev)
+        self.moment_im = torch.zeros((1, self.order + 1), dtype=f64, device=dev)
+        self._sorted_pos = torch.zeros((2, 0), dtype=f64, device=dev)
+        self._sorted_charge = torch.zeros(0, dtype=f64, device=dev)
+
+    def _build(self, capacity: int | None = None) -> int:
+        """ft:483-625: the whole build in td3_quadtree_build, restarted with twice the
+        node capacity while it reports the node arrays too small (ft:523-525)."""
+        n = self.pos.shape[1]
+        dev = self.device
+        if capacity is None:
+            capacity = 4 * (2 * n // self.leaf_capacity + 16)
+        f64, i64 = torch.float64, torch.int64
+        self.perm = torch.empty(n, dtype=i64, device=dev)
+        self._sorted_pos = torch.empty((2, n), dtype=f64, device=dev)
+        sizes = np.zeros(3, dtype=np.int64)
+        while True:
+            self.node_center = torch.empty((capacity, 2), dtype=f64, device=dev)
+            self.node_half = torch.empty(capacity, dtype=f64, device=dev)
+            self.node_start = torch.empty(capacity, dtype=i64, device=dev)
+            self.node_end = torch.empty(capacity, dtype=i64, device=dev)
+            self.node_child = torch.empty(capacity, dtype=i64, device=dev)
+            self.node_depth = torch.empty(capacity, dtype=i64, device=dev)
+            levels = np.zeros(capacity + 1, dtype=np.int64)
+            ws = _lib.workspace(_lib.query("td3_quadtree_build_workspace_size", n, capacity), dev)
+            q = self.root_quad
+            rc = _lib.call(
+                "td3_quadtree_build", self.pos.data_ptr(), n, q.xmid, q.ymid, q.half,
+                self.leaf_capacity, self.max_depth, capacity, self.node_center.data_ptr(),
+                self.node_half.data_ptr(), self.node_start.data_ptr(), self.node_end.data_ptr(),
+                self.node_child.data_ptr(), self.node_depth.data_ptr(), self.perm.data_ptr(),
+                self._sorted_pos.data_ptr(), levels.ctypes.data, sizes.ctypes.data,
+                ws.data_ptr(), ws.numel(), _lib.stream(dev),
+            )
+            self.build_restarts = getattr(self, "build_restarts", 0)
+            if rc == _lib.OK:
+                break
+            self.build_restarts += 1
+            capacity *= 2
+        self.levels = levels[: sizes[1] + 1].copy()
+        self._sorted_charge = self.charge[self.perm].contiguous()
+        return int(sizes[0])
+
+    # ------------------------------------------------------------------ moments
+    def _binomial(self) -> torch.Tensor:
+        size = 2 * self.order + 1
+        return _device_table(("binomial", size), lambda: _binomial_table(size), self.device)
+
+    def _moments(self) -> None:
+        """ft:663-744: cell charges and multipole moments from the charges."""
+        count, dev, f64 = self.node_count, self.device, torch.float64
+        n = self.pos.shape[1]
+        self.node_q = torch.empty(count, dtype=f64, device=dev)
+        self.node_qabs = torch.empty(count, dtype=f64, device=dev)
+        self.node_p = torch.empty((count, 2), dtype=f64, device=dev)
+        self.node_s = torch.zeros((count, 3), dtype=f64, device=dev)
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        stream = _lib.stream(dev)
+        common = (self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(), n,
+                  self.node_center.data_ptr(), self.node_start.data_ptr(),
+                  self.node_end.data_ptr(), self.node_child.data_ptr())
+        if self.kernel == "log":
+            self.moment_re = torch.empty((count, self.order + 1), dtype=f64, device=dev)
+            self.moment_im = torch.empty((count, self.order + 1), dtype=f64, device=dev)
+            binom = self._binomial()
+            _lib.call("td3_log_moments", levels.ctypes.data, len(levels) - 1, self.order, *common,
+                      binom.data_ptr(), binom.shape[0], self.node_qabs.data_ptr(),
+                      self.moment_re.data_ptr(), self.moment_im.data_ptr(), stream)
+            self.node_q.copy_(self.moment_re[:, 0])
+            self.node_p[:, 0] = self.moment_re[:, 1]
+            self.node_p[:, 1] = self.moment_im[:, 1]
+            return
+        self.moment_re = torch.zeros((1, 1), dtype=f64, device=dev)
+        self.moment_im = torch.zeros((1, 1), dtype=f64, device=dev)
+        _lib.call("td3_quadtree_moments", levels.ctypes.data, len(levels) - 1, *common,
+                  self.node_q.data_ptr(), self.node_qabs.data_ptr(), self.node_p.data_ptr(),
+                  self.node_s.data_ptr(), stream)
+
+    def _cartesian_tables(self):
+        from tree_d_3d_b200 import _cartesian
+
+        dev = self.device
+        t = _cartesian.tables(self.order)
+        out = {}
+        for name, value in t.items():
+            dtype = torch.float64 if value.dtype.kind == "f" else torch.int64
+            out[name] = _device_table(("cart", self.order, name), lambda v=value: v, dev, dtype)
+        return out
+
+    def _cartesian_moments(self) -> torch.Tensor:
+        """ft:1063-1084: the Cartesian moments of every cell, kept until the charges change."""
+        if self._cart_moments is None:
+            from tree_d_3d_b200 import _cartesian
+
+            t = self._cartesian_tables()
+            n_coef = _cartesian.size(self.order)
+            moments = torch.empty((self.node_count, n_coef), dtype=torch.float64,
+                                  device=self.device)
+            levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+            _lib.call("td3_cart_moments", levels.ctypes.data, len(levels) - 1,
+                      self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
+                      self.pos.shape[1], self.node_center.data_ptr(), self.node_start.data_ptr(),
+                      self.node_end.data_ptr(), self.node_child.data_ptr(), t["ex"].data_ptr(),
+                      t["ey"].data_ptr(), t["shift"].data_ptr(), t["shift_coef"].data_ptr(),
+                      t["shift_start"].data_ptr(), n_coef, moments.data_ptr(),
+                      _lib.stream(self.device))
+            self._cart_moments = moments
+        return self._cart_moments
+
+    def set_charges(self, charges) -> None:
+        """New charges (N,) for the same particles, without rebuilding (ft:853-868)."""
+        charges = _device(charges).reshape(-1)
+        if charges.shape[0] != self.pos.shape[1]:
+            raise ValueError("charges must have one entry per particle")
+        self.charge.copy_(charges)
+        self._cart_moments = None
+        if self.pos.shape[1]:
+            self._sorted_charge = self.charge[self.perm].contiguous()
+            self._moments()
+
+    @property
+    def root(self) -> FlatNode:
+        return FlatNode(self, 0)
+
+    def collect_nodes(self) -> list:
+        """Views of every node that holds at least one particle (ft:870-877)."""
+        occupied = torch.nonzero(self.node_end > self.node_start).flatten().tolist()
+        return [FlatNode(self, int(i)) for i in occupied]
