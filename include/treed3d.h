@@ -35,6 +35,7 @@ extern "C" {
 #define TD3_ECUDA 2       /* a CUDA call failed (td3_last_error) */
 #define TD3_ENEEDMORE 3   /* an output buffer is too small; the needed size is reported */
 #define TD3_EWORKSPACE 4  /* the workspace is smaller than its size query */
+#define TD3_EDEPTH 5      /* the tree is too deep for the walk (depth > 190) */
 
 #define TD3_KERNEL_COULOMB 0
 #define TD3_KERNEL_LOG 1
@@ -142,6 +143,45 @@ int td3_cart_moments(const int64_t* levels, int64_t n_levels, const double* sort
                      const int64_t* node_child, const int64_t* ex, const int64_t* ey,
                      const int64_t* shift, const double* shift_coef, const int64_t* shift_start,
                      int n_coef, double* moments, void* stream);
+
+/* ------------------------------------------------------------------ Barnes-Hut walk */
+
+/* An order of the m targets (2, m) in which consecutive ones are close: the stable
+ * sort of the reference's 16-bit Morton keys ((t - lo) * 65535 / span, x bits odd,
+ * y bits even), written to order (m, int64).  Replaces FlatQuadtree._target_order
+ * (src/tree_d_3d/flat_tree.py:891-912). */
+size_t td3_target_order_workspace_size(int64_t m);
+int td3_target_order(const double* targets, int64_t m, int64_t* order, void* workspace,
+                     size_t workspace_bytes, void* stream);
+
+/* Potential (m) and field (2, m) at `targets` by the Barnes-Hut walk, without k_e.
+ * kernel TD3_KERNEL_COULOMB uses node_q, node_p, node_s (monopole through quadrupole,
+ * softened far field); TD3_KERNEL_LOG uses moment_re / moment_im (nodes, order_p + 1)
+ * (unsoftened series).  A cell containing the target is always opened; otherwise it is
+ * accepted when 2h < theta |r - c| (Coulomb) or (4h) h < theta^2 |r - c|^2 (log), as in
+ * the reference.  Cells with node_qabs == 0 are skipped; leaves are summed directly
+ * (sorted_pos, sorted_charge in tree order, perm = source index of each slot), skipping
+ * source exclude[i] for target i.  order (m, may be NULL) is the processing order of
+ * the targets (warps take 32 consecutive ones).  tree_depth is the deepest node depth;
+ * above 190 the call returns TD3_EDEPTH.  with_potential = 0 writes phi = 0 and skips
+ * the log kernel's logarithms.
+ * Replaces evaluate_quadtree (src/tree_d_3d/kernels/evaluate_quadtree/
+ * evaluate_quadtree_cuda.cu:9-107), evaluate_log_quadtree (kernels/evaluate_log_quadtree/
+ * evaluate_log_quadtree_cuda.cu:9-104) and the CPU walk evaluate_groups
+ * (kernels/evaluate_groups/evaluate_groups_pyccel.py:16-297), called by
+ * FlatQuadtree.evaluate (src/tree_d_3d/flat_tree.py:987-1061). */
+size_t td3_walk_workspace_size(int64_t node_count, int kernel);
+int td3_evaluate_quadtree(int kernel, const double* targets, int64_t m, const int64_t* exclude,
+                          const int64_t* order, const double* sorted_pos,
+                          const double* sorted_charge, const int64_t* perm, int64_t n,
+                          int64_t node_count, const double* node_center, const double* node_half,
+                          const int64_t* node_start, const int64_t* node_end,
+                          const int64_t* node_child, const int64_t* node_depth,
+                          int64_t tree_depth, const double* node_q, const double* node_qabs,
+                          const double* node_p, const double* node_s, const double* moment_re,
+                          const double* moment_im, int order_p, double theta, double softening,
+                          int with_potential, double* phi, double* field, int64_t* status,
+                          void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------ utilities */
 

@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "libtreed3d.so"
 HEADER = HERE.parent / "include" / "treed3d.h"
 
-OK, EINVAL, ECUDA, ENEEDMORE, EWORKSPACE = 0, 1, 2, 3, 4
+OK, EINVAL, ECUDA, ENEEDMORE, EWORKSPACE, EDEPTH = 0, 1, 2, 3, 4, 5
 KERNEL_COULOMB, KERNEL_LOG = 0, 1
 
 _CTYPES = {
@@ -83,6 +83,10 @@ def declared_symbols() -> list:
 def call(name: str, *args) -> int:
     """Call entry point ``name``; raise LibraryError on an error code other than ENEEDMORE."""
     rc = getattr(lib(), name)(*args)
+    if rc == EDEPTH:
+        raise RuntimeError(
+            "the quadtree is too deep for the traversal of the CUDA kernels; lower max_depth"
+        )
     if rc not in (OK, ENEEDMORE):
         detail = lib().td3_last_error().decode() if rc == ECUDA else ""
         raise LibraryError(f"{name} failed with code {rc} {detail}".strip())

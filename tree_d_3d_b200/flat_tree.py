@@ -391,3 +391,87 @@ class FlatQuadtree:
         """Views of every node that holds at least one particle (ft:870-877)."""
         occupied = torch.nonzero(self.node_end > self.node_start).flatten().tolist()
         return [FlatNode(self, int(i)) for i in occupied]
+
+    # ------------------------------------------------------------------ walk
+    @property
+    def tree_depth(self) -> int:
+        """The depth of the deepest node."""
+        return len(self.levels) - 2
+
+    def _target_order(self, targets: torch.Tensor) -> torch.Tensor:
+        """ft:891-912: tree order for the sources themselves, else Morton order."""
+        if targets.shape == self.pos.shape and torch.equal(targets, self.pos):
+            return self.perm
+        m = targets.shape[1]
+        order = torch.empty(m, dtype=torch.int64, device=self.device)
+        ws = _lib.workspace(_lib.query("td3_target_order_workspace_size", m), self.device)
+        _lib.call("td3_target_order", targets.data_ptr(), m, order.data_ptr(), ws.data_ptr(),
+                  ws.numel(), _lib.stream(self.device))
+        return order
+
+    def _walk(self, targets, exclude, theta, softening, potential, phi, field, status):
+        m, n = targets.shape[1], self.pos.shape[1]
+        order = self._target_order(targets)
+        kernel = _kernel_code(self.kernel)
+        ws = _lib.workspace(_lib.query("td3_walk_workspace_size", self.node_count, kernel),
+                            self.device)
+        _lib.call(
+            "td3_evaluate_quadtree", kernel, targets.data_ptr(), m, exclude.data_ptr(),
+            order.data_ptr(), self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
+            self.perm.data_ptr(), n, self.node_count, self.node_center.data_ptr(),
+            self.node_half.data_ptr(), self.node_start.data_ptr(), self.node_end.data_ptr(),
+            self.node_child.data_ptr(), self.node_depth.data_ptr(), self.tree_depth,
+            self.node_q.data_ptr(), self.node_qabs.data_ptr(), self.node_p.data_ptr(),
+            self.node_s.data_ptr(), self.moment_re.data_ptr(), self.moment_im.data_ptr(),
+            self.order, float(theta), float(softening), 1 if potential else 0,
+            phi.data_ptr(), field.data_ptr(), status.data_ptr(), ws.data_ptr(), ws.numel(),
+            _lib.stream(self.device),
+        )
+
+    def evaluate(self, targets, *, exclude=None, theta=0.5, softening=0.0, potential=True):
+        """Potential (M,) and field (2, M) at ``targets`` (2, M) by the Barnes-Hut walk,
+        without ``k_e`` (ft:987-1061).
+
+        ``exclude[i]`` is a source index skipped for target ``i`` (-1: none);
+        ``potential=False`` returns the potential as zeros (and skips the line-charge
+        kernel's logarithms).
+        """
+        as_numpy = wants_numpy(targets)
+        targets = _points(targets, "targets")
+        m = targets.shape[1]
+        if exclude is None:
+            exclude = torch.full((m,), -1, dtype=torch.int64, device=self.device)
+        exclude = _device(exclude, torch.int64).reshape(-1)
+        phi = torch.zeros(m, dtype=torch.float64, device=self.device)
+        field = torch.zeros((2, m), dtype=torch.float64, device=self.device)
+        if self.pos.shape[1] and m:
+            status = status_word(self.device)
+            self._walk(targets, exclude, theta, softening, potential, phi, field, status)
+            _check(status)
+        if not potential:
+            phi.zero_()
+        return out((phi, field), as_numpy)
+
+    def field_at(self, positions, *, theta: float = 0.5, k_e: float = K_E,
+                 softening: float = 0.0, reference_radius: float = 1.0):
+        """Potential (n,) and field (2, n) at probes (2, n), times ``k_e`` (ft:1648-1676).
+
+        For line charges the potential is -2 k_e sum q ln(r / reference_radius).
+        """
+        theta = _finite("theta", theta, minimum=0)
+        reference_radius = _finite("reference_radius", reference_radius, positive=True)
+        k_e = _finite("k_e", k_e, minimum=0)
+        softening = _finite("softening", softening, minimum=0)
+        as_numpy = wants_numpy(positions)
+        positions = _points(positions, "positions")
+        if not bool(torch.isfinite(positions).all()):
+            raise ValueError("positions must be finite")
+        n = positions.shape[1]
+        if k_e == 0:
+            zeros = (torch.zeros(n, dtype=torch.float64, device=self.device),
+                     torch.zeros((2, n), dtype=torch.float64, device=self.device))
+            return out(zeros, as_numpy)
+        phi, field = self.evaluate(positions, theta=theta, softening=softening)
+        if self.kernel == "log":
+            phi = phi + 2 * torch.sum(self.charge) * float(np.log(reference_radius))
+        return out((k_e * phi, k_e * field), as_numpy)
