@@ -183,6 +183,104 @@ int td3_evaluate_quadtree(int kernel, const double* targets, int64_t m, const in
                           int with_potential, double* phi, double* field, int64_t* status,
                           void* workspace, size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------ FMM lists */
+
+/* The mutual dual-tree traversal of one tree from the pair (root, root): a pair of
+ * cells becomes an M2L pair if sqrt(2) (h_a + h_b) < theta d (d the centre distance), a
+ * P2P pair if both are leaves (or a == b is a leaf), else the pairs of the children
+ * of the larger (or the non-leaf) cell, or of a == b the 10 pairs c <= d; empty cells
+ * are dropped.  m2l (m2l_capacity, 2) and p2p (p2p_capacity, 2) receive the pairs in
+ * the reference's serial order (generation by generation, frontier order); sizes
+ * (HOST, 4) = n_m2l, n_p2p, next frontier, -1 on overflow, when TD3_ENEEDMORE is
+ * returned (retry with larger buffers).  frontier_capacity bounds one generation.
+ * Synchronises `stream` once per generation.  Replaces fmm_traverse
+ * (src/tree_d_3d/kernels/fmm_traverse/fmm_traverse_pyccel.py:15-106,
+ * fmm_traverse_cuda.cu:14-97) driven by FlatQuadtree._traverse
+ * (src/tree_d_3d/flat_tree.py:1318-1358); identical lists. */
+size_t td3_fmm_traverse_workspace_size(int64_t frontier_capacity);
+int td3_fmm_traverse(const double* node_center, const double* node_half,
+                     const int64_t* node_start, const int64_t* node_end,
+                     const int64_t* node_child, double theta, int64_t* m2l, int64_t m2l_capacity,
+                     int64_t* p2p, int64_t p2p_capacity, int64_t frontier_capacity,
+                     int64_t* sizes, void* workspace, size_t workspace_bytes, void* stream);
+
+/* The one-way traversal of a target tree (t_*) against a source tree (s_*) from
+ * (root, root), with the predicates of td3_fmm_traverse; pairs are (target cell,
+ * source cell), breadth first (the reference walks depth first: the same set of
+ * pairs in another order).  Replaces dual_traverse (src/tree_d_3d/kernels/
+ * dual_traverse/dual_traverse_pyccel.py:14-86) of FlatQuadtree._dual_lists
+ * (src/tree_d_3d/flat_tree.py:1086-1122).  Uses the workspace size of
+ * td3_fmm_traverse_workspace_size. */
+int td3_dual_traverse(const double* t_center, const double* t_half, const int64_t* t_start,
+                      const int64_t* t_end, const int64_t* t_child, const double* s_center,
+                      const double* s_half, const int64_t* s_start, const int64_t* s_end,
+                      const int64_t* s_child, double theta, int64_t* m2l, int64_t m2l_capacity,
+                      int64_t* p2p, int64_t p2p_capacity, int64_t frontier_capacity,
+                      int64_t* sizes, void* workspace, size_t workspace_bytes, void* stream);
+
+/* Rows by node of the pairs (count, 2): row_start (n_nodes + 1) and partners, in pair
+ * order; mutual != 0 lists b under a and a under b (once if a == b).  Replaces pair_csr
+ * (src/tree_d_3d/kernels/pair_csr/pair_csr_pyccel.py:12-45); identical rows. */
+size_t td3_pair_csr_workspace_size(int64_t count, int mutual, int64_t n_nodes);
+int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int64_t n_nodes,
+                 int64_t* row_start, int64_t* partners, void* workspace, size_t workspace_bytes,
+                 void* stream);
+
+/* ------------------------------------------------------------------ log-kernel FMM */
+
+/* M2L of the log kernel, FP64: adds to the local expansions (local_re / local_im
+ * (n_dst, order + 1)) of every destination cell n the translated multipoles of the
+ * source cells partners[row_start[n]:row_start[n + 1]]: with t = c_dst - c_src,
+ * w = 1/t and a'_k = a_k w^k, s_l = sum_k coeff[k, l] a'_k (coeff the reference's real
+ * M2L matrix, (order + 1)^2, _m2l_coefficients, src/tree_d_3d/flat_tree.py:234-245),
+ * b_0 += a_0 ln|t| - s_0, b_l += -(-1)^l s_l w^l.  (Im ln t, which only moves Im b_0,
+ * is dropped: Im b_0 never reaches the potential or the field.)  Replaces
+ * fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/fmm_m2l_host_pyccel.py:16-105) and
+ * fmm_m2l (kernels/fmm_m2l/fmm_m2l_cuda.cu:12-80). */
+int td3_fmm_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                const double* dst_center, const double* src_center, const double* moment_re,
+                const double* moment_im, int order, const double* coeff, double* local_re,
+                double* local_im, void* stream);
+
+/* L2L from the root down, level by level (levels HOST, n_levels + 1): every local
+ * expansion shifted into its children, b_m(child) += sum_{l>=m} C(l, m) b_l s^(l-m).
+ * Replaces fmm_downward (src/tree_d_3d/kernels/fmm_downward/fmm_downward_pyccel.py:15-64,
+ * fmm_downward_cuda.cu:10-51) and its per-level loop (src/tree_d_3d/flat_tree.py:1540-1552). */
+int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node_center,
+                     const int64_t* node_child, int order, const double* binomial,
+                     int binomial_size, double* local_re, double* local_im, void* stream);
+
+/* L2P (phi += -2 Re W, Ex - i Ey += 2 W') at the particles of every leaf plus the
+ * exact near field over the leaf's P2P partners (p2p_rows / p2p_partners: the mutual
+ * P2P pairs as rows, td3_pair_csr with mutual = 1), softened, excluding each particle
+ * itself; phi (n) and field (2, n) in input order (perm).  A coincident pair of two
+ * nonzero charges reports 1 + a particle index.  Replaces fmm_evaluate_host
+ * (src/tree_d_3d/kernels/fmm_evaluate_host/fmm_evaluate_host_pyccel.py:14-100) and
+ * fmm_evaluate (kernels/fmm_evaluate/fmm_evaluate_cuda.cu:11-87). */
+int td3_fmm_evaluate(const double* sorted_pos, const double* sorted_charge, const int64_t* perm,
+                     int64_t n, int64_t node_count, const double* node_center,
+                     const int64_t* node_start, const int64_t* node_end,
+                     const int64_t* node_child, int order, const double* local_re,
+                     const double* local_im, const int64_t* p2p_rows,
+                     const int64_t* p2p_partners, double softening, int with_potential,
+                     double* phi, double* field, int64_t* status, void* stream);
+
+/* fmm_at, log kernel: L2P at the m targets (sorted_targets (2, m) in target-tree order,
+ * target_perm their input indices, sorted_exclude their excluded source index) plus
+ * exact sums over the partner source leaves (rows / partners by target cell) of the
+ * source tree (sorted_pos, sorted_charge, perm, s_start, s_end), skipping zero charges
+ * and source exclude; results at the targets' input indices.  Replaces
+ * log_targets_host (src/tree_d_3d/kernels/log_targets_host/log_targets_host_pyccel.py:14-94). */
+int td3_log_targets(const double* sorted_targets, const int64_t* sorted_exclude,
+                    const int64_t* target_perm, int64_t m, int64_t t_count,
+                    const double* t_center, const int64_t* t_start, const int64_t* t_end,
+                    const int64_t* t_child, int order, const double* local_re,
+                    const double* local_im, const int64_t* rows, const int64_t* partners,
+                    const double* sorted_pos, const double* sorted_charge, const int64_t* perm,
+                    int64_t n, const int64_t* s_start, const int64_t* s_end, double softening,
+                    int with_potential, double* phi, double* field, int64_t* status,
+                    void* stream);
+
 /* ------------------------------------------------------------------ utilities */
 
 /* Stable radix sort of (key, value) uint32 pairs by the low `bits` bits of the key.

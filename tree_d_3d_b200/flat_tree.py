@@ -475,3 +475,109 @@ class FlatQuadtree:
         if self.kernel == "log":
             phi = phi + 2 * torch.sum(self.charge) * float(np.log(reference_radius))
         return out((k_e * phi, k_e * field), as_numpy)
+
+    # ------------------------------------------------------------------ FMM lists
+    def _traverse(self, theta: float):
+        """ft:1318-1358: the mutual M2L and P2P pair lists, restarting with larger
+        buffers while a generation overflows."""
+        dev = self.device
+        capacity = np.array([24, 16, 12]) * self.node_count + 64
+        sizes = np.zeros(4, dtype=np.int64)
+        while True:
+            m2l = torch.empty((int(capacity[0]), 2), dtype=torch.int64, device=dev)
+            p2p = torch.empty((int(capacity[1]), 2), dtype=torch.int64, device=dev)
+            ws = _lib.workspace(_lib.query("td3_fmm_traverse_workspace_size", int(capacity[2])), dev)
+            rc = _lib.call(
+                "td3_fmm_traverse", self.node_center.data_ptr(), self.node_half.data_ptr(),
+                self.node_start.data_ptr(), self.node_end.data_ptr(), self.node_child.data_ptr(),
+                float(theta), m2l.data_ptr(), int(capacity[0]), p2p.data_ptr(), int(capacity[1]),
+                int(capacity[2]), sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
+            if rc == _lib.OK:
+                return m2l[: sizes[0]].clone(), p2p[: sizes[1]].clone()
+            capacity = np.maximum(2 * capacity, sizes[:3] + 64)
+
+    def _rows(self, pairs: torch.Tensor, mutual: bool, n_nodes: int | None = None):
+        """pair_csr (K/pair_csr/pair_csr_pyccel.py:12-45): rows by node of ``pairs``."""
+        dev = self.device
+        n_nodes = self.node_count if n_nodes is None else n_nodes
+        count = pairs.shape[0]
+        rows = torch.zeros(n_nodes + 1, dtype=torch.int64, device=dev)
+        partners = torch.empty(max((2 if mutual else 1) * count, 1), dtype=torch.int64, device=dev)
+        ws = _lib.workspace(_lib.query("td3_pair_csr_workspace_size", count, int(mutual), n_nodes),
+                            dev)
+        _lib.call("td3_pair_csr", pairs.data_ptr(), count, int(mutual), n_nodes, rows.data_ptr(),
+                  partners.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream(dev))
+        return rows, partners
+
+    def _lists(self, theta: float) -> dict:
+        """The interaction lists of ``theta`` and their rows, kept across set_charges
+        (ft:1496-1498): they depend on the cells only."""
+        if theta not in self._traversals:
+            m2l, p2p = self._traverse(theta)
+            m2l_rows, m2l_partners = self._rows(m2l, mutual=True)
+            p2p_rows, p2p_partners = self._rows(p2p, mutual=True)
+            self._traversals[theta] = {
+                "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
+                "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
+            }
+        return self._traversals[theta]
+
+    def _m2l_matrix(self) -> torch.Tensor:
+        key = ("m2l_coefficients", self.order, self.symmetric)
+        return _device_table(key, lambda: _m2l_coefficients(self.order, self.symmetric),
+                             self.device)
+
+    # ------------------------------------------------------------------ FMM
+    def fmm(self, *, theta: float = 0.5, softening: float = 0.0, potential: bool = True):
+        """Potential (N,) and field (2, N) at every source by the FMM, without ``k_e``
+        (ft:1460-1634): complex expansions for ``kernel="log"``, Cartesian expansions of
+        the softened kernel for ``kernel="coulomb"``; each particle's own charge
+        excluded; ``potential=False`` returns zeros for the potential."""
+        theta = _finite("theta", theta, minimum=0)
+        if not 0 < theta < 1:
+            raise ValueError("FMM theta must lie in (0, 1)")
+        softening = _finite("softening", softening, minimum=0)
+        n, dev = self.pos.shape[1], self.device
+        phi = torch.zeros(n, dtype=torch.float64, device=dev)
+        field = torch.zeros((2, n), dtype=torch.float64, device=dev)
+        if not n:
+            return out((phi, field), self._numpy)
+        if self.kernel != "log":
+            self._coulomb_fmm(theta, softening, phi, field)
+            return out((phi, field), self._numpy)
+        lists = self._lists(theta)
+        local_re, local_im = self._log_locals(lists)
+        status = status_word(dev)
+        _lib.call(
+            "td3_fmm_evaluate", self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
+            self.perm.data_ptr(), n, self.node_count, self.node_center.data_ptr(),
+            self.node_start.data_ptr(), self.node_end.data_ptr(), self.node_child.data_ptr(),
+            self.order, local_re.data_ptr(), local_im.data_ptr(), lists["p2p_rows"].data_ptr(),
+            lists["p2p_partners"].data_ptr(), float(softening), 1 if potential else 0,
+            phi.data_ptr(), field.data_ptr(), status.data_ptr(), _lib.stream(dev))
+        _check(status)
+        self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
+        return out((phi, field), self._numpy)
+
+    def _log_locals(self, lists: dict):
+        """M2L into every cell's local expansion, then L2L down the tree."""
+        dev, count, w = self.device, self.node_count, self.order + 1
+        local_re = torch.zeros((count, w), dtype=torch.float64, device=dev)
+        local_im = torch.zeros((count, w), dtype=torch.float64, device=dev)
+        stream = _lib.stream(dev)
+        if lists["m2l"].shape[0]:
+            _lib.call("td3_fmm_m2l", lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(),
+                      count, self.node_center.data_ptr(), self.node_center.data_ptr(),
+                      self.moment_re.data_ptr(), self.moment_im.data_ptr(), self.order,
+                      self._m2l_matrix().data_ptr(), local_re.data_ptr(), local_im.data_ptr(),
+                      stream)
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        binom = self._binomial()
+        _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
+                  self.node_center.data_ptr(), self.node_child.data_ptr(), self.order,
+                  binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
+                  stream)
+        return local_re, local_im
+
+    def _coulomb_fmm(self, theta, softening, phi, field):
+        raise NotImplementedError("the Coulomb FMM is not built yet")
