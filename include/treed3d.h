@@ -250,34 +250,59 @@ int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node
                      const int64_t* node_child, int order, const double* binomial,
                      int binomial_size, double* local_re, double* local_im, void* stream);
 
-/* L2P (phi += -2 Re W, Ex - i Ey += 2 W') at the particles of every leaf plus the
- * exact near field over the leaf's P2P partners (p2p_rows / p2p_partners: the mutual
- * P2P pairs as rows, td3_pair_csr with mutual = 1), softened, excluding each particle
- * itself; phi (n) and field (2, n) in input order (perm).  A coincident pair of two
- * nonzero charges reports 1 + a particle index.  Replaces fmm_evaluate_host
- * (src/tree_d_3d/kernels/fmm_evaluate_host/fmm_evaluate_host_pyccel.py:14-100) and
- * fmm_evaluate (kernels/fmm_evaluate/fmm_evaluate_cuda.cu:11-87). */
-int td3_fmm_evaluate(const double* sorted_pos, const double* sorted_charge, const int64_t* perm,
-                     int64_t n, int64_t node_count, const double* node_center,
-                     const int64_t* node_start, const int64_t* node_end,
-                     const int64_t* node_child, int order, const double* local_re,
-                     const double* local_im, const int64_t* p2p_rows,
-                     const int64_t* p2p_partners, double softening, int with_potential,
+/* ------------------------------------------------------------------ near field */
+
+/* The work plan of the near field: every non-empty leaf's row of P2P partners
+ * (rows: n_nodes + 1 offsets, td3_pair_csr) cut into segments of at most `segment`
+ * partners.  seg_leaf (int32), seg_range (e0, e1 pairs) and seg_out (-1: the leaf has
+ * one segment and writes its final values; else the offset, in targets, of the
+ * segment's partial sums) receive n_seg entries; sizes (HOST, 2) = n_seg and the
+ * partial length (the caller allocates 3 * partial length doubles for the evaluation).
+ * TD3_ENEEDMORE when seg_capacity < n_seg (n_seg is still reported).  Synchronises
+ * `stream` once.  No reference counterpart (the reference's near field is serial on
+ * the CPU and one thread per pair with atomics on the GPU). */
+size_t td3_nearfield_plan_workspace_size(int64_t n_nodes);
+int td3_nearfield_plan(const int64_t* rows, int64_t n_nodes, const int64_t* node_child,
+                       const int64_t* node_start, const int64_t* node_end, int segment,
+                       int* seg_leaf, int64_t* seg_range, int64_t* seg_out, int64_t seg_capacity,
+                       int64_t* sizes, void* workspace, size_t workspace_bytes, void* stream);
+
+/* L2P at the particles of every leaf plus the exact near field over the leaf's P2P
+ * partners (the mutual P2P pairs as rows, cut by td3_nearfield_plan), softened,
+ * excluding each particle itself; phi (n) and field (2, n) in input order (perm).
+ * kernel TD3_KERNEL_LOG: complex local expansion local_a / local_b = local_re /
+ * local_im (nodes, order + 1), phi += -2 Re W, Ex - i Ey += 2 W' (W' skipped logs when
+ * with_potential = 0); TD3_KERNEL_COULOMB: Cartesian local expansion local_a (nodes,
+ * (order + 1)(order + 2)/2), softened Coulomb pairs.  A coincident pair of two nonzero
+ * charges reports 1 + a particle index.  partial: 3 * partial length doubles.
+ * Replaces fmm_evaluate_host (src/tree_d_3d/kernels/fmm_evaluate_host/
+ * fmm_evaluate_host_pyccel.py:14-100), fmm_evaluate (kernels/fmm_evaluate/
+ * fmm_evaluate_cuda.cu:11-87) and cart_evaluate_host (kernels/cart_evaluate_host/
+ * cart_evaluate_host_pyccel.py:16-110). */
+int td3_fmm_evaluate(int kernel, const double* sorted_pos, const double* sorted_charge,
+                     const int64_t* perm, int64_t n, const double* node_center,
+                     const int64_t* node_start, const int64_t* node_end, int order,
+                     const double* local_a, const double* local_b, const int64_t* p2p_partners,
+                     const int* seg_leaf, const int64_t* seg_range, const int64_t* seg_out,
+                     int64_t n_seg, double* partial, double softening, int with_potential,
                      double* phi, double* field, int64_t* status, void* stream);
 
-/* fmm_at, log kernel: L2P at the m targets (sorted_targets (2, m) in target-tree order,
- * target_perm their input indices, sorted_exclude their excluded source index) plus
- * exact sums over the partner source leaves (rows / partners by target cell) of the
- * source tree (sorted_pos, sorted_charge, perm, s_start, s_end), skipping zero charges
- * and source exclude; results at the targets' input indices.  Replaces
- * log_targets_host (src/tree_d_3d/kernels/log_targets_host/log_targets_host_pyccel.py:14-94). */
-int td3_log_targets(const double* sorted_targets, const int64_t* sorted_exclude,
-                    const int64_t* target_perm, int64_t m, int64_t t_count,
-                    const double* t_center, const int64_t* t_start, const int64_t* t_end,
-                    const int64_t* t_child, int order, const double* local_re,
-                    const double* local_im, const int64_t* rows, const int64_t* partners,
-                    const double* sorted_pos, const double* sorted_charge, const int64_t* perm,
-                    int64_t n, const int64_t* s_start, const int64_t* s_end, double softening,
+/* fmm_at: L2P at the m targets (sorted_targets (2, m) in target-tree order, target_perm
+ * their input indices, sorted_exclude their excluded source index) plus exact sums over
+ * the partner source leaves of each target leaf (the one-way P2P rows cut by
+ * td3_nearfield_plan on the target tree) of the source tree (sorted_pos, sorted_charge,
+ * perm, s_start, s_end), skipping zero charges and the excluded source; results at the
+ * targets' input indices; a coincident charge reports 1 + the target index.  Replaces
+ * log_targets_host (src/tree_d_3d/kernels/log_targets_host/log_targets_host_pyccel.py:14-94)
+ * and cart_targets_host (kernels/cart_targets_host/cart_targets_host_pyccel.py:16-98). */
+int td3_fmm_targets(int kernel, const double* sorted_targets, const int64_t* sorted_exclude,
+                    const int64_t* target_perm, int64_t m, const double* t_center,
+                    const int64_t* t_start, const int64_t* t_end, int order,
+                    const double* local_a, const double* local_b, const int64_t* p2p_partners,
+                    const int* seg_leaf, const int64_t* seg_range, const int64_t* seg_out,
+                    int64_t n_seg, double* partial, const double* sorted_pos,
+                    const double* sorted_charge, const int64_t* perm, int64_t n,
+                    const int64_t* s_start, const int64_t* s_end, double softening,
                     int with_potential, double* phi, double* field, int64_t* status,
                     void* stream);
 

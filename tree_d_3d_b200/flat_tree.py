@@ -168,6 +168,35 @@ def _m2l_coefficients(order: int, symmetric: bool) -> np.ndarray:
     return coeff
 
 
+#: partners per near-field work segment (one warp each)
+NEAR_SEGMENT = 32
+
+
+def _nearfield_plan(rows: torch.Tensor, tree) -> dict:
+    """The near-field work plan of one tree's leaf rows (td3_nearfield_plan): leaf rows
+    cut into segments of at most NEAR_SEGMENT partners, and the partial-sum buffer of
+    the rows that take several segments."""
+    dev = rows.device
+    n_nodes = rows.shape[0] - 1
+    entries = int(rows[-1].item())
+    capacity = n_nodes + entries // NEAR_SEGMENT + 1
+    seg_leaf = torch.empty(capacity, dtype=torch.int32, device=dev)
+    seg_range = torch.empty((capacity, 2), dtype=torch.int64, device=dev)
+    seg_out = torch.empty(capacity, dtype=torch.int64, device=dev)
+    sizes = np.zeros(2, dtype=np.int64)
+    ws = _lib.workspace(_lib.query("td3_nearfield_plan_workspace_size", n_nodes), dev)
+    _lib.call("td3_nearfield_plan", rows.data_ptr(), n_nodes, tree.node_child.data_ptr(),
+              tree.node_start.data_ptr(), tree.node_end.data_ptr(), NEAR_SEGMENT,
+              seg_leaf.data_ptr(), seg_range.data_ptr(), seg_out.data_ptr(), capacity,
+              sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
+    n_seg = int(sizes[0])
+    return {
+        "seg_leaf": seg_leaf[:n_seg], "seg_range": seg_range[:n_seg], "seg_out": seg_out[:n_seg],
+        "n_seg": n_seg,
+        "partial": torch.empty(3 * max(int(sizes[1]), 1), dtype=torch.float64, device=dev),
+    }
+
+
 def _device_table(key, make, dev, dtype=torch.float64):
     full = (key, dev)
     if full not in _TABLES:
@@ -510,16 +539,18 @@ class FlatQuadtree:
         return rows, partners
 
     def _lists(self, theta: float) -> dict:
-        """The interaction lists of ``theta`` and their rows, kept across set_charges
-        (ft:1496-1498): they depend on the cells only."""
+        """The interaction lists of ``theta``, their rows and the near-field plan, kept
+        across set_charges (ft:1496-1498): they depend on the cells only."""
         if theta not in self._traversals:
             m2l, p2p = self._traverse(theta)
             m2l_rows, m2l_partners = self._rows(m2l, mutual=True)
             p2p_rows, p2p_partners = self._rows(p2p, mutual=True)
-            self._traversals[theta] = {
+            lists = {
                 "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
                 "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
             }
+            lists["plan"] = _nearfield_plan(p2p_rows, self)
+            self._traversals[theta] = lists
         return self._traversals[theta]
 
     def _m2l_matrix(self) -> torch.Tensor:
@@ -548,13 +579,8 @@ class FlatQuadtree:
         lists = self._lists(theta)
         local_re, local_im = self._log_locals(lists)
         status = status_word(dev)
-        _lib.call(
-            "td3_fmm_evaluate", self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
-            self.perm.data_ptr(), n, self.node_count, self.node_center.data_ptr(),
-            self.node_start.data_ptr(), self.node_end.data_ptr(), self.node_child.data_ptr(),
-            self.order, local_re.data_ptr(), local_im.data_ptr(), lists["p2p_rows"].data_ptr(),
-            lists["p2p_partners"].data_ptr(), float(softening), 1 if potential else 0,
-            phi.data_ptr(), field.data_ptr(), status.data_ptr(), _lib.stream(dev))
+        self._evaluate_near(lists, _lib.KERNEL_LOG, local_re, local_im, softening, potential,
+                            phi, field, status)
         _check(status)
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
         return out((phi, field), self._numpy)
@@ -578,6 +604,20 @@ class FlatQuadtree:
                   binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
                   stream)
         return local_re, local_im
+
+    def _evaluate_near(self, lists, kernel, local_a, local_b, softening, potential, phi, field,
+                       status):
+        """L2P + P2P at the sources (td3_fmm_evaluate) over the near-field plan."""
+        plan = lists["plan"]
+        n = self.pos.shape[1]
+        _lib.call(
+            "td3_fmm_evaluate", kernel, self._sorted_pos.data_ptr(),
+            self._sorted_charge.data_ptr(), self.perm.data_ptr(), n, self.node_center.data_ptr(),
+            self.node_start.data_ptr(), self.node_end.data_ptr(), self.order, local_a.data_ptr(),
+            local_b.data_ptr(), lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
+            plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
+            plan["partial"].data_ptr(), float(softening), 1 if potential else 0, phi.data_ptr(),
+            field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
 
     def _coulomb_fmm(self, theta, softening, phi, field):
         raise NotImplementedError("the Coulomb FMM is not built yet")
