@@ -36,6 +36,7 @@ extern "C" {
 #define TD3_ENEEDMORE 3   /* an output buffer is too small; the needed size is reported */
 #define TD3_EWORKSPACE 4  /* the workspace is smaller than its size query */
 #define TD3_EDEPTH 5      /* the tree is too deep for the walk (depth > 190) */
+#define TD3_ETOOLARGE 6   /* the call needs more than a no-allocation entry's fixed scratch */
 
 #define TD3_KERNEL_COULOMB 0
 #define TD3_KERNEL_LOG 1
@@ -65,6 +66,22 @@ int td3_direct_sum(int kernel, const double* targets, int64_t n_targets, const i
                    const double* pos, const double* charge, int64_t n_sources, double softening,
                    int with_potential, double* phi, double* field, int64_t* status,
                    void* workspace, size_t workspace_bytes, void* stream);
+
+/* td3_direct_sum without a workspace, for callers that cannot allocate device memory
+ * (a host application that owns all device memory and passes only inputs and outputs,
+ * a loop where an allocation could block).  No counterpart in the reference.  Its
+ * scratch is a fixed device array of the library (4.6 MiB on every device that loads
+ * it, kept until exit), enough for at most TD3_DIRECT_NOALLOC_MAX_TARGETS targets and
+ * any number of sources; more targets return TD3_ETOOLARGE (td3_last_error says why).
+ * The first call on a device looks up the array's device address (once per device,
+ * with that device current); make that first call before any stream capture.  Every
+ * call shares the array: calls that overlap on the GPU (other streams, other threads)
+ * race on it.  Results equal td3_direct_sum's. */
+#define TD3_DIRECT_NOALLOC_MAX_TARGETS 65536
+int td3_direct_sum_noalloc(int kernel, const double* targets, int64_t n_targets,
+                           const int64_t* exclude, const double* pos, const double* charge,
+                           int64_t n_sources, double softening, int with_potential,
+                           double* phi, double* field, int64_t* status, void* stream);
 
 /* Exact pair energy sum_{i<j} q_i q_j / sqrt(r^2 + eps^2) of the Coulomb kernel, added
  * to energy[0] (device).  Replaces pair_energy (src/tree_d_3d/kernels/pair_energy/

@@ -18,7 +18,7 @@ HERE = Path(__file__).resolve().parent
 LIBRARY = HERE / "libtreed3d.so"
 HEADER = HERE.parent / "include" / "treed3d.h"
 
-OK, EINVAL, ECUDA, ENEEDMORE, EWORKSPACE, EDEPTH = 0, 1, 2, 3, 4, 5
+OK, EINVAL, ECUDA, ENEEDMORE, EWORKSPACE, EDEPTH, ETOOLARGE = 0, 1, 2, 3, 4, 5, 6
 KERNEL_COULOMB, KERNEL_LOG = 0, 1
 
 _CTYPES = {

@@ -29,6 +29,9 @@ typedef int64_t i64;
 // Records the CUDA error for td3_last_error and maps it to TD3_ECUDA.
 int td3_cuda_error(cudaError_t err);
 
+// Records a message for td3_last_error.
+void td3_set_error(const char* message);
+
 static inline cudaStream_t td3_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 static inline unsigned td3_blocks(i64 n, int threads) {

@@ -5,6 +5,8 @@
 // the targets alone cannot fill the GPU (few targets, many sources), the sources are
 // split into chunks along gridDim.y and each chunk writes partial sums to the
 // workspace, reduced afterwards in a fixed order (deterministic results).
+#include <mutex>
+
 #include "common.cuh"
 
 namespace {
@@ -239,4 +241,87 @@ extern "C" int td3_pair_energy(const double* pos, const double* charge, int64_t 
     k_sum_into<<<1, 256, 0, s>>>(partial, blocks, energy);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
+}
+
+// ------------------------------------------------------------------ without allocation
+//
+// td3_direct_sum_noalloc is td3_direct_sum for callers that cannot allocate device
+// memory: code running inside a host application that owns all device memory and
+// hands the solver only its inputs and outputs (a plugin with a fixed memory budget,
+// a control loop where an allocation could block).  Its scratch -- the partial sums of
+// the source chunks -- lives in the array below, a fixed part of every device that
+// loads the library, kept until the process exits.  The array holds the partial sums
+// of any call with at most TD3_DIRECT_NOALLOC_MAX_TARGETS targets (any number of
+// sources): 3 x chunks x targets doubles, at most 605,184 (4.6 MiB) for the chunk
+// counts that td3_direct_sum chooses.
+namespace {
+
+constexpr i64 NOALLOC_SCRATCH_DOUBLES = 605184;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) double g_direct_scratch[NOALLOC_SCRATCH_DOUBLES];
+
+std::mutex g_scratch_mutex;
+double* g_scratch_address[NOALLOC_MAX_DEVICES] = {};
+
+// The device address of g_direct_scratch on the current device, looked up once per
+// device.  In host code the array's name is only a host-side stand-in, so the address
+// must come from cudaGetSymbolAddress with that device current.
+int noalloc_scratch(double** out) {
+    int dev = 0;
+    TD3_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return TD3_EINVAL;
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_address[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_direct_scratch);
+        if (e != cudaSuccess) return td3_cuda_error(e);
+        g_scratch_address[dev] = static_cast<double*>(p);
+    }
+    *out = g_scratch_address[dev];
+    return TD3_OK;
+}
+
+}  // namespace
+
+extern "C" int td3_direct_sum_noalloc(int kernel, const double* targets, int64_t m,
+                                      const int64_t* exclude, const double* pos,
+                                      const double* charge, int64_t n, double softening,
+                                      int with_potential, double* phi, double* field,
+                                      int64_t* status, void* stream) {
+    if (m < 0 || n < 0 || (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG))
+        return TD3_EINVAL;
+    if (m > TD3_DIRECT_NOALLOC_MAX_TARGETS) {
+        td3_set_error("td3_direct_sum_noalloc: more targets than its fixed scratch holds "
+                      "(TD3_DIRECT_NOALLOC_MAX_TARGETS); use td3_direct_sum with a workspace");
+        return TD3_ETOOLARGE;
+    }
+    double* scratch = nullptr;
+    TD3_TRY_RC(noalloc_scratch(&scratch));
+    cudaStream_t s = td3_stream(stream);
+    if (m == 0) return TD3_OK;
+    if (n == 0) {
+        TD3_TRY(cudaMemsetAsync(phi, 0, sizeof(double) * m, s));
+        TD3_TRY(cudaMemsetAsync(field, 0, sizeof(double) * 2 * m, s));
+        return TD3_OK;
+    }
+    int chunks = direct_chunks(m, n);
+    if (chunks > 1 && (i64)3 * chunks * m > NOALLOC_SCRATCH_DOUBLES) {
+        td3_set_error("td3_direct_sum_noalloc: the partial sums exceed the fixed scratch");
+        return TD3_ETOOLARGE;
+    }
+    // every partial slot the reduction reads is written by the chunk pass first, so
+    // the scratch needs no clearing between calls
+    double eps2 = softening * softening;
+    bool pot = with_potential != 0;
+    if (kernel == TD3_KERNEL_COULOMB)
+        return pot ? launch_direct<TD3_KERNEL_COULOMB, true>(targets, m, exclude, pos, charge, n, eps2,
+                                                              phi, field, status, scratch, chunks, s)
+                   : launch_direct<TD3_KERNEL_COULOMB, false>(targets, m, exclude, pos, charge, n,
+                                                               eps2, phi, field, status, scratch,
+                                                               chunks, s);
+    return pot ? launch_direct<TD3_KERNEL_LOG, true>(targets, m, exclude, pos, charge, n, eps2, phi,
+                                                      field, status, scratch, chunks, s)
+               : launch_direct<TD3_KERNEL_LOG, false>(targets, m, exclude, pos, charge, n, eps2, phi,
+                                                       field, status, scratch, chunks, s);
 }
