@@ -186,6 +186,17 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The largest of every rank's ``value`` (the job's time is its slowest rank's)."""
+    import torch
+
+    if dist is None:
+        return value
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def gpu_step(pos, q, torch):
     from tree_d_3d_b200 import FlatQuadtree, Quad
 
@@ -277,9 +288,7 @@ def run_ours(args):
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / args.steps
     value = world * n * args.steps / (total_ms / 1e3)
 
@@ -317,10 +326,7 @@ def run_ours(args):
         b.record(stream)
         b.synchronize()
         e2e_ms += a.elapsed_time(b)
-    if dist:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
     e2e_value = world * n * args.steps / (e2e_ms / 1e3)
 
     # launches of our kernels per step, and the dominant kernel's roofline

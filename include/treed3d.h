@@ -267,6 +267,31 @@ int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node
                      const int64_t* node_child, int order, const double* binomial,
                      int binomial_size, double* local_re, double* local_im, void* stream);
 
+/* ------------------------------------------------------------------ Coulomb FMM */
+
+/* M2L of the softened Coulomb kernel with Cartesian expansions, FP64: for every
+ * destination cell n and source cell partners[row_start[n]:row_start[n + 1]], the
+ * Taylor coefficients A_g(t) of (|r|^2 + eps^2)^(-1/2) at t = c_dst - c_src by the
+ * reference's recurrence, then local[n, b] += coef * m_a * A_{a+b} over the M2L rows
+ * (b, a, a + b) of _cartesian.tables (src/tree_d_3d/_cartesian.py:40-107): row_a,
+ * row_g (int32), row_coef, b_start (int32, n_coef + 1: first row of each b).  moments
+ * (src cells, n_coef), local (n_dst, n_coef).  Replaces cart_m2l_host
+ * (src/tree_d_3d/kernels/cart_m2l_host/cart_m2l_host_pyccel.py:16-80). */
+int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                 const double* dst_center, const double* src_center, const double* moments,
+                 int order, double softening, const int* row_a, const int* row_g,
+                 const double* row_coef, const int* b_start, double* local, void* stream);
+
+/* L2L of the Cartesian local expansions from the root down (levels HOST, n_levels + 1):
+ * T_b(child) += C(g, b) T_g s^(g - b) over the shift rows regrouped by b (l2l_start
+ * (n_coef + 1), l2l_g, l2l_d = g - b, l2l_coef; int32 indices), ex / ey the powers of
+ * each coefficient.  Replaces cart_downward (src/tree_d_3d/kernels/cart_downward/
+ * cart_downward_pyccel.py:14-55). */
+int td3_cart_downward(const int64_t* levels, int64_t n_levels, const double* node_center,
+                      const int64_t* node_child, int order, const int64_t* ex, const int64_t* ey,
+                      const int* l2l_start, const int* l2l_g, const int* l2l_d,
+                      const double* l2l_coef, double* local, void* stream);
+
 /* ------------------------------------------------------------------ near field */
 
 /* The work plan of the near field: every non-empty leaf's row of P2P partners

@@ -71,7 +71,21 @@ def tables(order: int) -> dict:
                 shift_rows.append((ig, index(bx, by), index(gx - bx, gy - by)))
                 shift_coef.append(float(comb(gx, bx) * comb(gy, by)))
         shift_start.append(len(shift_rows))
+    # L2L by output coefficient: the shift rows of each b, in g order
+    by_b = sorted(range(len(shift_rows)), key=lambda r: shift_rows[r][1])
+    l2l_start = np.zeros(n_coef + 1, dtype=np.int32)
+    for r in by_b:
+        l2l_start[shift_rows[r][1] + 1] += 1
+    l2l_start = np.cumsum(l2l_start).astype(np.int32)
+    m2l_arr = np.array(m2l_rows, dtype=np.int64)
     out = {
+        "m2l_a": m2l_arr[:, 1].astype(np.int32),
+        "m2l_g": m2l_arr[:, 2].astype(np.int32),
+        "m2l_start32": np.array(m2l_start, dtype=np.int32),
+        "l2l_start": l2l_start,
+        "l2l_g": np.array([shift_rows[r][0] for r in by_b], dtype=np.int32),
+        "l2l_d": np.array([shift_rows[r][2] for r in by_b], dtype=np.int32),
+        "l2l_coef": np.array([shift_coef[r] for r in by_b]),
         "ex": ex,
         "ey": ey,
         "mono_parent": mono_parent,

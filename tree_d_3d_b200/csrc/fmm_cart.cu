@@ -1,0 +1,148 @@
+// The FMM of the softened Coulomb kernel in the plane with Cartesian expansions, FP64:
+//   M2L by destination row  (K/cart_m2l_host/cart_m2l_host_pyccel.py:16-80)
+//   L2L per level           (K/cart_downward/cart_downward_pyccel.py:14-55)
+// (moments: moments.cu; L2P + P2P: nearfield.cu.)
+//
+// M2L: one warp per destination cell.  For each partner the warp builds the Taylor
+// coefficients A_g(t), |g| <= p, of f = (|r|^2 + eps^2)^(-1/2) degree by degree in
+// shared memory (the coefficients of one degree depend only on the two below), then
+// every lane accumulates its local coefficients b over the M2L rows (b, a, a + b) of
+// the reference's tables: T_b += coef * m_a * A_{a+b}.
+#include "common.cuh"
+
+namespace {
+
+constexpr int CM2L_WARPS = 4;
+
+__global__ void __launch_bounds__(32 * CM2L_WARPS)
+k_m2l_cart(const i64* __restrict__ row_start, const i64* __restrict__ partners, i64 n_dst,
+           const double* __restrict__ dst_center, const double* __restrict__ src_center,
+           const double* __restrict__ moments, int order, double eps2,
+           const int* __restrict__ row_a, const int* __restrict__ row_g,
+           const double* __restrict__ row_coef, const int* __restrict__ b_start,
+           double* __restrict__ local) {
+    extern __shared__ double smem[];
+    int n_coef = (order + 1) * (order + 2) / 2;
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    double* A = smem + (2 * wib) * n_coef;
+    double* M = A + n_coef;
+    constexpr int PER_LANE = 8;  // coefficients per lane held in registers
+    for (i64 dst = (i64)blockIdx.x * CM2L_WARPS + wib; dst < n_dst; dst += (i64)gridDim.x * CM2L_WARPS) {
+        i64 e0 = row_start[dst], e1 = row_start[dst + 1];
+        if (e0 == e1) continue;
+        double cx = dst_center[2 * dst], cy = dst_center[2 * dst + 1];
+        for (int b0 = 0; b0 < n_coef; b0 += 32 * PER_LANE) {
+            double acc[PER_LANE];
+#pragma unroll
+            for (int j = 0; j < PER_LANE; ++j) acc[j] = 0.0;
+            for (i64 e = e0; e < e1; ++e) {
+                i64 src = partners[e];
+                double tx = cx - src_center[2 * src], ty = cy - src_center[2 * src + 1];
+                double r2 = tx * tx + ty * ty + eps2;
+                for (int i = lane; i < n_coef; i += 32) M[i] = moments[src * n_coef + i];
+                if (lane == 0) A[0] = 1.0 / sqrt(r2);
+                __syncwarp();
+                for (int n = 1; n <= order; ++n) {
+                    int base = n * (n + 1) / 2;
+                    for (int b = lane; b <= n; b += 32) {
+                        int a = n - b;
+                        double s = 0.0;
+                        if (a >= 1) s += (2 * n - 1) * tx * A[(n - 1) * n / 2 + b];
+                        if (b >= 1) s += (2 * n - 1) * ty * A[(n - 1) * n / 2 + b - 1];
+                        if (a >= 2) s += (n - 1) * A[(n - 2) * (n - 1) / 2 + b];
+                        if (b >= 2) s += (n - 1) * A[(n - 2) * (n - 1) / 2 + b - 2];
+                        A[base + b] = -s / (n * r2);
+                    }
+                    __syncwarp();
+                }
+#pragma unroll
+                for (int j = 0; j < PER_LANE; ++j) {
+                    int b = b0 + lane + 32 * j;
+                    if (b < n_coef) {
+                        double t = 0.0;
+                        for (int r = b_start[b]; r < b_start[b + 1]; ++r)
+                            t += row_coef[r] * M[row_a[r]] * A[row_g[r]];
+                        acc[j] += t;
+                    }
+                }
+                __syncwarp();
+            }
+#pragma unroll
+            for (int j = 0; j < PER_LANE; ++j) {
+                int b = b0 + lane + 32 * j;
+                if (b < n_coef) local[dst * n_coef + b] += acc[j];
+            }
+        }
+    }
+}
+
+// L2L of one level: thread per (node, child, b): T_b(child) += sum_g C(g, b) T_g s^(g-b)
+// over the rows of b (g, d = g - b, coef), the monomial s^d built as the reference's mono
+// recurrence builds it (d_y factors of s_y, then d_x of s_x).
+__global__ void k_l2l_cart(i64 lo, i64 hi, int n_coef, const double* __restrict__ center,
+                           const i64* __restrict__ child, const i64* __restrict__ ex,
+                           const i64* __restrict__ ey, const int* __restrict__ l2l_start,
+                           const int* __restrict__ l2l_g, const int* __restrict__ l2l_d,
+                           const double* __restrict__ l2l_coef, double* __restrict__ local) {
+    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    i64 node = lo + t / (4 * n_coef);
+    if (node >= hi) return;
+    i64 first = child[node];
+    if (first < 0) return;
+    int c = (int)((t / n_coef) % 4), b = (int)(t % n_coef);
+    i64 ch = first + c;
+    double sx = center[2 * ch] - center[2 * node], sy = center[2 * ch + 1] - center[2 * node + 1];
+    double acc = 0.0;
+    for (int r = l2l_start[b]; r < l2l_start[b + 1]; ++r) {
+        int d = l2l_d[r];
+        double mono = 1.0;
+        for (int k = 0; k < (int)ey[d]; ++k) mono = mono * sy;
+        for (int k = 0; k < (int)ex[d]; ++k) mono = mono * sx;
+        acc += l2l_coef[r] * local[node * n_coef + l2l_g[r]] * mono;
+    }
+    local[ch * n_coef + b] += acc;
+}
+
+}  // namespace
+
+extern "C" int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                            const double* dst_center, const double* src_center,
+                            const double* moments, int order, double softening,
+                            const int* row_a, const int* row_g, const double* row_coef,
+                            const int* b_start, double* local, void* stream) {
+    if (n_dst < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (n_dst == 0) return TD3_OK;
+    cudaStream_t s = td3_stream(stream);
+    int n_coef = (order + 1) * (order + 2) / 2;
+    size_t smem = sizeof(double) * 2 * n_coef * CM2L_WARPS;
+    if (smem > 48 * 1024)
+        TD3_TRY(cudaFuncSetAttribute(k_m2l_cart, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    i64 blocks = (n_dst + CM2L_WARPS - 1) / CM2L_WARPS;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    k_m2l_cart<<<(unsigned)blocks, 32 * CM2L_WARPS, smem, s>>>(
+        row_start, partners, n_dst, dst_center, src_center, moments, order,
+        softening * softening, row_a, row_g, row_coef, b_start, local);
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_cart_downward(const int64_t* levels, int64_t n_levels, const double* node_center,
+                                 const int64_t* node_child, int order, const int64_t* ex,
+                                 const int64_t* ey, const int* l2l_start, const int* l2l_g,
+                                 const int* l2l_d, const double* l2l_coef, double* local,
+                                 void* stream) {
+    if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    int n_coef = (order + 1) * (order + 2) / 2;
+    for (i64 level = 0; level + 1 < n_levels; ++level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        i64 threads = (hi - lo) * 4 * n_coef;
+        k_l2l_cart<<<td3_blocks(threads, 256), 256, 0, s>>>(lo, hi, n_coef, node_center, node_child,
+                                                            ex, ey, l2l_start, l2l_g, l2l_d,
+                                                            l2l_coef, local);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}

@@ -377,7 +377,10 @@ class FlatQuadtree:
         t = _cartesian.tables(self.order)
         out = {}
         for name, value in t.items():
-            dtype = torch.float64 if value.dtype.kind == "f" else torch.int64
+            if value.dtype.kind == "f":
+                dtype = torch.float64
+            else:
+                dtype = torch.int32 if value.dtype == np.int32 else torch.int64
             out[name] = _device_table(("cart", self.order, name), lambda v=value: v, dev, dtype)
         return out
 
@@ -619,5 +622,155 @@ class FlatQuadtree:
             plan["partial"].data_ptr(), float(softening), 1 if potential else 0, phi.data_ptr(),
             field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
 
+    # ------------------------------------------------------------------ fmm_at
+    def _dual_lists(self, tree: "FlatQuadtree", theta: float) -> dict:
+        """ft:1086-1122: one-way M2L / P2P pairs (target cell, source cell) as rows by
+        target cell, and the near-field plan of the target leaves."""
+        dev = self.device
+        capacity = np.array([16, 8, 12]) * (tree.node_count + self.node_count) + 64
+        sizes = np.zeros(4, dtype=np.int64)
+        while True:
+            m2l = torch.empty((int(capacity[0]), 2), dtype=torch.int64, device=dev)
+            p2p = torch.empty((int(capacity[1]), 2), dtype=torch.int64, device=dev)
+            ws = _lib.workspace(_lib.query("td3_fmm_traverse_workspace_size", int(capacity[2])), dev)
+            rc = _lib.call(
+                "td3_dual_traverse", tree.node_center.data_ptr(), tree.node_half.data_ptr(),
+                tree.node_start.data_ptr(), tree.node_end.data_ptr(), tree.node_child.data_ptr(),
+                self.node_center.data_ptr(), self.node_half.data_ptr(), self.node_start.data_ptr(),
+                self.node_end.data_ptr(), self.node_child.data_ptr(), float(theta),
+                m2l.data_ptr(), int(capacity[0]), p2p.data_ptr(), int(capacity[1]),
+                int(capacity[2]), sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
+            if rc == _lib.OK:
+                break
+            capacity = np.maximum(2 * capacity, sizes[:3] + 64)
+        m2l, p2p = m2l[: sizes[0]].clone(), p2p[: sizes[1]].clone()
+        m2l_rows, m2l_partners = self._rows(m2l, mutual=False, n_nodes=tree.node_count)
+        p2p_rows, p2p_partners = self._rows(p2p, mutual=False, n_nodes=tree.node_count)
+        return {
+            "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
+            "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
+            "plan": _nearfield_plan(p2p_rows, tree),
+        }
+
+    def _target_plan(self, targets: torch.Tensor, theta: float, leaf: int):
+        """ft:1124-1149: the target tree and the dual lists, kept while the targets
+        stay the same (repeated sums at the same points)."""
+        key = ("targets", theta, leaf)
+        cached = self._plans.get(key)
+        if (cached is not None and cached[0].shape == targets.shape
+                and torch.equal(cached[0], targets)):
+            return cached[1], cached[2]
+        m = targets.shape[1]
+        lo = targets.amin(dim=1).tolist()
+        hi = targets.amax(dim=1).tolist()
+        centre = (0.5 * (lo[0] + hi[0]), 0.5 * (lo[1] + hi[1]))
+        half = 0.5 * max(hi[0] - lo[0], hi[1] - lo[1]) * (1 + 1e-12) + 1e-300
+        tree = FlatQuadtree(targets, torch.zeros(m, dtype=torch.float64, device=self.device),
+                            Quad(centre[0], centre[1], half), leaf_capacity=leaf,
+                            max_depth=self.max_depth, kernel="coulomb")
+        lists = self._dual_lists(tree, theta)
+        self._plans[key] = (targets.clone(), tree, lists)
+        return tree, lists
+
+    def fmm_at(self, targets, *, exclude=None, theta: float = 0.5, softening: float = 0.0,
+               potential: bool = True, leaf_capacity: int | None = None):
+        """Potential (M,) and field (2, M) at ``targets`` (2, M) by the FMM, without
+        ``k_e`` (ft:1151-1316): a tree of the targets (``leaf_capacity`` per leaf, by
+        default the sources'), a one-way dual traversal against the source tree, M2L
+        into the target cells, L2L down the target tree, L2P plus exact sums over the
+        partner source leaves (skipping source ``exclude[i]``).  On the GPU."""
+        theta = _finite("theta", theta, minimum=0)
+        if not 0 < theta < 1:
+            raise ValueError("FMM theta must lie in (0, 1)")
+        softening = _finite("softening", softening, minimum=0)
+        as_numpy = wants_numpy(targets)
+        targets = _points(targets, "targets")
+        if not bool(torch.isfinite(targets).all()):
+            raise ValueError("targets must be finite")
+        m, n, dev = targets.shape[1], self.pos.shape[1], self.device
+        phi = torch.zeros(m, dtype=torch.float64, device=dev)
+        field = torch.zeros((2, m), dtype=torch.float64, device=dev)
+        if not m or not n:
+            return out((phi, field), as_numpy)
+        if exclude is None:
+            exclude = torch.full((m,), -1, dtype=torch.int64, device=dev)
+        exclude = _device(exclude, torch.int64).reshape(-1)
+        leaf = self.leaf_capacity if leaf_capacity is None else int(leaf_capacity)
+        tree, lists = self._target_plan(targets, theta, leaf)
+        texclude = exclude[tree.perm].contiguous()
+        stream = _lib.stream(dev)
+        n_m2l = int(lists["m2l"].shape[0])
+        if self.kernel == "log":
+            w = self.order + 1
+            local_a = torch.zeros((tree.node_count, w), dtype=torch.float64, device=dev)
+            local_b = torch.zeros_like(local_a)
+            if n_m2l:
+                _lib.call("td3_fmm_m2l", lists["m2l_rows"].data_ptr(),
+                          lists["m2l_partners"].data_ptr(), tree.node_count,
+                          tree.node_center.data_ptr(), self.node_center.data_ptr(),
+                          self.moment_re.data_ptr(), self.moment_im.data_ptr(), self.order,
+                          self._m2l_matrix().data_ptr(), local_a.data_ptr(), local_b.data_ptr(),
+                          stream)
+            levels = np.ascontiguousarray(tree.levels, dtype=np.int64)
+            binom = self._binomial()
+            _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
+                      tree.node_center.data_ptr(), tree.node_child.data_ptr(), self.order,
+                      binom.data_ptr(), binom.shape[0], local_a.data_ptr(), local_b.data_ptr(),
+                      stream)
+            kernel, with_pot = _lib.KERNEL_LOG, potential
+        else:
+            local_a = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"], n_m2l, tree,
+                                        softening)
+            local_b = local_a
+            kernel, with_pot = _lib.KERNEL_COULOMB, True
+        plan = lists["plan"]
+        status = status_word(dev)
+        _lib.call(
+            "td3_fmm_targets", kernel, tree._sorted_pos.data_ptr(), texclude.data_ptr(),
+            tree.perm.data_ptr(), m, tree.node_center.data_ptr(), tree.node_start.data_ptr(),
+            tree.node_end.data_ptr(), self.order, local_a.data_ptr(), local_b.data_ptr(),
+            lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
+            plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
+            plan["partial"].data_ptr(), self._sorted_pos.data_ptr(),
+            self._sorted_charge.data_ptr(), self.perm.data_ptr(), n, self.node_start.data_ptr(),
+            self.node_end.data_ptr(), float(softening), 1 if with_pot else 0, phi.data_ptr(),
+            field.data_ptr(), status.data_ptr(), stream)
+        _check(status)
+        if not potential:
+            phi.zero_()
+        return out((phi, field), as_numpy)
+
+    def _cart_locals(self, rows, partners, n_m2l, dst, softening):
+        """Cartesian M2L from this tree's cells into the cells of ``dst`` (this tree for
+        fmm, the target tree for fmm_at), then L2L down ``dst`` (ft:1371-1396)."""
+        from tree_d_3d_b200 import _cartesian
+
+        t = self._cartesian_tables()
+        n_coef = _cartesian.size(self.order)
+        stream = _lib.stream(self.device)
+        local = torch.zeros((dst.node_count, n_coef), dtype=torch.float64, device=self.device)
+        if n_m2l:
+            _lib.call("td3_cart_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
+                      dst.node_center.data_ptr(), self.node_center.data_ptr(),
+                      self._cartesian_moments().data_ptr(), self.order, float(softening),
+                      t["m2l_a"].data_ptr(), t["m2l_g"].data_ptr(), t["m2l_coef"].data_ptr(),
+                      t["m2l_start32"].data_ptr(), local.data_ptr(), stream)
+        levels = np.ascontiguousarray(dst.levels, dtype=np.int64)
+        _lib.call("td3_cart_downward", levels.ctypes.data, len(levels) - 1,
+                  dst.node_center.data_ptr(), dst.node_child.data_ptr(), self.order,
+                  t["ex"].data_ptr(), t["ey"].data_ptr(), t["l2l_start"].data_ptr(),
+                  t["l2l_g"].data_ptr(), t["l2l_d"].data_ptr(), t["l2l_coef"].data_ptr(),
+                  local.data_ptr(), stream)
+        return local
+
     def _coulomb_fmm(self, theta, softening, phi, field):
-        raise NotImplementedError("the Coulomb FMM is not built yet")
+        """ft:1360-1428: the Coulomb FMM with Cartesian expansions (the potential is
+        always computed, as in the reference)."""
+        lists = self._lists(theta)
+        local = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"],
+                                  lists["m2l"].shape[0], self, softening)
+        status = status_word(self.device)
+        self._evaluate_near(lists, _lib.KERNEL_COULOMB, local, local, softening, True, phi,
+                            field, status)
+        _check(status)
+        self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
