@@ -348,6 +348,47 @@ int td3_fmm_targets(int kernel, const double* sorted_targets, const int64_t* sor
                     int with_potential, double* phi, double* field, int64_t* status,
                     void* stream);
 
+/* ------------------------------------------------------------------ adjoint (backward) */
+
+/* Multipole moments of the adjoint FMM pass: monopoles sorted_weight (n) and point
+ * dipoles sorted_dipole (2, n) at the particles (tree order).  Log kernel: a_n = sum
+ * [w (z - c)^n - n e (z - c)^(n-1)], e = ex + i ey (moment_re / moment_im, node_wabs =
+ * sum |w|); Cartesian: m_g = sum [w (r - c)^g - e . grad (r - c)^g] (tables as
+ * td3_cart_moments).  No reference counterpart (the reference has no backward). */
+int td3_log_moments_adjoint(const int64_t* levels, int64_t n_levels, int order,
+                            const double* sorted_pos, const double* sorted_weight,
+                            const double* sorted_dipole, int64_t n, const double* node_center,
+                            const int64_t* node_start, const int64_t* node_end,
+                            const int64_t* node_child, const double* binomial,
+                            int binomial_size, double* node_wabs, double* moment_re,
+                            double* moment_im, void* stream);
+int td3_cart_moments_adjoint(const int64_t* levels, int64_t n_levels, const double* sorted_pos,
+                             const double* sorted_weight, const double* sorted_dipole, int64_t n,
+                             const double* node_center, const int64_t* node_start,
+                             const int64_t* node_end, const int64_t* node_child,
+                             const int64_t* ex, const int64_t* ey, const int64_t* shift,
+                             const double* shift_coef, const int64_t* shift_start, int n_coef,
+                             double* moments, void* stream);
+
+/* Backward of the FMM field at the sources: for upstream gradients w = dL/dphi and
+ * e = dL/dE (sorted_weight (n), sorted_dipole (2, n) in tree order) and the forward
+ * field efield (2, n, input order), writes qbar = dL/dq (n) and xbar = dL/dx (2, n) in
+ * input order:  qbar_k = Psi(x_k),  xbar_k = -w_k E_k + q_k grad Psi(x_k) - M_k e_k,
+ * with Psi(y) = sum_j [w_j G(y - x_j) + e_j . grad G(y - x_j)] (j != k) and M_k =
+ * sum_j q_j Hess G(x_k - x_j).  Far parts come from the adjoint local expansions
+ * adj_a / adj_b (value and gradient) and the forward ones fwd_a / fwd_b (Hessian),
+ * near parts pair by pair over the near-field plan (softened kernel; kernel as in
+ * td3_fmm_evaluate).  partial: 6 * partial length doubles.  No reference counterpart. */
+int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_charge,
+                    const int64_t* perm, int64_t n, const double* node_center,
+                    const int64_t* node_start, const int64_t* node_end, int order,
+                    const double* fwd_a, const double* fwd_b, const double* adj_a,
+                    const double* adj_b, const int64_t* p2p_partners, const int* seg_leaf,
+                    const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
+                    double* partial, const double* sorted_weight, const double* sorted_dipole,
+                    const double* efield, double softening, double* qbar, double* xbar,
+                    void* stream);
+
 /* ------------------------------------------------------------------ utilities */
 
 /* Stable radix sort of (key, value) uint32 pairs by the low `bits` bits of the key.

@@ -60,14 +60,17 @@ __global__ void k_coulomb_moments(i64 lo, i64 hi, const double* __restrict__ spo
     node_s[3 * node + 2] = syy;
 }
 
-// One thread per (node, n), n = 0..order.
+// One thread per (node, n), n = 0..order.  sdip (2, n_particles; may be null) adds
+// point dipoles e = (ex, ey) at the particles: a_n -= n e (z - c)^(n - 1), the moments
+// of the adjoint (transposed) FMM pass, whose sources are monopoles and dipoles.
 __global__ void k_log_moments(i64 lo, i64 hi, int order, const double* __restrict__ spos,
                               const double* __restrict__ scharge, i64 n_particles,
                               const double* __restrict__ node_center,
                               const i64* __restrict__ node_start, const i64* __restrict__ node_end,
                               const i64* __restrict__ node_child,
                               const double* __restrict__ binomial, int bsize, double* node_qabs,
-                              double* moment_re, double* moment_im) {
+                              double* moment_re, double* moment_im,
+                              const double* __restrict__ sdip) {
     i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     int w = order + 1;
     i64 node = lo + t / w;
@@ -89,6 +92,18 @@ __global__ void k_log_moments(i64 lo, i64 hi, int order, const double* __restric
             }
             acc_re += pr;
             acc_im += pi;
+            if (sdip && n > 0) {
+                // - n e (z - c)^(n-1)
+                double er = sdip[k], ei = sdip[n_particles + k];
+                double zr = 1.0, zi = 0.0;
+                for (int m = 0; m < n - 1; ++m) {
+                    double nr = zr * dx - zi * dy;
+                    zi = zr * dy + zi * dx;
+                    zr = nr;
+                }
+                acc_re -= n * (er * zr - ei * zi);
+                acc_im -= n * (er * zi + ei * zr);
+            }
         }
     } else {
         double sh_re[TD3_MAX_ORDER + 1], sh_im[TD3_MAX_ORDER + 1];
@@ -136,7 +151,8 @@ __global__ void k_cart_moments(i64 lo, i64 hi, int n_coef, const double* __restr
                                const i64* __restrict__ node_child, const i64* __restrict__ ex,
                                const i64* __restrict__ ey, const i64* __restrict__ shift,
                                const double* __restrict__ shift_coef,
-                               const i64* __restrict__ shift_start, double* moments) {
+                               const i64* __restrict__ shift_start, double* moments,
+                               const double* __restrict__ sdip) {
     i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     i64 node = lo + t / n_coef;
     int g = (int)(t % n_coef);
@@ -146,8 +162,15 @@ __global__ void k_cart_moments(i64 lo, i64 hi, int n_coef, const double* __restr
     double acc = 0.0;
     i64 first = node_child[node];
     if (first < 0) {
-        for (i64 k = node_start[node]; k < node_end[node]; ++k)
-            acc += monomial(scharge[k], spos[k] - xmid, spos[n_particles + k] - ymid, ga, gb);
+        for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+            double ux = spos[k] - xmid, uy = spos[n_particles + k] - ymid;
+            acc += monomial(scharge[k], ux, uy, ga, gb);
+            if (sdip) {
+                // a point dipole p = -e: m_g += p . grad (r - c)^g
+                if (ga > 0) acc -= sdip[k] * ga * monomial(1.0, ux, uy, ga - 1, gb);
+                if (gb > 0) acc -= sdip[n_particles + k] * gb * monomial(1.0, ux, uy, ga, gb - 1);
+            }
+        }
     } else {
         for (i64 child = first; child < first + 4; ++child) {
             if (node_end[child] == node_start[child]) continue;
@@ -199,7 +222,30 @@ extern "C" int td3_log_moments(const int64_t* levels, int64_t n_levels, int orde
         i64 threads = (hi - lo) * (order + 1);
         k_log_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
             lo, hi, order, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
-            node_child, binomial, binomial_size, node_qabs, moment_re, moment_im);
+            node_child, binomial, binomial_size, node_qabs, moment_re, moment_im, nullptr);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_log_moments_adjoint(const int64_t* levels, int64_t n_levels, int order,
+                                       const double* sorted_pos, const double* sorted_weight,
+                                       const double* sorted_dipole, int64_t n,
+                                       const double* node_center, const int64_t* node_start,
+                                       const int64_t* node_end, const int64_t* node_child,
+                                       const double* binomial, int binomial_size,
+                                       double* node_wabs, double* moment_re, double* moment_im,
+                                       void* stream) {
+    if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER || binomial_size < order + 1)
+        return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        i64 threads = (hi - lo) * (order + 1);
+        k_log_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
+            lo, hi, order, sorted_pos, sorted_weight, n, node_center, node_start, node_end,
+            node_child, binomial, binomial_size, node_wabs, moment_re, moment_im, sorted_dipole);
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;
@@ -220,7 +266,30 @@ extern "C" int td3_cart_moments(const int64_t* levels, int64_t n_levels, const d
         i64 threads = (hi - lo) * n_coef;
         k_cart_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
             lo, hi, n_coef, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
-            node_child, ex, ey, shift, shift_coef, shift_start, moments);
+            node_child, ex, ey, shift, shift_coef, shift_start, moments, nullptr);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_cart_moments_adjoint(const int64_t* levels, int64_t n_levels,
+                                        const double* sorted_pos, const double* sorted_weight,
+                                        const double* sorted_dipole, int64_t n,
+                                        const double* node_center, const int64_t* node_start,
+                                        const int64_t* node_end, const int64_t* node_child,
+                                        const int64_t* ex, const int64_t* ey,
+                                        const int64_t* shift, const double* shift_coef,
+                                        const int64_t* shift_start, int n_coef, double* moments,
+                                        void* stream) {
+    if (n_levels < 1 || n_coef < 1) return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        i64 threads = (hi - lo) * n_coef;
+        k_cart_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
+            lo, hi, n_coef, sorted_pos, sorted_weight, n, node_center, node_start, node_end,
+            node_child, ex, ey, shift, shift_coef, shift_start, moments, sorted_dipole);
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;

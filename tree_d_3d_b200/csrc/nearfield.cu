@@ -116,6 +116,64 @@ __device__ __forceinline__ void eval_local(const double* __restrict__ local_a,
         l2p_cart(local_a + leaf * width, order, ux, uy, phi, fx, fy);
 }
 
+// Value, gradient and Hessian of the potential of a local expansion at u = r - c:
+// log kernel phi = -2 Re W (W = sum b_l u^l), Coulomb phi = sum T_(a,b) ux^a uy^b.
+struct LocalJet {
+    double v, gx, gy, hxx, hxy, hyy;
+};
+
+__device__ __forceinline__ LocalJet jet_complex(const double* __restrict__ lre,
+                                                const double* __restrict__ lim, int order,
+                                                double ux, double uy) {
+    double wr = lre[order], wi = lim[order], d1r = 0.0, d1i = 0.0, d2r = 0.0, d2i = 0.0;
+    for (int l = order - 1; l >= 0; --l) {
+        double t;
+        t = d2r * ux - d2i * uy + d1r;
+        d2i = d2r * uy + d2i * ux + d1i;
+        d2r = t;
+        t = d1r * ux - d1i * uy + wr;
+        d1i = d1r * uy + d1i * ux + wi;
+        d1r = t;
+        t = wr * ux - wi * uy + lre[l];
+        wi = wr * uy + wi * ux + lim[l];
+        wr = t;
+    }
+    // W'' = 2 d2
+    return {-2.0 * wr, -2.0 * d1r, 2.0 * d1i, -4.0 * d2r, 4.0 * d2i, 4.0 * d2r};
+}
+
+__device__ __forceinline__ LocalJet jet_cart(const double* __restrict__ T, int order, double ux,
+                                             double uy) {
+    // outer Horner in uy over P_b(ux) and its x-derivatives, inner Horner in ux
+    double q = 0.0, qy = 0.0, qyy = 0.0, gx = 0.0, gxy = 0.0, k = 0.0;
+    for (int b = order; b >= 0; --b) {
+        int top = order - b;
+        int n = top + b;
+        double p = T[n * (n + 1) / 2 + b], p1 = 0.0, p2 = 0.0;
+        for (int a = top - 1; a >= 0; --a) {
+            n = a + b;
+            p2 = p2 * ux + p1;
+            p1 = p1 * ux + p;
+            p = p * ux + T[n * (n + 1) / 2 + b];
+        }
+        qyy = qyy * uy + qy;
+        qy = qy * uy + q;
+        q = q * uy + p;
+        gxy = gxy * uy + gx;
+        gx = gx * uy + p1;
+        k = k * uy + 2.0 * p2;
+    }
+    return {q, gx, qy, k, gxy, 2.0 * qyy};
+}
+
+template <int LOCAL>
+__device__ __forceinline__ LocalJet local_jet(const double* __restrict__ la,
+                                              const double* __restrict__ lb, i64 leaf, int order,
+                                              int width, double ux, double uy) {
+    if (LOCAL == LOCAL_COMPLEX) return jet_complex(la + leaf * width, lb + leaf * width, order, ux, uy);
+    return jet_cart(la + leaf * width, order, ux, uy);
+}
+
 struct Sources {
     const double* pos;     // (2, n) tree order
     const double* charge;  // (n) tree order
@@ -263,6 +321,157 @@ __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_
     }
 }
 
+// ------------------------------------------------------------------ adjoint pass
+// Backward of (phi, E) at the sources for upstream gradients (w = dL/dphi, e = dL/dE):
+//   dL/dq_k = Psi(x_k),  dL/dx_k = -w_k E_k + q_k grad Psi(x_k) - M_k e_k,
+// Psi(y) = sum_j [w_j G(y - x_j) + e_j . grad G(y - x_j)] (monopoles w and dipoles e at
+// the sources, j != k), M_k = sum_j q_j Hess G(x_k - x_j) (the Hessian of the forward
+// potential).  Near parts are summed here pair by pair; the far parts come from the
+// adjoint pass's local expansion (value and gradient) and the forward one (Hessian).
+struct Adjoint {
+    const double* weight;  // (n) w in tree order
+    const double* dipole;  // (2, n) e in tree order
+    const double* efield;  // (2, n) forward E, input order
+    double* qbar;          // (n) input order
+    double* xbar;          // (2, n) input order
+};
+
+template <int KERNEL>
+__device__ __forceinline__ void adjoint_pair(double dx, double dy, double eps2, double qj,
+                                             double wj, double exj, double eyj, double* acc) {
+    double s = dx * dx + dy * dy + eps2;
+    double de = exj * dx + eyj * dy;
+    if (KERNEL == TD3_KERNEL_LOG) {
+        // G = -ln s, grad G = -2 d / s, Hess G = -2 I / s + 4 d d^T / s^2
+        double inv = 1.0 / s;
+        double lg = log(s);
+        acc[0] += -wj * lg - 2.0 * de * inv;
+        double t = 4.0 * de * inv * inv;
+        acc[1] += -2.0 * inv * (wj * dx + exj) + t * dx;
+        acc[2] += -2.0 * inv * (wj * dy + eyj) + t * dy;
+        double q4 = 4.0 * qj * inv * inv;
+        acc[3] += -2.0 * qj * inv + q4 * dx * dx;
+        acc[4] += q4 * dx * dy;
+        acc[5] += -2.0 * qj * inv + q4 * dy * dy;
+    } else {
+        // G = s^(-1/2), grad G = -d s^(-3/2), Hess G = -I s^(-3/2) + 3 d d^T s^(-5/2)
+        double r = rsqrt(s);
+        double r3 = r * r * r;
+        double r5 = r3 * r * r;
+        acc[0] += wj * r - de * r3;
+        double t = 3.0 * de * r5;
+        acc[1] += -r3 * (wj * dx + exj) + t * dx;
+        acc[2] += -r3 * (wj * dy + eyj) + t * dy;
+        double q3 = 3.0 * qj * r5;
+        acc[3] += -qj * r3 + q3 * dx * dx;
+        acc[4] += q3 * dx * dy;
+        acc[5] += -qj * r3 + q3 * dy * dy;
+    }
+}
+
+template <int LOCAL>
+__device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, i64 n,
+                                               double ux, double uy, i64 leaf, int order,
+                                               int width, const double* fa, const double* fb,
+                                               const double* ba, const double* bb,
+                                               const Sources& S, const Adjoint& A) {
+    LocalJet f = local_jet<LOCAL>(fa, fb, leaf, order, width, ux, uy);  // forward: Hessian
+    LocalJet b = local_jet<LOCAL>(ba, bb, leaf, order, width, ux, uy);  // adjoint: Psi
+    double psi = acc[0] + b.v;
+    double gx = acc[1] + b.gx, gy = acc[2] + b.gy;
+    double mxx = acc[3] + f.hxx, mxy = acc[4] + f.hxy, myy = acc[5] + f.hyy;
+    double q = S.charge[k], w = A.weight[k], ex = A.dipole[k], ey = A.dipole[n + k];
+    A.qbar[i] = psi;
+    A.xbar[i] = -w * A.efield[i] + q * gx - (mxx * ex + mxy * ey);
+    A.xbar[n + i] = -w * A.efield[n + i] + q * gy - (mxy * ex + myy * ey);
+}
+
+template <int KERNEL, int LOCAL>
+__global__ void __launch_bounds__(32 * NF_WARPS)
+k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
+               const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
+               const i64* __restrict__ partners, const double* __restrict__ fa,
+               const double* __restrict__ fb, const double* __restrict__ ba,
+               const double* __restrict__ bb, int order, int width, double eps2,
+               double* __restrict__ partial) {
+    int lane = threadIdx.x & 31;
+    i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    if (seg >= n_seg) return;
+    i64 leaf = seg_leaf[seg];
+    longlong2 er = seg_range[seg];
+    i64 outp = seg_out[seg];
+    i64 s0 = T.start[leaf];
+    int count = (int)(T.end[leaf] - s0);
+    int tsz = pow2_at_least(count < 32 ? count : 32);
+    int slices = 32 / tsz;
+    int ti = lane % tsz, slice = lane / tsz;
+    i64 n = S.n;
+    for (int base = 0; base < count; base += tsz) {
+        int it = base + ti;
+        bool valid = it < count;
+        i64 k = s0 + (valid ? it : 0);
+        double xi = S.pos[k], yi = S.pos[n + k];
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        if (valid) {
+            for (i64 e = er.x + slice; e < er.y; e += slices) {
+                i64 b = partners[e];
+                i64 b1 = S.end[b];
+                for (i64 j = S.start[b]; j < b1; ++j) {
+                    if (j == k) continue;
+                    double dx = xi - S.pos[j], dy = yi - S.pos[n + j];
+                    if (dx * dx + dy * dy + eps2 == 0.0) continue;
+                    adjoint_pair<KERNEL>(dx, dy, eps2, S.charge[j], A.weight[j], A.dipole[j],
+                                         A.dipole[n + j], acc);
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 6; ++c)
+            for (int off = tsz; off < 32; off <<= 1)
+                acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+        if (valid && slice == 0) {
+            if (outp < 0) {
+                adjoint_finish<LOCAL>(acc, k, T.perm[k], n, xi - T.center[2 * leaf],
+                                      yi - T.center[2 * leaf + 1], leaf, order, width, fa, fb, ba,
+                                      bb, S, A);
+            } else {
+                i64 p = outp + it;
+                for (int c = 0; c < 6; ++c) partial[6 * p + c] = acc[c];
+            }
+        }
+    }
+}
+
+template <int LOCAL>
+__global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg,
+                                      const int* __restrict__ seg_leaf,
+                                      const i64* __restrict__ seg_out, const double* __restrict__ fa,
+                                      const double* __restrict__ fb, const double* __restrict__ ba,
+                                      const double* __restrict__ bb, int order, int width,
+                                      const double* __restrict__ partial) {
+    i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    int lane = threadIdx.x & 31;
+    if (seg >= n_seg) return;
+    i64 p0 = seg_out[seg];
+    if (p0 < 0 || (seg > 0 && seg_leaf[seg - 1] == seg_leaf[seg])) return;
+    i64 leaf = seg_leaf[seg];
+    i64 s0 = T.start[leaf];
+    int count = (int)(T.end[leaf] - s0);
+    i64 last = seg;
+    while (last + 1 < n_seg && seg_leaf[last + 1] == leaf) ++last;
+    for (int it = lane; it < count; it += 32) {
+        double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (i64 s = seg; s <= last; ++s) {
+            i64 p = seg_out[s] + it;
+            for (int c = 0; c < 6; ++c) acc[c] += partial[6 * p + c];
+        }
+        i64 k = s0 + it;
+        adjoint_finish<LOCAL>(acc, k, T.perm[k], S.n, S.pos[k] - T.center[2 * leaf],
+                              S.pos[S.n + k] - T.center[2 * leaf + 1], leaf, order, width, fa, fb,
+                              ba, bb, S, A);
+    }
+}
+
 template <int KERNEL, bool POT, bool OTHER, int LOCAL>
 int launch_near(const Targets& T, const Sources& S, i64 n_seg, const int* seg_leaf,
                 const longlong2* seg_range, const i64* seg_out, const i64* partners,
@@ -374,6 +583,45 @@ extern "C" int td3_fmm_evaluate(int kernel, const double* sorted_pos, const doub
                                             seg_out, p2p_partners, local_a, local_b, order,
                                             (order + 1) * (order + 2) / 2, eps2, partial, phi, field,
                                             status, s);
+}
+
+extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_charge,
+                               const int64_t* perm, int64_t n, const double* node_center,
+                               const int64_t* node_start, const int64_t* node_end, int order,
+                               const double* fwd_a, const double* fwd_b, const double* adj_a,
+                               const double* adj_b, const int64_t* p2p_partners,
+                               const int* seg_leaf, const int64_t* seg_range,
+                               const int64_t* seg_out, int64_t n_seg, double* partial,
+                               const double* sorted_weight, const double* sorted_dipole,
+                               const double* efield, double softening, double* qbar,
+                               double* xbar, void* stream) {
+    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
+    if (n == 0 || n_seg == 0) return TD3_OK;
+    Targets T{sorted_pos, nullptr, perm, node_center, node_start, node_end, n};
+    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n};
+    Adjoint A{sorted_weight, sorted_dipole, efield, qbar, xbar};
+    double eps2 = softening * softening;
+    cudaStream_t s = td3_stream(stream);
+    const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
+    unsigned blocks = td3_blocks(n_seg, NF_WARPS);
+    if (kernel == TD3_KERNEL_LOG) {
+        int width = order + 1;
+        k_near_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX><<<blocks, 32 * NF_WARPS, 0, s>>>(
+            T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b, order,
+            width, eps2, partial);
+        k_near_adjoint_finish<LOCAL_COMPLEX><<<blocks, 32 * NF_WARPS, 0, s>>>(
+            T, S, A, n_seg, seg_leaf, seg_out, fwd_a, fwd_b, adj_a, adj_b, order, width, partial);
+    } else {
+        int width = (order + 1) * (order + 2) / 2;
+        k_near_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART><<<blocks, 32 * NF_WARPS, 0, s>>>(
+            T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b, order,
+            width, eps2, partial);
+        k_near_adjoint_finish<LOCAL_CART><<<blocks, 32 * NF_WARPS, 0, s>>>(
+            T, S, A, n_seg, seg_leaf, seg_out, fwd_a, fwd_b, adj_a, adj_b, order, width, partial);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
 }
 
 extern "C" int td3_fmm_targets(int kernel, const double* sorted_targets,

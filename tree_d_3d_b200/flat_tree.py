@@ -192,7 +192,7 @@ def _nearfield_plan(rows: torch.Tensor, tree) -> dict:
     n_seg = int(sizes[0])
     return {
         "seg_leaf": seg_leaf[:n_seg], "seg_range": seg_range[:n_seg], "seg_out": seg_out[:n_seg],
-        "n_seg": n_seg,
+        "n_seg": n_seg, "partial_len": int(sizes[1]),
         "partial": torch.empty(3 * max(int(sizes[1]), 1), dtype=torch.float64, device=dev),
     }
 
@@ -588,16 +588,18 @@ class FlatQuadtree:
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
         return out((phi, field), self._numpy)
 
-    def _log_locals(self, lists: dict):
-        """M2L into every cell's local expansion, then L2L down the tree."""
+    def _log_locals(self, lists: dict, moments=None):
+        """M2L into every cell's local expansion, then L2L down the tree (``moments``:
+        (moment_re, moment_im), by default the tree's own)."""
         dev, count, w = self.device, self.node_count, self.order + 1
+        mre, mim = moments if moments is not None else (self.moment_re, self.moment_im)
         local_re = torch.zeros((count, w), dtype=torch.float64, device=dev)
         local_im = torch.zeros((count, w), dtype=torch.float64, device=dev)
         stream = _lib.stream(dev)
         if lists["m2l"].shape[0]:
             _lib.call("td3_fmm_m2l", lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(),
                       count, self.node_center.data_ptr(), self.node_center.data_ptr(),
-                      self.moment_re.data_ptr(), self.moment_im.data_ptr(), self.order,
+                      mre.data_ptr(), mim.data_ptr(), self.order,
                       self._m2l_matrix().data_ptr(), local_re.data_ptr(), local_im.data_ptr(),
                       stream)
         levels = np.ascontiguousarray(self.levels, dtype=np.int64)
@@ -621,6 +623,88 @@ class FlatQuadtree:
             plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
             plan["partial"].data_ptr(), float(softening), 1 if potential else 0, phi.data_ptr(),
             field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
+
+    # ------------------------------------------------------------------ backward
+    def _fmm_adjoint(self, theta: float, softening: float, weight: torch.Tensor,
+                     dipole: torch.Tensor, efield: torch.Tensor):
+        """The backward of ``fmm`` at the sources: for upstream gradients ``weight`` =
+        dL/dphi (N,) and ``dipole`` = dL/dE (2, N), and the forward field ``efield``,
+        returns (dL/dq (N,), dL/dx (2, N)) by one adjoint FMM pass (monopole + dipole
+        sources) plus the Hessian of the forward expansions."""
+        from tree_d_3d_b200 import _cartesian
+
+        lists = self._lists(theta)
+        n, dev, count = self.pos.shape[1], self.device, self.node_count
+        sw = weight.to(torch.float64)[self.perm].contiguous()
+        sd = dipole.to(torch.float64)[:, self.perm].contiguous()
+        efield = efield.to(torch.float64).contiguous()
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        stream = _lib.stream(dev)
+        if self.kernel == "log":
+            w = self.order + 1
+            fwd_a, fwd_b = self._log_locals(lists)
+            mre = torch.empty((count, w), dtype=torch.float64, device=dev)
+            mim = torch.empty_like(mre)
+            wabs = torch.empty(count, dtype=torch.float64, device=dev)
+            binom = self._binomial()
+            _lib.call("td3_log_moments_adjoint", levels.ctypes.data, len(levels) - 1, self.order,
+                      self._sorted_pos.data_ptr(), sw.data_ptr(), sd.data_ptr(), n,
+                      self.node_center.data_ptr(), self.node_start.data_ptr(),
+                      self.node_end.data_ptr(), self.node_child.data_ptr(), binom.data_ptr(),
+                      binom.shape[0], wabs.data_ptr(), mre.data_ptr(), mim.data_ptr(), stream)
+            adj_a, adj_b = self._log_locals(lists, moments=(mre, mim))
+            kernel = _lib.KERNEL_LOG
+        else:
+            t = self._cartesian_tables()
+            n_coef = _cartesian.size(self.order)
+            n_m2l = lists["m2l"].shape[0]
+            fwd_a = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"], n_m2l, self,
+                                      softening)
+            moments = torch.empty((count, n_coef), dtype=torch.float64, device=dev)
+            _lib.call("td3_cart_moments_adjoint", levels.ctypes.data, len(levels) - 1,
+                      self._sorted_pos.data_ptr(), sw.data_ptr(), sd.data_ptr(), n,
+                      self.node_center.data_ptr(), self.node_start.data_ptr(),
+                      self.node_end.data_ptr(), self.node_child.data_ptr(), t["ex"].data_ptr(),
+                      t["ey"].data_ptr(), t["shift"].data_ptr(), t["shift_coef"].data_ptr(),
+                      t["shift_start"].data_ptr(), n_coef, moments.data_ptr(), stream)
+            adj_a = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"], n_m2l, self,
+                                      softening, moments=moments)
+            fwd_b, adj_b = fwd_a, adj_a
+            kernel = _lib.KERNEL_COULOMB
+        plan = lists["plan"]
+        partial = torch.empty(6 * max(plan["partial_len"], 1), dtype=torch.float64, device=dev)
+        qbar = torch.zeros(n, dtype=torch.float64, device=dev)
+        xbar = torch.zeros((2, n), dtype=torch.float64, device=dev)
+        _lib.call("td3_fmm_adjoint", kernel, self._sorted_pos.data_ptr(),
+                  self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
+                  self.node_center.data_ptr(), self.node_start.data_ptr(), self.node_end.data_ptr(),
+                  self.order, fwd_a.data_ptr(), fwd_b.data_ptr(), adj_a.data_ptr(),
+                  adj_b.data_ptr(), lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
+                  plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
+                  partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), efield.data_ptr(),
+                  float(softening), qbar.data_ptr(), xbar.data_ptr(), stream)
+        return qbar, xbar
+
+    def _move_within_cells(self, positions) -> None:
+        """New positions for the same particles in the same cells (the tree's topology
+        and interaction lists stay): for derivatives of the expansions at fixed
+        topology.  Raises if a particle leaves its leaf."""
+        positions = _points(positions, "positions")
+        sorted_pos = positions[:, self.perm].contiguous()
+        # the non-empty leaves tile the slots 0..N-1 in the order of their starts
+        leaves = torch.nonzero((self.node_child < 0) & (self.node_end > self.node_start)).flatten()
+        leaves = leaves[torch.argsort(self.node_start[leaves])]
+        leaf_of = torch.repeat_interleave(leaves, (self.node_end - self.node_start)[leaves])
+        c = self.node_center[leaf_of]
+        h = self.node_half[leaf_of]
+        inside = (sorted_pos[0] >= c[:, 0] - h) & (sorted_pos[0] <= c[:, 0] + h) & \
+                 (sorted_pos[1] >= c[:, 1] - h) & (sorted_pos[1] <= c[:, 1] + h)
+        if not bool(inside.all()):
+            raise ValueError("a particle left its cell; rebuild the tree")
+        self.pos = positions.clone()
+        self._sorted_pos = sorted_pos
+        self._cart_moments = None
+        self._moments()
 
     # ------------------------------------------------------------------ fmm_at
     def _dual_lists(self, tree: "FlatQuadtree", theta: float) -> dict:
@@ -740,7 +824,7 @@ class FlatQuadtree:
             phi.zero_()
         return out((phi, field), as_numpy)
 
-    def _cart_locals(self, rows, partners, n_m2l, dst, softening):
+    def _cart_locals(self, rows, partners, n_m2l, dst, softening, moments=None):
         """Cartesian M2L from this tree's cells into the cells of ``dst`` (this tree for
         fmm, the target tree for fmm_at), then L2L down ``dst`` (ft:1371-1396)."""
         from tree_d_3d_b200 import _cartesian
@@ -748,11 +832,13 @@ class FlatQuadtree:
         t = self._cartesian_tables()
         n_coef = _cartesian.size(self.order)
         stream = _lib.stream(self.device)
+        if moments is None:
+            moments = self._cartesian_moments()
         local = torch.zeros((dst.node_count, n_coef), dtype=torch.float64, device=self.device)
         if n_m2l:
             _lib.call("td3_cart_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                       dst.node_center.data_ptr(), self.node_center.data_ptr(),
-                      self._cartesian_moments().data_ptr(), self.order, float(softening),
+                      moments.data_ptr(), self.order, float(softening),
                       t["m2l_a"].data_ptr(), t["m2l_g"].data_ptr(), t["m2l_coef"].data_ptr(),
                       t["m2l_start32"].data_ptr(), local.data_ptr(), stream)
         levels = np.ascontiguousarray(dst.levels, dtype=np.int64)
