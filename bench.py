@@ -1,18 +1,24 @@
-"""Benchmark of the field solver: FMM particles/s at N = 1M, p = 12 on one B200.
+"""Benchmark of the field solver: FMM particles/s at N = 1M, p = 12, mixed precision vs
+FP64, field plus backward, on one B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-A step is one FMM field evaluation of a fresh tree of the workload: the tree build
-with its moments, the traversal and interaction lists, M2L, L2L, and L2P + P2P at all
-N particles (log kernel, order 12, theta 0.5, leaf 8, softening 1e-3), on the 1M
-8-Gaussian mixture with +-1 charges of net zero (synthetic, seeded).  ``value`` is
-whole-job particles/s with the inputs resident in HBM; ``e2e`` is the same through the
-public API from pinned host buffers, host-device copies inside the timed region.
+A step takes the 1M particles of the workload (8-Gaussian mixture, +-1 charges of net
+zero; log kernel, order 12, theta 0.5, leaf 8, softening 1e-3), builds a fresh tree
+(build, moments, traversal, interaction lists) and evaluates the FMM potential and
+field at every particle in mixed precision (FP32 near field with compensated sums,
+FP32 M2L on size-scaled expansions, FP64 M2M / L2L / L2P), then runs the hand-written
+backward of L = sum w phi + sum e . E (fixed seeded w, e) to dL/dq and dL/dx.
+``value`` is whole-job particles/s with the inputs resident in HBM; the same step in
+the plain FP64 form is timed beside it (``fp64``), and the mixed field error against
+the FP64 direct sum on 4096 sampled particles is reported (``rel_err_field``).
+``e2e`` is the mixed step through the public API from pinned host buffers, with the
+host-device copies of its inputs and results inside the timed region.
 
 ``--impl reference`` times the reference algorithm on the host cores: the C
-restatement of the reference's CPU kernels (``oracle/``) with OpenMP on every core,
-on a bounded sample of the same workload.  Under torchrun with N > 1 every rank runs
-an independent replica (the path needs no exchange on one tree); rank 0 prints.
+restatement of the reference's CPU kernels (``oracle/``) with OpenMP on every core
+(field only: the reference has no backward), on a bounded sample of the workload.
+Under torchrun with N > 1 every rank runs an independent replica; rank 0 prints.
 """
 
 from __future__ import annotations
@@ -38,7 +44,11 @@ SOFTENING = 1e-3
 SEED = 3
 CPU_SAMPLE = 250_000
 L2_FLUSH_BYTES = 256 << 20
-WORKLOAD = "log-kernel FMM, 1M particles, 8-Gaussian mixture, p=12, theta=0.5, leaf 8"
+METRIC = "FMM particles/s at N=1M p=12: mixed-prec vs FP64 GPU at rel err<=1e-6, +backward"
+WORKLOAD = ("log-kernel FMM field + backward, 1M particles, 8-Gaussian mixture, p=12, "
+            "theta=0.5, leaf 8, fresh tree per step")
+FP32_PEAK = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA lanes x 2 flop x max SM clock
+FP64_PEAK = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 def _args():
@@ -50,7 +60,7 @@ def _args():
     p.add_argument("--n", type=int, default=N_PARTICLES)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--trace-only", action="store_true",
-                   help="timed steps only (no e2e, launch count or kernel timing): for ncu")
+                   help="timed mixed steps only (no e2e, FP64 arm, counts or errors): for ncu")
     return p.parse_args()
 
 
@@ -64,6 +74,7 @@ def _config(n):
         "leaf_capacity": LEAF,
         "softening": SOFTENING,
         "distribution": "mixture of 8 Gaussians (sigma 0.02-0.2), charges +-1, net zero",
+        "loss": "L = sum w phi + sum e.E, w and e seeded N(0, 1)",
         "l2": "flushed before every step (256 MiB write, outside the step's events)",
     }
 
@@ -80,7 +91,7 @@ def _cpu_fmm(pos, q):
 
 def cpu_baseline(repeats=2):
     """The oracle (C restatement of the reference's CPU kernels, OpenMP on all cores)
-    on a bounded sample of the workload; particles/s."""
+    on a bounded sample of the workload, field only; particles/s."""
     from oracle import flat_tree_oracle as oracle
     from tree_d_3d_b200 import synthetic
 
@@ -94,7 +105,8 @@ def cpu_baseline(repeats=2):
         "unit": "particles/s",
         "cores": cores,
         "kind": "port",
-        "sample": f"{CPU_SAMPLE} particles of the same distribution, build + FMM per run, best of {repeats}",
+        "sample": (f"{CPU_SAMPLE} particles of the workload's distribution, tree build + "
+                   f"FP64 FMM field (the reference has no backward), best of {repeats}"),
     }
 
 
@@ -113,9 +125,11 @@ def run_reference(args):
     times = [_cpu_fmm(pos, q) for _ in range(args.steps)]
     total = sum(times)
     value = CPU_SAMPLE * args.steps / total
+    sample = (f"{CPU_SAMPLE} particles of the workload's distribution per step, tree build + "
+              "FP64 FMM field (the reference has no backward)")
     line = {
         "impl": "reference",
-        "metric": "FMM particles/s at N=1M p=12",
+        "metric": METRIC,
         "value": value,
         "unit": "particles/s",
         "n_gpus": args.gpus,
@@ -129,7 +143,7 @@ def run_reference(args):
         "data": "synthetic",
         "config": _config(N_PARTICLES),
         "cpu_baseline": {"value": value, "unit": "particles/s", "cores": cores, "kind": "port",
-                         "sample": f"{CPU_SAMPLE} particles of the workload's distribution per step"},
+                         "sample": sample},
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -197,12 +211,32 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
-def gpu_step(pos, q, torch):
-    from tree_d_3d_b200 import FlatQuadtree, Quad
+def gpu_step(pos, q, w, e, precision, backward=True):
+    """One step: a fresh tree, the FMM field at every particle and its backward."""
+    from tree_d_3d_b200 import Quad
+    from tree_d_3d_b200.autograd import fmm_field
 
-    tree = FlatQuadtree(pos, q, Quad(0.0, 0.0, 1.0), kernel="log", order=ORDER, leaf_capacity=LEAF)
-    phi, field = tree.fmm(theta=THETA, softening=SOFTENING)
-    return tree, phi, field
+    p = pos.detach().requires_grad_(backward)
+    c = q.detach().requires_grad_(backward)
+    phi, field = fmm_field(p, c, Quad(0.0, 0.0, 1.0), kernel="log", order=ORDER, theta=THETA,
+                           softening=SOFTENING, leaf_capacity=LEAF, precision=precision)
+    if backward:
+        ((w * phi).sum() + (e * field).sum()).backward()
+    return phi, field, p.grad, c.grad
+
+
+def time_steps(fn, steps, flush, torch):
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for _ in range(steps):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    return total
 
 
 def count_our_launches(fn, torch):
@@ -221,28 +255,48 @@ def count_our_launches(fn, torch):
     return counts
 
 
-def time_m2l(tree, torch, reps):
-    """The M2L kernel alone (CUDA events on its stream), average ms per launch."""
+def time_m2l_mixed(tree, torch, reps):
+    """The mixed M2L kernel alone (CUDA events on its stream), average ms per launch."""
     from tree_d_3d_b200 import _lib
+    from tree_d_3d_b200.flat_tree import _m2l_coefficients
 
     lists = tree._lists(THETA)
     count, w = tree.node_count, tree.order + 1
     lre = torch.zeros((count, w), dtype=torch.float64, device=tree.device)
     lim = torch.zeros_like(lre)
+    hat = torch.empty((count, w, 2), dtype=torch.float32, device=tree.device)
+    stream = _lib.stream(tree.device)
+    _lib.call("td3_scale_moments", count, tree.order, tree.moment_re.data_ptr(),
+              tree.moment_im.data_ptr(), tree.node_half.data_ptr(), hat.data_ptr(), stream)
+    coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
     args = (lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(), count,
-            tree.node_center.data_ptr(), tree.node_center.data_ptr(), tree.moment_re.data_ptr(),
-            tree.moment_im.data_ptr(), tree.order, tree._m2l_matrix().data_ptr(),
-            lre.data_ptr(), lim.data_ptr(), _lib.stream(tree.device))
-    _lib.call("td3_fmm_m2l", *args)
-    stream = torch.cuda.current_stream()
+            tree.node_center.data_ptr(), tree.node_half.data_ptr(), tree.node_center.data_ptr(),
+            tree.node_half.data_ptr(), hat.data_ptr(), tree.order, coeff.ctypes.data,
+            lre.data_ptr(), lim.data_ptr(), stream)
+    _lib.call("td3_fmm_m2l_mixed", *args)
+    cur = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
-    start.record(stream)
+    start.record(cur)
     for _ in range(reps):
-        _lib.call("td3_fmm_m2l", *args)
-    stop.record(stream)
+        _lib.call("td3_fmm_m2l_mixed", *args)
+    stop.record(cur)
     torch.cuda.synchronize()
     return start.elapsed_time(stop) / reps, int(lists["m2l"].shape[0])
+
+
+def field_error(pos, q, precision, torch, n_sample=4096):
+    """Normwise relative field error against the FP64 direct sum on sampled particles."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, direct_field
+
+    tree = FlatQuadtree(pos, q, Quad(0.0, 0.0, 1.0), kernel="log", order=ORDER,
+                        leaf_capacity=LEAF, precision=precision)
+    _, field = tree.fmm(theta=THETA, softening=SOFTENING)
+    idx = torch.tensor(np.random.default_rng(0).choice(pos.shape[1], n_sample, replace=False),
+                       device=pos.device)
+    _, ref = direct_field(pos[:, idx], pos, q, softening=SOFTENING, exclude=idx, kernel="log")
+    diff = (field[:, idx] - ref).abs().max() / ref.abs().max()
+    return float(diff), tree
 
 
 def run_ours(args):
@@ -254,8 +308,9 @@ def run_ours(args):
     torch.cuda.set_device(local)
     dist = None
     if world > 1:
-        import torch.distributed as dist_mod
         from datetime import timedelta
+
+        import torch.distributed as dist_mod
 
         dist = dist_mod
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
@@ -264,34 +319,28 @@ def run_ours(args):
     dev = torch.device("cuda", local)
     n = args.n
     pos_np, q_np = synthetic.mixture8(n, seed=SEED)
+    rng = np.random.default_rng(SEED + 1)
+    w_np, e_np = rng.normal(size=n), rng.normal(size=(2, n))
     pos = torch.tensor(pos_np, device=dev)
     q = torch.tensor(q_np, device=dev)
+    w = torch.tensor(w_np, device=dev)
+    e = torch.tensor(e_np, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
     for _ in range(args.warmup):
-        gpu_step(pos, q, torch)
+        gpu_step(pos, q, w, e, "mixed")
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
-    stream = torch.cuda.current_stream()
-    total_ms = 0.0
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
-        for _ in range(args.steps):
-            flush.fill_(1.0)
-            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            a.record(stream)
-            gpu_step(pos, q, torch)
-            b.record(stream)
-            b.synchronize()
-            total_ms += a.elapsed_time(b)
+        total_ms = time_steps(lambda: gpu_step(pos, q, w, e, "mixed"), args.steps, flush, torch)
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
     total_ms = max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / args.steps
     value = world * n * args.steps / (total_ms / 1e3)
-
     if args.trace_only:
         if dist:
             dist.destroy_process_group()
@@ -299,52 +348,52 @@ def run_ours(args):
             print(json.dumps({"trace_only": True, "ms_per_step": ms_per_step}), flush=True)
         return 0
 
-    # end to end through the public API: pinned host inputs in, host results out
-    from tree_d_3d_b200 import FlatQuadtree, Quad
+    # the plain FP64 form of the same step
+    for _ in range(max(1, args.warmup // 2)):
+        gpu_step(pos, q, w, e, "fp64")
+    fp64_ms = max_over_ranks(time_steps(lambda: gpu_step(pos, q, w, e, "fp64"), args.steps,
+                                        flush, torch), dist, dev)
+    fp64_value = world * n * args.steps / (fp64_ms / 1e3)
+    fwd_mixed = time_steps(lambda: gpu_step(pos, q, w, e, "mixed", backward=False), 3, flush,
+                           torch) / 3
+    fwd_fp64 = time_steps(lambda: gpu_step(pos, q, w, e, "fp64", backward=False), 3, flush,
+                          torch) / 3
 
-    pos_h = torch.tensor(pos_np).pin_memory()
-    q_h = torch.tensor(q_np).pin_memory()
-    phi_h = torch.empty(n, dtype=torch.float64).pin_memory()
-    field_h = torch.empty((2, n), dtype=torch.float64).pin_memory()
+    # end to end through the public API: pinned host inputs in, host results out
+    pos_h, q_h = torch.tensor(pos_np).pin_memory(), torch.tensor(q_np).pin_memory()
+    w_h, e_h = torch.tensor(w_np).pin_memory(), torch.tensor(e_np).pin_memory()
+    outs = [torch.empty(n, dtype=torch.float64).pin_memory(),
+            torch.empty((2, n), dtype=torch.float64).pin_memory(),
+            torch.empty((2, n), dtype=torch.float64).pin_memory(),
+            torch.empty(n, dtype=torch.float64).pin_memory()]
 
     def e2e_step():
-        p = pos_h.to(dev, non_blocking=True)
-        c = q_h.to(dev, non_blocking=True)
-        tree = FlatQuadtree(p, c, Quad(0.0, 0.0, 1.0), kernel="log", order=ORDER, leaf_capacity=LEAF)
-        phi, field = tree.fmm(theta=THETA, softening=SOFTENING)
-        phi_h.copy_(phi, non_blocking=True)
-        field_h.copy_(field, non_blocking=True)
+        results = gpu_step(pos_h.to(dev, non_blocking=True), q_h.to(dev, non_blocking=True),
+                           w_h.to(dev, non_blocking=True), e_h.to(dev, non_blocking=True), "mixed")
+        for host, r in zip(outs, results):
+            host.copy_(r, non_blocking=True)
 
     e2e_step()
     torch.cuda.synchronize()
-    e2e_ms = 0.0
-    for _ in range(args.steps):
-        flush.fill_(1.0)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        e2e_step()
-        b.record(stream)
-        b.synchronize()
-        e2e_ms += a.elapsed_time(b)
-    e2e_ms = max_over_ranks(e2e_ms, dist, dev)
+    e2e_ms = max_over_ranks(time_steps(e2e_step, args.steps, flush, torch), dist, dev)
     e2e_value = world * n * args.steps / (e2e_ms / 1e3)
 
-    # launches of our kernels per step, and the dominant kernel's roofline
-    launches = count_our_launches(lambda: gpu_step(pos, q, torch), torch)
-    tree, _, _ = gpu_step(pos, q, torch)
-    m2l_ms, n_m2l = time_m2l(tree, torch, reps=5)
-    w = ORDER + 1
-    flops = 2 * n_m2l * 8 * w * w  # directed translations x 8 (p + 1)^2
+    launches = count_our_launches(lambda: gpu_step(pos, q, w, e, "mixed"), torch)
+    err_mixed, tree = field_error(pos, q, "mixed", torch)
+    err_fp64, _ = field_error(pos, q, "fp64", torch)
+    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5)
+    width = ORDER + 1
+    flops = 2 * n_m2l * 8 * width * width  # directed translations x 8 (p + 1)^2
     achieved = flops / (m2l_ms * 1e-3) / 1e12
-    fp64_peak = 37.0  # nominal B200 FP64 (no measured FP64 peak is available)
     roofline = {
-        "kernel": "k_m2l_log (FP64 M2L)",
-        "bound": "fp64",
+        "kernel": "k_m2l_mixed<12> (FP32 M2L, forward)",
+        "bound": "fp32",
         "achieved": achieved,
-        "peak": fp64_peak,
+        "peak": FP32_PEAK,
         "unit": "TFLOP/s",
-        "frac": achieved / fp64_peak,
-        "peak_source": "nominal B200 FP64 FMA rate; MEASURED_PEAKS.json has no FP64 figure",
+        "frac": achieved / FP32_PEAK,
+        "peak_source": ("nominal FP32 FMA rate at the max SM clock (148 SM x 128 lanes x 2 x "
+                        "1965 MHz); MEASURED_PEAKS.json has no FP32 CUDA-core figure"),
         "traffic": None,
         "ms_per_launch": m2l_ms,
         "flop_per_launch": flops,
@@ -356,7 +405,7 @@ def run_ours(args):
     if rank != 0:
         return 0
     line = {
-        "metric": "FMM particles/s at N=1M p=12",
+        "metric": METRIC,
         "value": value,
         "unit": "particles/s",
         "n_gpus": world,
@@ -366,12 +415,17 @@ def run_ours(args):
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f64",
+        "dtype": "f32+f64 mixed",
         "data": "synthetic",
-        "config": {**_config(n), "parallelism": f"replicas x{world}", "precision": "fp64",
-                   "pipeline": "build + moments + traverse + M2L + L2L + L2P/P2P per step"},
+        "config": {**_config(n), "parallelism": f"replicas x{world}", "precision": "mixed"},
+        "fp64": {"value": fp64_value, "ms_per_step": fp64_ms / args.steps,
+                 "speedup_mixed_over_fp64": value / fp64_value,
+                 "rel_err_field": err_fp64},
+        "rel_err_field": err_mixed,
+        "forward_only_ms": {"mixed": fwd_mixed, "fp64": fwd_fp64},
         "e2e": {"value": e2e_value, "unit": "particles/s",
-                "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 3 * 8 * n},
+                "h2d_bytes_per_step": 8 * n * (2 + 1 + 1 + 2),
+                "d2h_bytes_per_step": 8 * n * (1 + 2 + 2 + 1)},
         "gpu_launches": int(sum(launches.values()) * args.steps),
         "launches_per_step": launches,
         "roofline": roofline,

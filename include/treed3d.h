@@ -259,6 +259,21 @@ int td3_fmm_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst
                 const double* moment_im, int order, const double* coeff, double* local_re,
                 double* local_im, void* stream);
 
+/* Mixed-precision M2L of the log kernel: moments scaled by the cell size, hat (nodes,
+ * order + 1) complex float pairs with hat_k = a_k / h^k (td3_scale_moments), translated
+ * in FP32 with ws = h_src / t and wd = h_dst / t (|ws|, |wd| < 1 for separated cells):
+ * s_l = sum_k coeff[k, l] hat_k ws^k, bhat_0 = a_0 ln|t| - s_0, bhat_l = -(-1)^l s_l wd^l,
+ * and local_re / local_im (FP64) += bhat_l / h_dst^l.  coeff is a HOST (order + 1)^2
+ * array (the reference's M2L matrix); order <= 20.  The FP32 counterpart of
+ * td3_fmm_m2l (reference: fmm_m2l_host, src/tree_d_3d/kernels/fmm_m2l_host/
+ * fmm_m2l_host_pyccel.py:16-105). */
+int td3_scale_moments(int64_t count, int order, const double* moment_re,
+                      const double* moment_im, const double* node_half, float* hat, void* stream);
+int td3_fmm_m2l_mixed(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                      const double* dst_center, const double* dst_half, const double* src_center,
+                      const double* src_half, const float* hat, int order, const double* coeff,
+                      double* local_re, double* local_im, void* stream);
+
 /* L2L from the root down, level by level (levels HOST, n_levels + 1): every local
  * expansion shifted into its children, b_m(child) += sum_{l>=m} C(l, m) b_l s^(l-m).
  * Replaces fmm_downward (src/tree_d_3d/kernels/fmm_downward/fmm_downward_pyccel.py:15-64,
@@ -317,6 +332,8 @@ int td3_nearfield_plan(const int64_t* rows, int64_t n_nodes, const int64_t* node
  * with_potential = 0); TD3_KERNEL_COULOMB: Cartesian local expansion local_a (nodes,
  * (order + 1)(order + 2)/2), softened Coulomb pairs.  A coincident pair of two nonzero
  * charges reports 1 + a particle index.  partial: 3 * partial length doubles.
+ * mixed != 0: the pair arithmetic in FP32 (pair differences taken in FP64, then
+ * rounded) with compensated (Kahan) accumulation; the local expansions in FP64.
  * Replaces fmm_evaluate_host (src/tree_d_3d/kernels/fmm_evaluate_host/
  * fmm_evaluate_host_pyccel.py:14-100), fmm_evaluate (kernels/fmm_evaluate/
  * fmm_evaluate_cuda.cu:11-87) and cart_evaluate_host (kernels/cart_evaluate_host/
@@ -327,7 +344,7 @@ int td3_fmm_evaluate(int kernel, const double* sorted_pos, const double* sorted_
                      const double* local_a, const double* local_b, const int64_t* p2p_partners,
                      const int* seg_leaf, const int64_t* seg_range, const int64_t* seg_out,
                      int64_t n_seg, double* partial, double softening, int with_potential,
-                     double* phi, double* field, int64_t* status, void* stream);
+                     int mixed, double* phi, double* field, int64_t* status, void* stream);
 
 /* fmm_at: L2P at the m targets (sorted_targets (2, m) in target-tree order, target_perm
  * their input indices, sorted_exclude their excluded source index) plus exact sums over
@@ -345,7 +362,7 @@ int td3_fmm_targets(int kernel, const double* sorted_targets, const int64_t* sor
                     int64_t n_seg, double* partial, const double* sorted_pos,
                     const double* sorted_charge, const int64_t* perm, int64_t n,
                     const int64_t* s_start, const int64_t* s_end, double softening,
-                    int with_potential, double* phi, double* field, int64_t* status,
+                    int with_potential, int mixed, double* phi, double* field, int64_t* status,
                     void* stream);
 
 /* ------------------------------------------------------------------ adjoint (backward) */
@@ -386,8 +403,8 @@ int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_c
                     const double* adj_b, const int64_t* p2p_partners, const int* seg_leaf,
                     const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
                     double* partial, const double* sorted_weight, const double* sorted_dipole,
-                    const double* efield, double softening, double* qbar, double* xbar,
-                    void* stream);
+                    const double* efield, double softening, int mixed, double* qbar,
+                    double* xbar, void* stream);
 
 /* ------------------------------------------------------------------ utilities */
 

@@ -146,6 +146,130 @@ __global__ void k_l2l_log(i64 lo, i64 hi, int order, const double* __restrict__ 
     local_im[ch * w + m] += acc_im;
 }
 
+// ------------------------------------------------------------------ mixed precision
+// Moments scaled by the cell size, hat_k = a_k / h^k (|hat_k| <= sum |q|), in FP32.
+__global__ void k_scale_moments(i64 count, int order, const double* __restrict__ mre,
+                                const double* __restrict__ mim, const double* __restrict__ half,
+                                float2* __restrict__ hat) {
+    int w = order + 1;
+    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= count * w) return;
+    i64 node = t / w;
+    int k = (int)(t % w);
+    double inv = 1.0 / half[node], s = 1.0;
+    for (int j = 0; j < k; ++j) s *= inv;
+    hat[t] = make_float2((float)(mre[t] * s), (float)(mim[t] * s));
+}
+
+template <int P>
+struct CoefTable {
+    float c[(P + 1) * (P + 1)];
+};
+
+// M2L in FP32, one lane per translation (partner), one warp per destination cell.
+// With w = 1/t, ws = h_src w and wd = h_dst w (|ws|, |wd| < 1 for separated cells):
+//   a'_k = hat_k ws^k,  s_l = sum_k coeff[k, l] a'_k,
+//   bhat_0 = a_0 ln|t| - s_0,  bhat_l = -(-1)^l s_l wd^l  (b_l = bhat_l / h_dst^l),
+// the reference's translation with every quantity O(1).  The coefficient matrix is a
+// kernel parameter (constant bank), the sums over the partners are warp reductions,
+// and the locals are added in FP64.
+template <int P>
+__global__ void __launch_bounds__(32 * M2L_WARPS)
+k_m2l_mixed(const i64* __restrict__ row_start, const i64* __restrict__ partners, i64 n_dst,
+            const double* __restrict__ dst_center, const double* __restrict__ dst_half,
+            const double* __restrict__ src_center, const double* __restrict__ src_half,
+            const float2* __restrict__ hat, int order, const CoefTable<P> C,
+            double* __restrict__ local_re, double* __restrict__ local_im) {
+    constexpr int W = P + 1;
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int w = order + 1;
+    for (i64 dst = (i64)blockIdx.x * M2L_WARPS + wib; dst < n_dst; dst += (i64)gridDim.x * M2L_WARPS) {
+        i64 e0 = row_start[dst], e1 = row_start[dst + 1];
+        if (e0 == e1) continue;
+        double cx = dst_center[2 * dst], cy = dst_center[2 * dst + 1], hd = dst_half[dst];
+        float br[W], bi[W];
+#pragma unroll
+        for (int l = 0; l < W; ++l) br[l] = bi[l] = 0.0f;
+        for (i64 base = e0; base < e1; base += 32) {
+            i64 e = base + lane;
+            if (e >= e1) continue;
+            i64 src = partners[e];
+            double tr = cx - src_center[2 * src], ti = cy - src_center[2 * src + 1];
+            double t2 = tr * tr + ti * ti, inv = 1.0 / t2, hs = src_half[src];
+            float wsr = (float)(hs * tr * inv), wsi = (float)(-hs * ti * inv);
+            float wdr = (float)(hd * tr * inv), wdi = (float)(-hd * ti * inv);
+            float lnt = (float)(0.5 * log(t2));
+            const float2* a = hat + src * w;
+            float ar[W], ai[W];
+            float pr = 1.0f, pi = 0.0f;
+#pragma unroll
+            for (int k = 0; k < W; ++k) {
+                float2 m = k < w ? a[k] : make_float2(0.0f, 0.0f);
+                ar[k] = m.x * pr - m.y * pi;
+                ai[k] = m.x * pi + m.y * pr;
+                float nr = pr * wsr - pi * wsi;
+                pi = pr * wsi + pi * wsr;
+                pr = nr;
+            }
+            float qr = 1.0f, qi = 0.0f;
+#pragma unroll
+            for (int l = 0; l < W; ++l) {
+                float sr = 0.0f, si = 0.0f;
+#pragma unroll
+                for (int k = 0; k < W; ++k) {
+                    sr += C.c[k * W + l] * ar[k];
+                    si += C.c[k * W + l] * ai[k];
+                }
+                if (l == 0) {
+                    br[0] += ar[0] * lnt - sr;
+                    bi[0] += ai[0] * lnt - si;
+                } else {
+                    float sign = (l & 1) ? 1.0f : -1.0f;
+                    br[l] += sign * (sr * qr - si * qi);
+                    bi[l] += sign * (sr * qi + si * qr);
+                }
+                float nr = qr * wdr - qi * wdi;
+                qi = qr * wdi + qi * wdr;
+                qr = nr;
+            }
+        }
+        double inv_h = 1.0 / hd, scale = 1.0;
+#pragma unroll
+        for (int l = 0; l < W; ++l) {
+            float vr = br[l], vi = bi[l];
+            for (int off = 16; off > 0; off >>= 1) {
+                vr += __shfl_xor_sync(0xffffffffu, vr, off);
+                vi += __shfl_xor_sync(0xffffffffu, vi, off);
+            }
+            if (lane == 0 && l < w) {
+                local_re[dst * w + l] += (double)vr * scale;
+                local_im[dst * w + l] += (double)vi * scale;
+            }
+            scale *= inv_h;
+        }
+    }
+}
+
+template <int P>
+int launch_m2l_mixed(const i64* row_start, const i64* partners, i64 n_dst, const double* dst_center,
+                     const double* dst_half, const double* src_center, const double* src_half,
+                     const float2* hat, int order, const double* coeff, double* lre, double* lim,
+                     cudaStream_t s) {
+    // the reference's matrix, zero-padded from (order + 1)^2 to (P + 1)^2
+    CoefTable<P> C;
+    int w = order + 1;
+    for (int k = 0; k <= P; ++k)
+        for (int l = 0; l <= P; ++l)
+            C.c[k * (P + 1) + l] = (k < w && l < w) ? (float)coeff[k * w + l] : 0.0f;
+    i64 blocks = (n_dst + M2L_WARPS - 1) / M2L_WARPS;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    k_m2l_mixed<P><<<(unsigned)blocks, 32 * M2L_WARPS, 0, s>>>(row_start, partners, n_dst,
+                                                                dst_center, dst_half, src_center,
+                                                                src_half, hat, order, C, lre, lim);
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
 template <int G, int CPL>
 void launch_m2l(const i64* row_start, const i64* partners, i64 n_dst, const double* dst_center,
                 const double* src_center, const double* mre, const double* mim, int order,
@@ -180,6 +304,43 @@ extern "C" int td3_fmm_m2l(const int64_t* row_start, const int64_t* partners, in
                           order, coeff, local_re, local_im, s);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
+}
+
+extern "C" int td3_scale_moments(int64_t count, int order, const double* moment_re,
+                                 const double* moment_im, const double* node_half, float* hat,
+                                 void* stream) {
+    if (count < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (count == 0) return TD3_OK;
+    i64 threads = count * (order + 1);
+    k_scale_moments<<<td3_blocks(threads, 256), 256, 0, td3_stream(stream)>>>(
+        count, order, moment_re, moment_im, node_half, reinterpret_cast<float2*>(hat));
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_fmm_m2l_mixed(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                                 const double* dst_center, const double* dst_half,
+                                 const double* src_center, const double* src_half,
+                                 const float* hat, int order, const double* coeff,
+                                 double* local_re, double* local_im, void* stream) {
+    if (n_dst < 0 || order < 0 || order > 20) return TD3_EINVAL;
+    if (n_dst == 0) return TD3_OK;
+    cudaStream_t s = td3_stream(stream);
+    const float2* h = reinterpret_cast<const float2*>(hat);
+    if (order <= 4)
+        return launch_m2l_mixed<4>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+                                   src_half, h, order, coeff, local_re, local_im, s);
+    if (order <= 8)
+        return launch_m2l_mixed<8>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+                                   src_half, h, order, coeff, local_re, local_im, s);
+    if (order <= 12)
+        return launch_m2l_mixed<12>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+                                    src_half, h, order, coeff, local_re, local_im, s);
+    if (order <= 16)
+        return launch_m2l_mixed<16>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+                                    src_half, h, order, coeff, local_re, local_im, s);
+    return launch_m2l_mixed<20>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+                                src_half, h, order, coeff, local_re, local_im, s);
 }
 
 extern "C" int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node_center,

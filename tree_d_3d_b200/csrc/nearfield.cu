@@ -193,11 +193,70 @@ struct Targets {
     i64 m;
 };
 
+// Compensated (Kahan) FP32 sum: the running error c is subtracted from each new term.
+struct KahanF {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x) {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// The mixed-precision near field of one target over a run of partner leaves: the pair
+// difference in FP64 (exact enough for close pairs far from the origin), rounded to
+// FP32, then FP32 kernel arithmetic with compensated accumulation.
+template <int KERNEL, bool POT, bool OTHER>
+__device__ __forceinline__ void near_mixed(const Sources& S, const i64* __restrict__ partners,
+                                           i64 e_begin, i64 e_end, int step, double xi, double yi,
+                                           double qi, i64 k, i64 skip, double eps2, double& pot,
+                                           double& ex, double& ey, bool& bad) {
+    KahanF p, x, y;
+    float eps2f = (float)eps2;
+    for (i64 e = e_begin; e < e_end; e += step) {
+        i64 b = partners[e];
+        i64 b1 = S.end[b];
+        for (i64 j = S.start[b]; j < b1; ++j) {
+            double qj = S.charge[j];
+            if (OTHER) {
+                if (qj == 0.0 || S.index[j] == skip) continue;
+            } else if (j == k) {
+                continue;
+            }
+            double dx64 = xi - S.pos[j], dy64 = yi - S.pos[S.n + j];
+            if (dx64 == 0.0 && dy64 == 0.0 && eps2 == 0.0) {
+                bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
+                continue;
+            }
+            float dx = (float)dx64, dy = (float)dy64, q = (float)qj;
+            float r2 = dx * dx + dy * dy + eps2f;
+            if (KERNEL == TD3_KERNEL_LOG) {
+                if (POT) p.add(-q * __logf(r2));
+                float f = __fdividef(2.0f * q, r2);
+                x.add(f * dx);
+                y.add(f * dy);
+            } else {
+                float inv_r = rsqrtf(r2);
+                float qr3 = q * inv_r * inv_r * inv_r;
+                p.add(q * inv_r);
+                x.add(qr3 * dx);
+                y.add(qr3 * dy);
+            }
+        }
+    }
+    pot = p.value();
+    ex = x.value();
+    ey = y.value();
+}
+
 // One warp per segment.  OTHER: targets and sources are different point sets (fmm_at):
 // zero charges and source exclude[i] are skipped and any coincidence is an error.
 // Otherwise targets are the sources themselves: a particle skips itself and a
-// coincident pair is an error only if both charges are nonzero.
-template <int KERNEL, bool POT, bool OTHER, int LOCAL>
+// coincident pair is an error only if both charges are nonzero.  MIXED: FP32 pair
+// arithmetic with compensated sums (near_mixed), else FP64.
+template <int KERNEL, bool POT, bool OTHER, int LOCAL, bool MIXED>
 __global__ void __launch_bounds__(32 * NF_WARPS)
 k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
        const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
@@ -225,7 +284,10 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
         i64 skip = OTHER ? (T.exclude ? T.exclude[k] : -1) : k;
         double pot = 0.0, ex = 0.0, ey = 0.0;
         bool bad = false;
-        if (valid) {
+        if (valid && MIXED) {
+            near_mixed<KERNEL, POT, OTHER>(S, partners, er.x + slice, er.y, slices, xi, yi, qi, k,
+                                           skip, eps2, pot, ex, ey, bad);
+        } else if (valid) {
             for (i64 e = er.x + slice; e < er.y; e += slices) {
                 i64 b = partners[e];
                 i64 b1 = S.end[b];
@@ -369,6 +431,38 @@ __device__ __forceinline__ void adjoint_pair(double dx, double dy, double eps2, 
     }
 }
 
+// adjoint_pair in FP32 with compensated accumulators (the pair difference arrives in FP32
+// after an FP64 subtraction).
+template <int KERNEL>
+__device__ __forceinline__ void adjoint_pair_mixed(float dx, float dy, float eps2, float qj,
+                                                   float wj, float exj, float eyj, KahanF* acc) {
+    float s = dx * dx + dy * dy + eps2;
+    float de = exj * dx + eyj * dy;
+    if (KERNEL == TD3_KERNEL_LOG) {
+        float inv = __frcp_rn(s);
+        acc[0].add(-wj * __logf(s) - 2.0f * de * inv);
+        float t = 4.0f * de * inv * inv;
+        acc[1].add(-2.0f * inv * (wj * dx + exj) + t * dx);
+        acc[2].add(-2.0f * inv * (wj * dy + eyj) + t * dy);
+        float q4 = 4.0f * qj * inv * inv;
+        acc[3].add(-2.0f * qj * inv + q4 * dx * dx);
+        acc[4].add(q4 * dx * dy);
+        acc[5].add(-2.0f * qj * inv + q4 * dy * dy);
+    } else {
+        float r = rsqrtf(s);
+        float r3 = r * r * r;
+        float r5 = r3 * r * r;
+        acc[0].add(wj * r - de * r3);
+        float t = 3.0f * de * r5;
+        acc[1].add(-r3 * (wj * dx + exj) + t * dx);
+        acc[2].add(-r3 * (wj * dy + eyj) + t * dy);
+        float q3 = 3.0f * qj * r5;
+        acc[3].add(-qj * r3 + q3 * dx * dx);
+        acc[4].add(q3 * dx * dy);
+        acc[5].add(-qj * r3 + q3 * dy * dy);
+    }
+}
+
 template <int LOCAL>
 __device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, i64 n,
                                                double ux, double uy, i64 leaf, int order,
@@ -386,7 +480,7 @@ __device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, 
     A.xbar[n + i] = -w * A.efield[n + i] + q * gy - (mxy * ex + myy * ey);
 }
 
-template <int KERNEL, int LOCAL>
+template <int KERNEL, int LOCAL, bool MIXED>
 __global__ void __launch_bounds__(32 * NF_WARPS)
 k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
                const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
@@ -412,7 +506,23 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
         i64 k = s0 + (valid ? it : 0);
         double xi = S.pos[k], yi = S.pos[n + k];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (valid) {
+        if (valid && MIXED) {
+            KahanF kacc[6];
+            float eps2f = (float)eps2;
+            for (i64 e = er.x + slice; e < er.y; e += slices) {
+                i64 b = partners[e];
+                i64 b1 = S.end[b];
+                for (i64 j = S.start[b]; j < b1; ++j) {
+                    if (j == k) continue;
+                    double dx = xi - S.pos[j], dy = yi - S.pos[n + j];
+                    if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) continue;
+                    adjoint_pair_mixed<KERNEL>((float)dx, (float)dy, eps2f, (float)S.charge[j],
+                                               (float)A.weight[j], (float)A.dipole[j],
+                                               (float)A.dipole[n + j], kacc);
+                }
+            }
+            for (int c = 0; c < 6; ++c) acc[c] = kacc[c].value();
+        } else if (valid) {
             for (i64 e = er.x + slice; e < er.y; e += slices) {
                 i64 b = partners[e];
                 i64 b1 = S.end[b];
@@ -472,48 +582,53 @@ __global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg
     }
 }
 
-template <int KERNEL, bool POT, bool OTHER, int LOCAL>
-int launch_near(const Targets& T, const Sources& S, i64 n_seg, const int* seg_leaf,
-                const longlong2* seg_range, const i64* seg_out, const i64* partners,
-                const double* la, const double* lb, int order, int width, double eps2,
-                double* partial, double* phi, double* field, i64* status, cudaStream_t s) {
-    if (n_seg == 0) return TD3_OK;
-    unsigned blocks = td3_blocks(n_seg, NF_WARPS);
-    k_near<KERNEL, POT, OTHER, LOCAL><<<blocks, 32 * NF_WARPS, 0, s>>>(
-        T, S, n_seg, seg_leaf, seg_range, seg_out, partners, la, lb, order, width, eps2, partial,
-        phi, field, status);
-    k_near_finish<POT, LOCAL><<<blocks, 32 * NF_WARPS, 0, s>>>(T, n_seg, seg_leaf, seg_out, la, lb,
-                                                               order, width, partial, phi, field);
+struct NearArgs {
+    Targets T;
+    Sources S;
+    i64 n_seg;
+    const int* seg_leaf;
+    const longlong2* seg_range;
+    const i64* seg_out;
+    const i64* partners;
+    const double* la;
+    const double* lb;
+    int order, width;
+    double eps2;
+    double* partial;
+    double* phi;
+    double* field;
+    i64* status;
+};
+
+template <int KERNEL, bool POT, bool OTHER, int LOCAL, bool MIXED>
+int launch_near(const NearArgs& a, cudaStream_t s) {
+    if (a.n_seg == 0) return TD3_OK;
+    unsigned blocks = td3_blocks(a.n_seg, NF_WARPS);
+    k_near<KERNEL, POT, OTHER, LOCAL, MIXED><<<blocks, 32 * NF_WARPS, 0, s>>>(
+        a.T, a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out, a.partners, a.la, a.lb, a.order,
+        a.width, a.eps2, a.partial, a.phi, a.field, a.status);
+    k_near_finish<POT, LOCAL><<<blocks, 32 * NF_WARPS, 0, s>>>(a.T, a.n_seg, a.seg_leaf, a.seg_out,
+                                                               a.la, a.lb, a.order, a.width,
+                                                               a.partial, a.phi, a.field);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
 
 template <bool OTHER, int LOCAL>
-int dispatch_near(int kernel, int with_potential, const Targets& T, const Sources& S, i64 n_seg,
-                  const int* seg_leaf, const longlong2* seg_range, const i64* seg_out,
-                  const i64* partners, const double* la, const double* lb, int order, int width,
-                  double eps2, double* partial, double* phi, double* field, i64* status,
-                  cudaStream_t s) {
-    if (kernel == TD3_KERNEL_LOG)
-        return with_potential
-                   ? launch_near<TD3_KERNEL_LOG, true, OTHER, LOCAL>(T, S, n_seg, seg_leaf, seg_range,
-                                                                      seg_out, partners, la, lb, order,
-                                                                      width, eps2, partial, phi,
-                                                                      field, status, s)
-                   : launch_near<TD3_KERNEL_LOG, false, OTHER, LOCAL>(T, S, n_seg, seg_leaf, seg_range,
-                                                                       seg_out, partners, la, lb,
-                                                                       order, width, eps2, partial,
-                                                                       phi, field, status, s);
-    return with_potential
-               ? launch_near<TD3_KERNEL_COULOMB, true, OTHER, LOCAL>(T, S, n_seg, seg_leaf, seg_range,
-                                                                      seg_out, partners, la, lb,
-                                                                      order, width, eps2, partial,
-                                                                      phi, field, status, s)
-               : launch_near<TD3_KERNEL_COULOMB, false, OTHER, LOCAL>(T, S, n_seg, seg_leaf,
-                                                                       seg_range, seg_out, partners,
-                                                                       la, lb, order, width, eps2,
-                                                                       partial, phi, field, status,
-                                                                       s);
+int dispatch_near(int kernel, int with_potential, int mixed, const NearArgs& a, cudaStream_t s) {
+    constexpr int LG = TD3_KERNEL_LOG, CL = TD3_KERNEL_COULOMB;
+    if (kernel == LG) {
+        if (with_potential)
+            return mixed ? launch_near<LG, true, OTHER, LOCAL, true>(a, s)
+                         : launch_near<LG, true, OTHER, LOCAL, false>(a, s);
+        return mixed ? launch_near<LG, false, OTHER, LOCAL, true>(a, s)
+                     : launch_near<LG, false, OTHER, LOCAL, false>(a, s);
+    }
+    if (with_potential)
+        return mixed ? launch_near<CL, true, OTHER, LOCAL, true>(a, s)
+                     : launch_near<CL, true, OTHER, LOCAL, false>(a, s);
+    return mixed ? launch_near<CL, false, OTHER, LOCAL, true>(a, s)
+                 : launch_near<CL, false, OTHER, LOCAL, false>(a, s);
 }
 
 }  // namespace
@@ -565,24 +680,35 @@ extern "C" int td3_fmm_evaluate(int kernel, const double* sorted_pos, const doub
                                 const double* local_a, const double* local_b,
                                 const int64_t* p2p_partners, const int* seg_leaf,
                                 const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
-                                double* partial, double softening, int with_potential,
+                                double* partial, double softening, int with_potential, int mixed,
                                 double* phi, double* field, int64_t* status, void* stream) {
     if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
     if (n == 0) return TD3_OK;
-    Targets T{sorted_pos, nullptr, perm, node_center, node_start, node_end, n};
-    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n};
-    double eps2 = softening * softening;
+    bool lg = kernel == TD3_KERNEL_LOG;
+    NearArgs a{Targets{sorted_pos, nullptr, perm, node_center, node_start, node_end, n},
+               Sources{sorted_pos, sorted_charge, perm, node_start, node_end, n},
+               n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
+               p2p_partners, local_a, local_b, order,
+               lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,
+               phi, field, status};
     cudaStream_t s = td3_stream(stream);
-    const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
-    if (kernel == TD3_KERNEL_LOG)
-        return dispatch_near<false, LOCAL_COMPLEX>(kernel, with_potential, T, S, n_seg, seg_leaf, sr,
-                                                   seg_out, p2p_partners, local_a, local_b, order,
-                                                   order + 1, eps2, partial, phi, field, status, s);
-    return dispatch_near<false, LOCAL_CART>(kernel, with_potential, T, S, n_seg, seg_leaf, sr,
-                                            seg_out, p2p_partners, local_a, local_b, order,
-                                            (order + 1) * (order + 2) / 2, eps2, partial, phi, field,
-                                            status, s);
+    if (lg) return dispatch_near<false, LOCAL_COMPLEX>(kernel, with_potential, mixed, a, s);
+    return dispatch_near<false, LOCAL_CART>(kernel, with_potential, mixed, a, s);
+}
+
+template <int KERNEL, int LOCAL, bool MIXED>
+void launch_adjoint(const Targets& T, const Sources& S, const Adjoint& A, i64 n_seg,
+                    const int* seg_leaf, const longlong2* sr, const i64* seg_out,
+                    const i64* partners, const double* fa, const double* fb, const double* ba,
+                    const double* bb, int order, int width, double eps2, double* partial,
+                    cudaStream_t s) {
+    unsigned blocks = td3_blocks(n_seg, NF_WARPS);
+    k_near_adjoint<KERNEL, LOCAL, MIXED><<<blocks, 32 * NF_WARPS, 0, s>>>(
+        T, S, A, n_seg, seg_leaf, sr, seg_out, partners, fa, fb, ba, bb, order, width, eps2,
+        partial);
+    k_near_adjoint_finish<LOCAL><<<blocks, 32 * NF_WARPS, 0, s>>>(
+        T, S, A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb, order, width, partial);
 }
 
 extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_charge,
@@ -593,7 +719,7 @@ extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const doubl
                                const int* seg_leaf, const int64_t* seg_range,
                                const int64_t* seg_out, int64_t n_seg, double* partial,
                                const double* sorted_weight, const double* sorted_dipole,
-                               const double* efield, double softening, double* qbar,
+                               const double* efield, double softening, int mixed, double* qbar,
                                double* xbar, void* stream) {
     if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
@@ -604,21 +730,29 @@ extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const doubl
     double eps2 = softening * softening;
     cudaStream_t s = td3_stream(stream);
     const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
-    unsigned blocks = td3_blocks(n_seg, NF_WARPS);
     if (kernel == TD3_KERNEL_LOG) {
         int width = order + 1;
-        k_near_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX><<<blocks, 32 * NF_WARPS, 0, s>>>(
-            T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b, order,
-            width, eps2, partial);
-        k_near_adjoint_finish<LOCAL_COMPLEX><<<blocks, 32 * NF_WARPS, 0, s>>>(
-            T, S, A, n_seg, seg_leaf, seg_out, fwd_a, fwd_b, adj_a, adj_b, order, width, partial);
+        if (mixed)
+            launch_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX, true>(T, S, A, n_seg, seg_leaf, sr, seg_out,
+                                                                p2p_partners, fwd_a, fwd_b, adj_a,
+                                                                adj_b, order, width, eps2, partial, s);
+        else
+            launch_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX, false>(T, S, A, n_seg, seg_leaf, sr,
+                                                                 seg_out, p2p_partners, fwd_a, fwd_b,
+                                                                 adj_a, adj_b, order, width, eps2,
+                                                                 partial, s);
     } else {
         int width = (order + 1) * (order + 2) / 2;
-        k_near_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART><<<blocks, 32 * NF_WARPS, 0, s>>>(
-            T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b, order,
-            width, eps2, partial);
-        k_near_adjoint_finish<LOCAL_CART><<<blocks, 32 * NF_WARPS, 0, s>>>(
-            T, S, A, n_seg, seg_leaf, seg_out, fwd_a, fwd_b, adj_a, adj_b, order, width, partial);
+        if (mixed)
+            launch_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART, true>(T, S, A, n_seg, seg_leaf, sr,
+                                                                 seg_out, p2p_partners, fwd_a, fwd_b,
+                                                                 adj_a, adj_b, order, width, eps2,
+                                                                 partial, s);
+        else
+            launch_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART, false>(T, S, A, n_seg, seg_leaf, sr,
+                                                                  seg_out, p2p_partners, fwd_a, fwd_b,
+                                                                  adj_a, adj_b, order, width, eps2,
+                                                                  partial, s);
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;
@@ -634,21 +768,19 @@ extern "C" int td3_fmm_targets(int kernel, const double* sorted_targets,
                                const double* sorted_pos, const double* sorted_charge,
                                const int64_t* perm, int64_t n, const int64_t* s_start,
                                const int64_t* s_end, double softening, int with_potential,
-                               double* phi, double* field, int64_t* status, void* stream) {
+                               int mixed, double* phi, double* field, int64_t* status,
+                               void* stream) {
     if (m < 0 || n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
     if (m == 0) return TD3_OK;
-    Targets T{sorted_targets, sorted_exclude, target_perm, t_center, t_start, t_end, m};
-    Sources S{sorted_pos, sorted_charge, perm, s_start, s_end, n};
-    double eps2 = softening * softening;
+    bool lg = kernel == TD3_KERNEL_LOG;
+    NearArgs a{Targets{sorted_targets, sorted_exclude, target_perm, t_center, t_start, t_end, m},
+               Sources{sorted_pos, sorted_charge, perm, s_start, s_end, n},
+               n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
+               p2p_partners, local_a, local_b, order,
+               lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,
+               phi, field, status};
     cudaStream_t s = td3_stream(stream);
-    const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
-    if (kernel == TD3_KERNEL_LOG)
-        return dispatch_near<true, LOCAL_COMPLEX>(kernel, with_potential, T, S, n_seg, seg_leaf, sr,
-                                                  seg_out, p2p_partners, local_a, local_b, order,
-                                                  order + 1, eps2, partial, phi, field, status, s);
-    return dispatch_near<true, LOCAL_CART>(kernel, with_potential, T, S, n_seg, seg_leaf, sr,
-                                           seg_out, p2p_partners, local_a, local_b, order,
-                                           (order + 1) * (order + 2) / 2, eps2, partial, phi, field,
-                                           status, s);
+    if (lg) return dispatch_near<true, LOCAL_COMPLEX>(kernel, with_potential, mixed, a, s);
+    return dispatch_near<true, LOCAL_CART>(kernel, with_potential, mixed, a, s);
 }

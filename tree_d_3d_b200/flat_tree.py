@@ -342,6 +342,7 @@ class FlatQuadtree:
 
     def _moments(self) -> None:
         """ft:663-744: cell charges and multipole moments from the charges."""
+        self._fwd_locals = None
         count, dev, f64 = self.node_count, self.device, torch.float64
         n = self.pos.shape[1]
         self.node_q = torch.empty(count, dtype=f64, device=dev)
@@ -581,6 +582,7 @@ class FlatQuadtree:
             return out((phi, field), self._numpy)
         lists = self._lists(theta)
         local_re, local_im = self._log_locals(lists)
+        self._fwd_locals = ((theta, softening), local_re, local_im)
         status = status_word(dev)
         self._evaluate_near(lists, _lib.KERNEL_LOG, local_re, local_im, softening, potential,
                             phi, field, status)
@@ -597,11 +599,8 @@ class FlatQuadtree:
         local_im = torch.zeros((count, w), dtype=torch.float64, device=dev)
         stream = _lib.stream(dev)
         if lists["m2l"].shape[0]:
-            _lib.call("td3_fmm_m2l", lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(),
-                      count, self.node_center.data_ptr(), self.node_center.data_ptr(),
-                      mre.data_ptr(), mim.data_ptr(), self.order,
-                      self._m2l_matrix().data_ptr(), local_re.data_ptr(), local_im.data_ptr(),
-                      stream)
+            self._m2l_log(lists["m2l_rows"], lists["m2l_partners"], self, (mre, mim), local_re,
+                          local_im)
         levels = np.ascontiguousarray(self.levels, dtype=np.int64)
         binom = self._binomial()
         _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
@@ -621,8 +620,34 @@ class FlatQuadtree:
             self.node_start.data_ptr(), self.node_end.data_ptr(), self.order, local_a.data_ptr(),
             local_b.data_ptr(), lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
             plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
-            plan["partial"].data_ptr(), float(softening), 1 if potential else 0, phi.data_ptr(),
-            field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
+            plan["partial"].data_ptr(), float(softening), 1 if potential else 0, self._mixed,
+            phi.data_ptr(), field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
+
+    @property
+    def _mixed(self) -> int:
+        return 1 if self.precision == "mixed" else 0
+
+    def _m2l_log(self, rows, partners, dst, moments, local_re, local_im):
+        """Log-kernel M2L from this tree's cells into ``dst``'s: FP64, or FP32 on moments
+        scaled by the cell size for ``precision="mixed"`` (orders up to 20)."""
+        stream = _lib.stream(self.device)
+        mre, mim = moments
+        if self.precision == "mixed" and self.order <= 20:
+            hat = torch.empty((self.node_count, self.order + 1, 2), dtype=torch.float32,
+                              device=self.device)
+            _lib.call("td3_scale_moments", self.node_count, self.order, mre.data_ptr(),
+                      mim.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(), stream)
+            coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
+            _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), partners.data_ptr(), dst.node_count,
+                      dst.node_center.data_ptr(), dst.node_half.data_ptr(),
+                      self.node_center.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(),
+                      self.order, coeff.ctypes.data, local_re.data_ptr(), local_im.data_ptr(),
+                      stream)
+            return
+        _lib.call("td3_fmm_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
+                  dst.node_center.data_ptr(), self.node_center.data_ptr(), mre.data_ptr(),
+                  mim.data_ptr(), self.order, self._m2l_matrix().data_ptr(), local_re.data_ptr(),
+                  local_im.data_ptr(), stream)
 
     # ------------------------------------------------------------------ backward
     def _fmm_adjoint(self, theta: float, softening: float, weight: torch.Tensor,
@@ -640,9 +665,12 @@ class FlatQuadtree:
         efield = efield.to(torch.float64).contiguous()
         levels = np.ascontiguousarray(self.levels, dtype=np.int64)
         stream = _lib.stream(dev)
+        kept = getattr(self, "_fwd_locals", None)
+        if kept is not None and kept[0] != (theta, softening):
+            kept = None
         if self.kernel == "log":
             w = self.order + 1
-            fwd_a, fwd_b = self._log_locals(lists)
+            fwd_a, fwd_b = (kept[1], kept[2]) if kept else self._log_locals(lists)
             mre = torch.empty((count, w), dtype=torch.float64, device=dev)
             mim = torch.empty_like(mre)
             wabs = torch.empty(count, dtype=torch.float64, device=dev)
@@ -658,8 +686,8 @@ class FlatQuadtree:
             t = self._cartesian_tables()
             n_coef = _cartesian.size(self.order)
             n_m2l = lists["m2l"].shape[0]
-            fwd_a = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"], n_m2l, self,
-                                      softening)
+            fwd_a = kept[1] if kept else self._cart_locals(
+                lists["m2l_rows"], lists["m2l_partners"], n_m2l, self, softening)
             moments = torch.empty((count, n_coef), dtype=torch.float64, device=dev)
             _lib.call("td3_cart_moments_adjoint", levels.ctypes.data, len(levels) - 1,
                       self._sorted_pos.data_ptr(), sw.data_ptr(), sd.data_ptr(), n,
@@ -682,7 +710,7 @@ class FlatQuadtree:
                   adj_b.data_ptr(), lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
                   plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
                   partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), efield.data_ptr(),
-                  float(softening), qbar.data_ptr(), xbar.data_ptr(), stream)
+                  float(softening), self._mixed, qbar.data_ptr(), xbar.data_ptr(), stream)
         return qbar, xbar
 
     def _move_within_cells(self, positions) -> None:
@@ -789,12 +817,8 @@ class FlatQuadtree:
             local_a = torch.zeros((tree.node_count, w), dtype=torch.float64, device=dev)
             local_b = torch.zeros_like(local_a)
             if n_m2l:
-                _lib.call("td3_fmm_m2l", lists["m2l_rows"].data_ptr(),
-                          lists["m2l_partners"].data_ptr(), tree.node_count,
-                          tree.node_center.data_ptr(), self.node_center.data_ptr(),
-                          self.moment_re.data_ptr(), self.moment_im.data_ptr(), self.order,
-                          self._m2l_matrix().data_ptr(), local_a.data_ptr(), local_b.data_ptr(),
-                          stream)
+                self._m2l_log(lists["m2l_rows"], lists["m2l_partners"], tree,
+                              (self.moment_re, self.moment_im), local_a, local_b)
             levels = np.ascontiguousarray(tree.levels, dtype=np.int64)
             binom = self._binomial()
             _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
@@ -817,8 +841,8 @@ class FlatQuadtree:
             plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
             plan["partial"].data_ptr(), self._sorted_pos.data_ptr(),
             self._sorted_charge.data_ptr(), self.perm.data_ptr(), n, self.node_start.data_ptr(),
-            self.node_end.data_ptr(), float(softening), 1 if with_pot else 0, phi.data_ptr(),
-            field.data_ptr(), status.data_ptr(), stream)
+            self.node_end.data_ptr(), float(softening), 1 if with_pot else 0, self._mixed,
+            phi.data_ptr(), field.data_ptr(), status.data_ptr(), stream)
         _check(status)
         if not potential:
             phi.zero_()
@@ -855,6 +879,7 @@ class FlatQuadtree:
         lists = self._lists(theta)
         local = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"],
                                   lists["m2l"].shape[0], self, softening)
+        self._fwd_locals = ((theta, softening), local, local)
         status = status_word(self.device)
         self._evaluate_near(lists, _lib.KERNEL_COULOMB, local, local, softening, True, phi,
                             field, status)
