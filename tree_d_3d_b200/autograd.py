@@ -39,6 +39,7 @@ class _FMMField(torch.autograd.Function):
     def backward(ctx, grad_phi, grad_field):
         (field,) = ctx.saved_tensors
         tree = ctx.tree
+        ctx.tree = None  # the tree's buffers go as soon as the backward is done
         n = field.shape[1]
         if grad_phi is None:
             grad_phi = torch.zeros(n, dtype=torch.float64, device=field.device)

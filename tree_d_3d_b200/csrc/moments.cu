@@ -135,6 +135,132 @@ __global__ void k_log_moments(i64 lo, i64 hi, int order, const double* __restric
     if (n == 0) node_qabs[node] = qabs;
 }
 
+// The same moments with one thread per node and every coefficient in registers (orders
+// up to P, compile-time loop bounds); the operations and their order per coefficient are
+// those of k_log_moments, so the results are the same bits.
+template <int P>
+__global__ void k_log_moments_node(i64 lo, i64 hi, int order, const double* __restrict__ spos,
+                                   const double* __restrict__ scharge, i64 n_particles,
+                                   const double* __restrict__ node_center,
+                                   const i64* __restrict__ node_start,
+                                   const i64* __restrict__ node_end,
+                                   const i64* __restrict__ node_child,
+                                   const double* __restrict__ binomial, int bsize,
+                                   double* node_qabs, double* moment_re, double* moment_im,
+                                   const double* __restrict__ sdip) {
+    constexpr int W = P + 1;
+    i64 node = lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= hi) return;
+    int w = order + 1;
+    double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
+    double ar[W], ai[W];
+#pragma unroll
+    for (int n = 0; n < W; ++n) ar[n] = ai[n] = 0.0;
+    double qabs = 0.0;
+    i64 first = node_child[node];
+    if (first < 0) {
+        for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+            double q = scharge[k];
+            qabs += fabs(q);
+            double dx = spos[k] - xmid, dy = spos[n_particles + k] - ymid;
+            double pr = q, pi = 0.0;
+#pragma unroll
+            for (int n = 0; n < W; ++n) {
+                ar[n] += pr;
+                ai[n] += pi;
+                double next_re = pr * dx - pi * dy;
+                pi = pr * dy + pi * dx;
+                pr = next_re;
+            }
+            if (sdip) {
+                double er = sdip[k], ei = sdip[n_particles + k];
+                double zr = 1.0, zi = 0.0;
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    ar[n] -= n * (er * zr - ei * zi);
+                    ai[n] -= n * (er * zi + ei * zr);
+                    double nr = zr * dx - zi * dy;
+                    zi = zr * dy + zi * dx;
+                    zr = nr;
+                }
+            }
+        }
+    } else {
+        for (i64 child = first; child < first + 4; ++child) {
+            qabs += node_qabs[child];
+            if (node_end[child] == node_start[child]) continue;
+            double s_re = node_center[2 * child] - xmid;
+            double s_im = node_center[2 * child + 1] - ymid;
+            double sh_re[W], sh_im[W], cr[W], ci[W];
+            sh_re[0] = 1.0;
+            sh_im[0] = 0.0;
+#pragma unroll
+            for (int n = 1; n < W; ++n) {
+                sh_re[n] = sh_re[n - 1] * s_re - sh_im[n - 1] * s_im;
+                sh_im[n] = sh_re[n - 1] * s_im + sh_im[n - 1] * s_re;
+            }
+#pragma unroll
+            for (int m = 0; m < W; ++m) {
+                cr[m] = m < w ? moment_re[child * w + m] : 0.0;
+                ci[m] = m < w ? moment_im[child * w + m] : 0.0;
+            }
+#pragma unroll
+            for (int n = 0; n < W; ++n) {
+                double acc_re = 0.0, acc_im = 0.0;
+#pragma unroll
+                for (int m = 0; m <= n; ++m) {
+                    double c = binomial[n * bsize + m];
+                    double a_re = cr[m] * c, a_im = ci[m] * c;
+                    acc_re += a_re * sh_re[n - m] - a_im * sh_im[n - m];
+                    acc_im += a_re * sh_im[n - m] + a_im * sh_re[n - m];
+                }
+                ar[n] += acc_re;
+                ai[n] += acc_im;
+            }
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < W; ++n) {
+        if (n < w) {
+            moment_re[node * w + n] = ar[n];
+            moment_im[node * w + n] = ai[n];
+        }
+    }
+    node_qabs[node] = qabs;
+}
+
+// Moments of every level, deepest first, with the per-node kernel for orders up to 16.
+int launch_log_moments(const int64_t* levels, int64_t n_levels, int order, const double* spos,
+                       const double* scharge, int64_t n, const double* center, const i64* start,
+                       const i64* end, const i64* child, const double* binomial, int bsize,
+                       double* qabs, double* mre, double* mim, const double* sdip,
+                       cudaStream_t s) {
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        unsigned nb = td3_blocks(hi - lo, MOM_THREADS);
+#define TD3_NODE_MOMENTS(P)                                                                  \
+    k_log_moments_node<P><<<nb, MOM_THREADS, 0, s>>>(lo, hi, order, spos, scharge, n, center, \
+                                                     start, end, child, binomial, bsize, qabs,\
+                                                     mre, mim, sdip)
+        if (order <= 4)
+            TD3_NODE_MOMENTS(4);
+        else if (order <= 8)
+            TD3_NODE_MOMENTS(8);
+        else if (order <= 12)
+            TD3_NODE_MOMENTS(12);
+        else if (order <= 16)
+            TD3_NODE_MOMENTS(16);
+        else
+            k_log_moments<<<td3_blocks((hi - lo) * (order + 1), MOM_THREADS), MOM_THREADS, 0, s>>>(
+                lo, hi, order, spos, scharge, n, center, start, end, child, binomial, bsize, qabs,
+                mre, mim, sdip);
+#undef TD3_NODE_MOMENTS
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
 // One thread per (node, coefficient g).  The monomial u^(a,b) is built as the
 // reference's mono recurrence builds it: b factors of u_y, then a factors of u_x.
 __device__ __forceinline__ double monomial(double start, double ux, double uy, int a, int b) {
@@ -215,17 +341,9 @@ extern "C" int td3_log_moments(const int64_t* levels, int64_t n_levels, int orde
                                double* moment_re, double* moment_im, void* stream) {
     if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER || binomial_size < order + 1)
         return TD3_EINVAL;
-    cudaStream_t s = td3_stream(stream);
-    for (i64 level = n_levels - 1; level >= 0; --level) {
-        i64 lo = levels[level], hi = levels[level + 1];
-        if (hi <= lo) continue;
-        i64 threads = (hi - lo) * (order + 1);
-        k_log_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
-            lo, hi, order, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
-            node_child, binomial, binomial_size, node_qabs, moment_re, moment_im, nullptr);
-    }
-    TD3_CHECK_LAUNCH();
-    return TD3_OK;
+    return launch_log_moments(levels, n_levels, order, sorted_pos, sorted_charge, n, node_center,
+                              node_start, node_end, node_child, binomial, binomial_size,
+                              node_qabs, moment_re, moment_im, nullptr, td3_stream(stream));
 }
 
 extern "C" int td3_log_moments_adjoint(const int64_t* levels, int64_t n_levels, int order,
@@ -238,17 +356,9 @@ extern "C" int td3_log_moments_adjoint(const int64_t* levels, int64_t n_levels, 
                                        void* stream) {
     if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER || binomial_size < order + 1)
         return TD3_EINVAL;
-    cudaStream_t s = td3_stream(stream);
-    for (i64 level = n_levels - 1; level >= 0; --level) {
-        i64 lo = levels[level], hi = levels[level + 1];
-        if (hi <= lo) continue;
-        i64 threads = (hi - lo) * (order + 1);
-        k_log_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
-            lo, hi, order, sorted_pos, sorted_weight, n, node_center, node_start, node_end,
-            node_child, binomial, binomial_size, node_wabs, moment_re, moment_im, sorted_dipole);
-    }
-    TD3_CHECK_LAUNCH();
-    return TD3_OK;
+    return launch_log_moments(levels, n_levels, order, sorted_pos, sorted_weight, n, node_center,
+                              node_start, node_end, node_child, binomial, binomial_size,
+                              node_wabs, moment_re, moment_im, sorted_dipole, td3_stream(stream));
 }
 
 extern "C" int td3_cart_moments(const int64_t* levels, int64_t n_levels, const double* sorted_pos,

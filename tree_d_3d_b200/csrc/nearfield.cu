@@ -345,6 +345,23 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
     }
 }
 
+// The number of consecutive segments of `leaf` starting at its first segment `seg`,
+// found 32 segments at a time (the same value in every lane).
+__device__ __forceinline__ i64 leaf_segments(const int* __restrict__ seg_leaf, i64 seg, i64 n_seg,
+                                             i64 leaf, int lane) {
+    i64 count = 0;
+    for (;;) {
+        i64 s = seg + count + lane;
+        bool same = s < n_seg && seg_leaf[s] == leaf;
+        unsigned m = __ballot_sync(0xffffffffu, same);
+        if (m == 0xffffffffu) {
+            count += 32;
+            continue;
+        }
+        return count + __ffs(~m) - 1;
+    }
+}
+
 // Leaves whose row took several segments: partial sums in segment order, plus L2P.
 template <bool POT, int LOCAL>
 __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_leaf,
@@ -361,25 +378,33 @@ __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_
     i64 leaf = seg_leaf[seg];
     i64 s0 = T.start[leaf];
     int count = (int)(T.end[leaf] - s0);
-    i64 last = seg;
-    while (last + 1 < n_seg && seg_leaf[last + 1] == leaf) ++last;
-    for (int it = lane; it < count; it += 32) {
+    i64 nseg = leaf_segments(seg_leaf, seg, n_seg, leaf, lane);
+    // the partial sums of a target over the leaf's segments: lanes split the segments
+    // (a row can take thousands), a fixed-order warp reduction combines them
+    for (int it = 0; it < count; ++it) {
         double pot = 0.0, ex = 0.0, ey = 0.0;
-        for (i64 s = seg; s <= last; ++s) {
+        for (i64 s = seg + lane; s < seg + nseg; s += 32) {
             i64 p = seg_out[s] + it;
             pot += partial[3 * p];
             ex += partial[3 * p + 1];
             ey += partial[3 * p + 2];
         }
-        i64 k = s0 + it;
-        double xi = T.pos[k], yi = T.pos[T.m + k];
-        double lp, lx, ly;
-        eval_local<LOCAL>(local_a, local_b, leaf, order, width, xi - T.center[2 * leaf],
-                          yi - T.center[2 * leaf + 1], lp, lx, ly);
-        i64 i = T.perm[k];
-        phi[i] = POT ? lp + pot : 0.0;
-        field[i] = lx + ex;
-        field[T.m + i] = ly + ey;
+        for (int off = 16; off > 0; off >>= 1) {
+            pot += __shfl_xor_sync(0xffffffffu, pot, off);
+            ex += __shfl_xor_sync(0xffffffffu, ex, off);
+            ey += __shfl_xor_sync(0xffffffffu, ey, off);
+        }
+        if (lane == (it & 31)) {
+            i64 k = s0 + it;
+            double xi = T.pos[k], yi = T.pos[T.m + k];
+            double lp, lx, ly;
+            eval_local<LOCAL>(local_a, local_b, leaf, order, width, xi - T.center[2 * leaf],
+                              yi - T.center[2 * leaf + 1], lp, lx, ly);
+            i64 i = T.perm[k];
+            phi[i] = POT ? lp + pot : 0.0;
+            field[i] = lx + ex;
+            field[T.m + i] = ly + ey;
+        }
     }
 }
 
@@ -567,18 +592,22 @@ __global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg
     i64 leaf = seg_leaf[seg];
     i64 s0 = T.start[leaf];
     int count = (int)(T.end[leaf] - s0);
-    i64 last = seg;
-    while (last + 1 < n_seg && seg_leaf[last + 1] == leaf) ++last;
-    for (int it = lane; it < count; it += 32) {
+    i64 nseg = leaf_segments(seg_leaf, seg, n_seg, leaf, lane);
+    for (int it = 0; it < count; ++it) {
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (i64 s = seg; s <= last; ++s) {
+        for (i64 s = seg + lane; s < seg + nseg; s += 32) {
             i64 p = seg_out[s] + it;
             for (int c = 0; c < 6; ++c) acc[c] += partial[6 * p + c];
         }
-        i64 k = s0 + it;
-        adjoint_finish<LOCAL>(acc, k, T.perm[k], S.n, S.pos[k] - T.center[2 * leaf],
-                              S.pos[S.n + k] - T.center[2 * leaf + 1], leaf, order, width, fa, fb,
-                              ba, bb, S, A);
+        for (int c = 0; c < 6; ++c)
+            for (int off = 16; off > 0; off >>= 1)
+                acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
+        if (lane == (it & 31)) {
+            i64 k = s0 + it;
+            adjoint_finish<LOCAL>(acc, k, T.perm[k], S.n, S.pos[k] - T.center[2 * leaf],
+                                  S.pos[S.n + k] - T.center[2 * leaf + 1], leaf, order, width,
+                                  fa, fb, ba, bb, S, A);
+        }
     }
 }
 

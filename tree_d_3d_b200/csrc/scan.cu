@@ -103,11 +103,40 @@ __global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, i64 n
     }
 }
 
+// Arrays of one tile: the whole scan in one block, one launch.
+template <typename T>
+__global__ void k_single_tile_scan(const T* __restrict__ in, T* __restrict__ out, i64 n,
+                                   T* __restrict__ total_out) {
+    i64 base = (i64)threadIdx.x * SCAN_ITEMS;
+    T v[SCAN_ITEMS];
+    T s = 0;
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        i64 k = base + i;
+        v[i] = k < n ? in[k] : T(0);
+        s += v[i];
+    }
+    T total;
+    T off = block_exclusive(s, &total);
+#pragma unroll
+    for (int i = 0; i < SCAN_ITEMS; ++i) {
+        i64 k = base + i;
+        if (k < n) out[k] = off;
+        off += v[i];
+    }
+    if (threadIdx.x == 0 && total_out) *total_out = total;
+}
+
 template <typename T>
 int exclusive_scan(const T* in, T* out, i64 n, T* total, void* ws, size_t ws_bytes,
                    cudaStream_t stream) {
     if (n <= 0) {
         if (total) TD3_TRY(cudaMemsetAsync(total, 0, sizeof(T), stream));
+        return TD3_OK;
+    }
+    if (n <= SCAN_TILE) {
+        k_single_tile_scan<T><<<1, SCAN_THREADS, 0, stream>>>(in, out, n, total);
+        TD3_CHECK_LAUNCH();
         return TD3_OK;
     }
     i64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
