@@ -266,15 +266,13 @@ def time_m2l_mixed(tree, torch, reps):
     count, w = tree.node_count, tree.order + 1
     lre = torch.zeros((count, w), dtype=torch.float64, device=tree.device)
     lim = torch.zeros_like(lre)
-    hat = torch.empty((count, w, 2), dtype=torch.float32, device=tree.device)
+    hat = tree._scaled_moments((tree.moment_re, tree.moment_im))
     stream = _lib.stream(tree.device)
-    _lib.call("td3_scale_moments", count, tree.order, tree.moment_re.data_ptr(),
-              tree.moment_im.data_ptr(), tree.node_half.data_ptr(), hat.data_ptr(), stream)
     coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
     args = (lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(), count,
             tree.node_center.data_ptr(), tree.node_half.data_ptr(), tree.node_center.data_ptr(),
             tree.node_half.data_ptr(), hat.data_ptr(), tree.order, coeff.ctypes.data,
-            lre.data_ptr(), lim.data_ptr(), stream)
+            tree._unit, lre.data_ptr(), lim.data_ptr(), stream)
     _lib.call("td3_fmm_m2l_mixed", *args)
     cur = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

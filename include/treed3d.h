@@ -181,7 +181,10 @@ int td3_target_order(const double* targets, int64_t m, int64_t* order, void* wor
  * source exclude[i] for target i.  order (m, may be NULL) is the processing order of
  * the targets (warps take 32 consecutive ones).  tree_depth is the deepest node depth;
  * above 190 the call returns TD3_EDEPTH.  with_potential = 0 writes phi = 0 and skips
- * the log kernel's logarithms.
+ * the log kernel's logarithms.  mixed = 1 keeps the FP64 opening decisions and evaluates
+ * leaf pairs and far-field terms in FP32 with compensated sums; the log kernel then
+ * reads moment_hat (nodes, order_p + 1, 2) FP32, hat_k = a_k / h^k (td3_scale_moments)
+ * instead of moment_re / moment_im.  mixed = 0 ignores moment_hat (may be NULL).
  * Replaces evaluate_quadtree (src/tree_d_3d/kernels/evaluate_quadtree/
  * evaluate_quadtree_cuda.cu:9-107), evaluate_log_quadtree (kernels/evaluate_log_quadtree/
  * evaluate_log_quadtree_cuda.cu:9-104) and the CPU walk evaluate_groups
@@ -196,9 +199,10 @@ int td3_evaluate_quadtree(int kernel, const double* targets, int64_t m, const in
                           const int64_t* node_child, const int64_t* node_depth,
                           int64_t tree_depth, const double* node_q, const double* node_qabs,
                           const double* node_p, const double* node_s, const double* moment_re,
-                          const double* moment_im, int order_p, double theta, double softening,
-                          int with_potential, double* phi, double* field, int64_t* status,
-                          void* workspace, size_t workspace_bytes, void* stream);
+                          const double* moment_im, const float* moment_hat, int order_p,
+                          double theta, double softening, int with_potential, int mixed,
+                          double* phi, double* field, int64_t* status, void* workspace,
+                          size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------ FMM lists */
 
@@ -263,8 +267,10 @@ int td3_fmm_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst
  * order + 1) complex float pairs with hat_k = a_k / h^k (td3_scale_moments), translated
  * in FP32 with ws = h_src / t and wd = h_dst / t (|ws|, |wd| < 1 for separated cells):
  * s_l = sum_k coeff[k, l] hat_k ws^k, bhat_0 = a_0 ln|t| - s_0, bhat_l = -(-1)^l s_l wd^l,
- * and local_re / local_im (FP64) += bhat_l / h_dst^l.  coeff is a HOST (order + 1)^2
- * array (the reference's M2L matrix); order <= 20.  The FP32 counterpart of
+ * and local_re / local_im (FP64) += bhat_l / h_dst^l.  ln|t| is formed as ln|t / unit|
+ * in FP32 plus ln(unit) sum a_0 in FP64 (unit > 0: a length of the problem, e.g. the
+ * root half-width).  coeff is a HOST (order + 1)^2 array (the reference's M2L matrix);
+ * order <= 20.  The FP32 counterpart of
  * td3_fmm_m2l (reference: fmm_m2l_host, src/tree_d_3d/kernels/fmm_m2l_host/
  * fmm_m2l_host_pyccel.py:16-105). */
 int td3_scale_moments(int64_t count, int order, const double* moment_re,
@@ -272,7 +278,7 @@ int td3_scale_moments(int64_t count, int order, const double* moment_re,
 int td3_fmm_m2l_mixed(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
                       const double* dst_center, const double* dst_half, const double* src_center,
                       const double* src_half, const float* hat, int order, const double* coeff,
-                      double* local_re, double* local_im, void* stream);
+                      double unit, double* local_re, double* local_im, void* stream);
 
 /* L2L from the root down, level by level (levels HOST, n_levels + 1): every local
  * expansion shifted into its children, b_m(child) += sum_{l>=m} C(l, m) b_l s^(l-m).
@@ -332,8 +338,10 @@ int td3_nearfield_plan(const int64_t* rows, int64_t n_nodes, const int64_t* node
  * with_potential = 0); TD3_KERNEL_COULOMB: Cartesian local expansion local_a (nodes,
  * (order + 1)(order + 2)/2), softened Coulomb pairs.  A coincident pair of two nonzero
  * charges reports 1 + a particle index.  partial: 3 * partial length doubles.
- * mixed != 0: the pair arithmetic in FP32 (pair differences taken in FP64, then
- * rounded) with compensated (Kahan) accumulation; the local expansions in FP64.
+ * mixed != 0: the pair arithmetic in FP32 (pair differences taken in FP64, divided by
+ * `unit` > 0, a length of the problem such as the root half-width, then rounded) with
+ * compensated (Kahan) accumulation, rescaled in FP64 (the log kernel's ln unit^2 times
+ * the charge sum added in FP64); the local expansions in FP64.  mixed = 0 ignores unit.
  * Replaces fmm_evaluate_host (src/tree_d_3d/kernels/fmm_evaluate_host/
  * fmm_evaluate_host_pyccel.py:14-100), fmm_evaluate (kernels/fmm_evaluate/
  * fmm_evaluate_cuda.cu:11-87) and cart_evaluate_host (kernels/cart_evaluate_host/
@@ -344,14 +352,16 @@ int td3_fmm_evaluate(int kernel, const double* sorted_pos, const double* sorted_
                      const double* local_a, const double* local_b, const int64_t* p2p_partners,
                      const int* seg_leaf, const int64_t* seg_range, const int64_t* seg_out,
                      int64_t n_seg, double* partial, double softening, int with_potential,
-                     int mixed, double* phi, double* field, int64_t* status, void* stream);
+                     int mixed, double unit, double* phi, double* field, int64_t* status,
+                     void* stream);
 
 /* fmm_at: L2P at the m targets (sorted_targets (2, m) in target-tree order, target_perm
  * their input indices, sorted_exclude their excluded source index) plus exact sums over
  * the partner source leaves of each target leaf (the one-way P2P rows cut by
  * td3_nearfield_plan on the target tree) of the source tree (sorted_pos, sorted_charge,
  * perm, s_start, s_end), skipping zero charges and the excluded source; results at the
- * targets' input indices; a coincident charge reports 1 + the target index.  Replaces
+ * targets' input indices; a coincident charge reports 1 + the target index.  mixed and
+ * unit as in td3_fmm_evaluate.  Replaces
  * log_targets_host (src/tree_d_3d/kernels/log_targets_host/log_targets_host_pyccel.py:14-94)
  * and cart_targets_host (kernels/cart_targets_host/cart_targets_host_pyccel.py:16-98). */
 int td3_fmm_targets(int kernel, const double* sorted_targets, const int64_t* sorted_exclude,
@@ -362,8 +372,8 @@ int td3_fmm_targets(int kernel, const double* sorted_targets, const int64_t* sor
                     int64_t n_seg, double* partial, const double* sorted_pos,
                     const double* sorted_charge, const int64_t* perm, int64_t n,
                     const int64_t* s_start, const int64_t* s_end, double softening,
-                    int with_potential, int mixed, double* phi, double* field, int64_t* status,
-                    void* stream);
+                    int with_potential, int mixed, double unit, double* phi, double* field,
+                    int64_t* status, void* stream);
 
 /* ------------------------------------------------------------------ adjoint (backward) */
 
@@ -395,7 +405,8 @@ int td3_cart_moments_adjoint(const int64_t* levels, int64_t n_levels, const doub
  * sum_j q_j Hess G(x_k - x_j).  Far parts come from the adjoint local expansions
  * adj_a / adj_b (value and gradient) and the forward ones fwd_a / fwd_b (Hessian),
  * near parts pair by pair over the near-field plan (softened kernel; kernel as in
- * td3_fmm_evaluate).  partial: 6 * partial length doubles.  No reference counterpart. */
+ * td3_fmm_evaluate, mixed and unit too).  partial: 6 * partial length doubles.  No
+ * reference counterpart. */
 int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_charge,
                     const int64_t* perm, int64_t n, const double* node_center,
                     const int64_t* node_start, const int64_t* node_end, int order,
@@ -403,8 +414,8 @@ int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_c
                     const double* adj_b, const int64_t* p2p_partners, const int* seg_leaf,
                     const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
                     double* partial, const double* sorted_weight, const double* sorted_dipole,
-                    const double* efield, double softening, int mixed, double* qbar,
-                    double* xbar, void* stream);
+                    const double* efield, double softening, int mixed, double unit,
+                    double* qbar, double* xbar, void* stream);
 
 /* ------------------------------------------------------------------ utilities */
 

@@ -88,3 +88,49 @@ def test_mixed_backward_matches_fp64(kernel):
         grads[precision] = (Q.grad.cpu().numpy(), P.grad.cpu().numpy())
     assert relative(grads["mixed"][0], grads["fp64"][0]) < TOL
     assert relative(grads["mixed"][1], grads["fp64"][1]) < TOL
+
+
+@pytest.mark.parametrize("kernel,eps,scale", [("log", 0.0, 1.0), ("log", 1e-3, 1.0),
+                                              ("coulomb", 0.0, 1.0), ("coulomb", 1e-3, 1.0),
+                                              ("log", 0.0, 1e-12), ("coulomb", 0.0, 1e12)])
+def test_mixed_walk_matches_fp64_walk(kernel, eps, scale):
+    """The mixed Barnes-Hut walk takes the FP64 walk's cells (exact decisions) and its
+    field and potential agree with FP64 to 1e-6, also at length scales far from 1 (the
+    FP32 far-field terms are formed in units of the distance and the cell size)."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, synthetic
+
+    pos, q = synthetic.mixture8(200_000, seed=21)
+    P = torch.tensor(pos * scale, device="cuda")
+    Q = torch.tensor(q, device="cuda")
+    idx = torch.arange(200_000, device="cuda")
+    out = {}
+    for precision in ("fp64", "mixed"):
+        tree = FlatQuadtree(P, Q, Quad(0, 0, scale), kernel=kernel, order=12,
+                            precision=precision)
+        out[precision] = tree.evaluate(P, exclude=idx, theta=0.5, softening=eps * scale)
+    for comp in (0, 1):
+        assert relative(out["mixed"][comp].cpu().numpy(), out["fp64"][comp].cpu().numpy()) < TOL
+
+
+@pytest.mark.parametrize("kernel,scale", [("log", 1e-12), ("log", 1e9), ("coulomb", 1e-12)])
+def test_mixed_fmm_and_backward_at_extreme_length_scales(kernel, scale):
+    """The mixed FMM works in units of the root half-width: at length scales far from 1
+    its fields, potentials and gradients stay within 1e-6 of FP64."""
+    from tree_d_3d_b200 import Quad, synthetic
+    from tree_d_3d_b200.autograd import fmm_field
+
+    pos, q = synthetic.mixture8(100_000, seed=31)
+    rng = np.random.default_rng(32)
+    w = torch.tensor(rng.normal(size=pos.shape[1]), device="cuda")
+    e = torch.tensor(rng.normal(size=pos.shape), device="cuda")
+    eps = 1e-3 * scale if kernel == "coulomb" else 0.0
+    out = {}
+    for precision in ("fp64", "mixed"):
+        P = torch.tensor(pos * scale, device="cuda", requires_grad=True)
+        Q = torch.tensor(q, device="cuda", requires_grad=True)
+        phi, field = fmm_field(P, Q, Quad(0, 0, scale), kernel=kernel, order=12,
+                               softening=eps, precision=precision)
+        ((w * phi).sum() + (e * field).sum()).backward()
+        out[precision] = [t.detach().cpu().numpy() for t in (phi, field, Q.grad, P.grad)]
+    for a, b in zip(out["mixed"], out["fp64"]):
+        assert relative(a, b) < TOL

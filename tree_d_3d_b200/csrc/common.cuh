@@ -75,6 +75,27 @@ __device__ __forceinline__ double xnorm2(double rx, double ry) {
     return xadd(xmul(rx, rx), xmul(ry, ry));
 }
 
+// Compensated (Kahan) FP32 sum of the mixed-precision kernels: the running error c is
+// subtracted from each new term; value() returns the sum in FP64.
+struct KahanF {
+    float s = 0.0f, c = 0.0f;
+    __device__ __forceinline__ void add(float x) {
+        float y = x - c;
+        float t = s + y;
+        c = (t - s) - y;
+        s = t;
+    }
+    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// ln(x) for x > 0 of any FP64 magnitude in FP32 arithmetic: x = f 2^e with f in [0.5, 1)
+// (frexp, exact), ln x = ln f + e ln 2.
+__device__ __forceinline__ float log_split(double x) {
+    int e;
+    double f = frexp(x, &e);
+    return __logf((float)f) + (float)e * 0.693147180559945309f;
+}
+
 // sqrt(2.0) correctly rounded, the `root2` of the traversal predicates.
 #define TD3_ROOT2 1.4142135623730951
 

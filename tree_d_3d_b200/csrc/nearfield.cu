@@ -181,6 +181,7 @@ struct Sources {
     const i64* start;
     const i64* end;
     i64 n;
+    double unit;  // length unit L of the mixed-precision pair arithmetic
 };
 
 struct Targets {
@@ -193,28 +194,19 @@ struct Targets {
     i64 m;
 };
 
-// Compensated (Kahan) FP32 sum: the running error c is subtracted from each new term.
-struct KahanF {
-    float s = 0.0f, c = 0.0f;
-    __device__ __forceinline__ void add(float x) {
-        float y = x - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
-};
-
 // The mixed-precision near field of one target over a run of partner leaves: the pair
-// difference in FP64 (exact enough for close pairs far from the origin), rounded to
-// FP32, then FP32 kernel arithmetic with compensated accumulation.
+// difference in FP64 (exact enough for close pairs far from the origin), in units of
+// S.unit = L and rounded to FP32, then FP32 kernel arithmetic with compensated
+// accumulation.  Coulomb: phi = sum q / r' / L, E = sum q d' / r'^3 / L^2; log:
+// phi = sum -q ln r'^2 - ln L^2 sum q (the charge sum in FP64), E = sum 2 q d' / r'^2 / L.
 template <int KERNEL, bool POT, bool OTHER>
 __device__ __forceinline__ void near_mixed(const Sources& S, const i64* __restrict__ partners,
                                            i64 e_begin, i64 e_end, int step, double xi, double yi,
                                            double qi, i64 k, i64 skip, double eps2, double& pot,
                                            double& ex, double& ey, bool& bad) {
     KahanF p, x, y;
-    float eps2f = (float)eps2;
+    double inv_unit = 1.0 / S.unit, qsum = 0.0;
+    float eps2f = (float)(eps2 * inv_unit * inv_unit);
     for (i64 e = e_begin; e < e_end; e += step) {
         i64 b = partners[e];
         i64 b1 = S.end[b];
@@ -230,10 +222,13 @@ __device__ __forceinline__ void near_mixed(const Sources& S, const i64* __restri
                 bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
                 continue;
             }
-            float dx = (float)dx64, dy = (float)dy64, q = (float)qj;
+            float dx = (float)(dx64 * inv_unit), dy = (float)(dy64 * inv_unit), q = (float)qj;
             float r2 = dx * dx + dy * dy + eps2f;
             if (KERNEL == TD3_KERNEL_LOG) {
-                if (POT) p.add(-q * __logf(r2));
+                if (POT) {
+                    p.add(-q * __logf(r2));
+                    qsum += qj;
+                }
                 float f = __fdividef(2.0f * q, r2);
                 x.add(f * dx);
                 y.add(f * dy);
@@ -246,9 +241,15 @@ __device__ __forceinline__ void near_mixed(const Sources& S, const i64* __restri
             }
         }
     }
-    pot = p.value();
-    ex = x.value();
-    ey = y.value();
+    if (KERNEL == TD3_KERNEL_LOG) {
+        pot = p.value() - 2.0 * log(S.unit) * qsum;
+        ex = x.value() * inv_unit;
+        ey = y.value() * inv_unit;
+    } else {
+        pot = p.value() * inv_unit;
+        ex = x.value() * inv_unit * inv_unit;
+        ey = y.value() * inv_unit * inv_unit;
+    }
 }
 
 // One warp per segment.  OTHER: targets and sources are different point sets (fmm_at):
@@ -532,8 +533,12 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
         double xi = S.pos[k], yi = S.pos[n + k];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         if (valid && MIXED) {
+            // in units of L = S.unit (d' = d / L, e' = e / L): the log kernel's sums scale
+            // as (1, 1/L, 1/L^2) plus -ln L^2 sum w for Psi, the Coulomb kernel's as
+            // (1/L, 1/L^2, 1/L^3)
             KahanF kacc[6];
-            float eps2f = (float)eps2;
+            double inv_unit = 1.0 / S.unit, wsum = 0.0;
+            float eps2f = (float)(eps2 * inv_unit * inv_unit);
             for (i64 e = er.x + slice; e < er.y; e += slices) {
                 i64 b = partners[e];
                 i64 b1 = S.end[b];
@@ -541,12 +546,19 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
                     if (j == k) continue;
                     double dx = xi - S.pos[j], dy = yi - S.pos[n + j];
                     if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) continue;
-                    adjoint_pair_mixed<KERNEL>((float)dx, (float)dy, eps2f, (float)S.charge[j],
-                                               (float)A.weight[j], (float)A.dipole[j],
-                                               (float)A.dipole[n + j], kacc);
+                    double wj = A.weight[j];
+                    if (KERNEL == TD3_KERNEL_LOG) wsum += wj;
+                    adjoint_pair_mixed<KERNEL>(
+                        (float)(dx * inv_unit), (float)(dy * inv_unit), eps2f, (float)S.charge[j],
+                        (float)wj, (float)(A.dipole[j] * inv_unit),
+                        (float)(A.dipole[n + j] * inv_unit), kacc);
                 }
             }
-            for (int c = 0; c < 6; ++c) acc[c] = kacc[c].value();
+            double s0 = KERNEL == TD3_KERNEL_LOG ? 1.0 : inv_unit;
+            acc[0] = kacc[0].value() * s0;
+            if (KERNEL == TD3_KERNEL_LOG) acc[0] -= 2.0 * log(S.unit) * wsum;
+            for (int c = 1; c < 3; ++c) acc[c] = kacc[c].value() * (s0 * inv_unit);
+            for (int c = 3; c < 6; ++c) acc[c] = kacc[c].value() * (s0 * inv_unit * inv_unit);
         } else if (valid) {
             for (i64 e = er.x + slice; e < er.y; e += slices) {
                 i64 b = partners[e];
@@ -710,13 +722,15 @@ extern "C" int td3_fmm_evaluate(int kernel, const double* sorted_pos, const doub
                                 const int64_t* p2p_partners, const int* seg_leaf,
                                 const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
                                 double* partial, double softening, int with_potential, int mixed,
-                                double* phi, double* field, int64_t* status, void* stream) {
+                                double unit, double* phi, double* field, int64_t* status,
+                                void* stream) {
     if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (mixed && !(unit > 0.0 && unit < INFINITY)) return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
     if (n == 0) return TD3_OK;
     bool lg = kernel == TD3_KERNEL_LOG;
     NearArgs a{Targets{sorted_pos, nullptr, perm, node_center, node_start, node_end, n},
-               Sources{sorted_pos, sorted_charge, perm, node_start, node_end, n},
+               Sources{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit},
                n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
                p2p_partners, local_a, local_b, order,
                lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,
@@ -748,13 +762,14 @@ extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const doubl
                                const int* seg_leaf, const int64_t* seg_range,
                                const int64_t* seg_out, int64_t n_seg, double* partial,
                                const double* sorted_weight, const double* sorted_dipole,
-                               const double* efield, double softening, int mixed, double* qbar,
-                               double* xbar, void* stream) {
+                               const double* efield, double softening, int mixed, double unit,
+                               double* qbar, double* xbar, void* stream) {
     if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (mixed && !(unit > 0.0 && unit < INFINITY)) return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
     if (n == 0 || n_seg == 0) return TD3_OK;
     Targets T{sorted_pos, nullptr, perm, node_center, node_start, node_end, n};
-    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n};
+    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit};
     Adjoint A{sorted_weight, sorted_dipole, efield, qbar, xbar};
     double eps2 = softening * softening;
     cudaStream_t s = td3_stream(stream);
@@ -797,14 +812,15 @@ extern "C" int td3_fmm_targets(int kernel, const double* sorted_targets,
                                const double* sorted_pos, const double* sorted_charge,
                                const int64_t* perm, int64_t n, const int64_t* s_start,
                                const int64_t* s_end, double softening, int with_potential,
-                               int mixed, double* phi, double* field, int64_t* status,
-                               void* stream) {
+                               int mixed, double unit, double* phi, double* field,
+                               int64_t* status, void* stream) {
     if (m < 0 || n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (mixed && !(unit > 0.0 && unit < INFINITY)) return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
     if (m == 0) return TD3_OK;
     bool lg = kernel == TD3_KERNEL_LOG;
     NearArgs a{Targets{sorted_targets, sorted_exclude, target_perm, t_center, t_start, t_end, m},
-               Sources{sorted_pos, sorted_charge, perm, s_start, s_end, n},
+               Sources{sorted_pos, sorted_charge, perm, s_start, s_end, n, unit},
                n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
                p2p_partners, local_a, local_b, order,
                lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,

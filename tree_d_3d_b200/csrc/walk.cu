@@ -83,7 +83,12 @@ __device__ __forceinline__ bool inside_cell(double tx, double ty, double cx, dou
     return tx >= xsub(cx, h) && tx <= xadd(cx, h) && ty >= xsub(cy, h) && ty <= xadd(cy, h);
 }
 
-template <bool POT>
+// The mixed-precision form of the walk (MIXED): the opening decisions are the exactly
+// rounded FP64 tests of the FP64 form, so every target takes the same terms; a leaf pair
+// forms its difference in FP64 and the kernel in FP32, and a far-field term is evaluated
+// in FP32 in units of the distance (Coulomb) or on size-scaled moments (log) so no FP32
+// intermediate under- or overflows for small cells.  Terms go into compensated FP32 sums.
+template <bool POT, bool MIXED>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_coulomb(const double* __restrict__ targets, i64 m, const i64* __restrict__ exclude,
                const i64* __restrict__ order, const double* __restrict__ spos,
@@ -99,6 +104,11 @@ k_walk_coulomb(const double* __restrict__ targets, i64 m, const i64* __restrict_
     double tx = valid ? targets[i] : 0.0, ty = valid ? targets[m + i] : 0.0;
     i64 skip = valid ? exclude[i] : -2;
     double pot = 0.0, ex = 0.0, ey = 0.0;
+    // MIXED: lengths in units of the root half-width L (FP32 terms O(1) at any scale);
+    // the sums are q / r' and q d' / r'^3, so phi = sum / L and E = sum / L^2.
+    KahanF kp, kx, ky;
+    double unit = nodes[2], inv_unit = 1.0 / unit;
+    float eps2f = (float)(eps2 * inv_unit * inv_unit);
     bool bad = false;
     unsigned* mk = masks[wib];
     unsigned active = __ballot_sync(0xffffffffu, valid);
@@ -124,6 +134,20 @@ k_walk_coulomb(const double* __restrict__ targets, i64 m, const i64* __restrict_
                     if (c == 0.0 || sindex[k] == skip) continue;
                     double dx = tx - spos[k];
                     double dy = ty - spos[n + k];
+                    if constexpr (MIXED) {
+                        if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) {
+                            bad = true;
+                            break;
+                        }
+                        float fx = (float)(dx * inv_unit), fy = (float)(dy * inv_unit);
+                        float qf = (float)c;
+                        float ir = rsqrtf(fmaf(fx, fx, fmaf(fy, fy, eps2f)));
+                        float qr3 = qf * ir * ir * ir;
+                        if (POT) kp.add(qf * ir);
+                        kx.add(qr3 * fx);
+                        ky.add(qr3 * fy);
+                        continue;
+                    }
                     double r2 = dx * dx + dy * dy + eps2;
                     if (r2 == 0.0) {
                         bad = true;
@@ -143,9 +167,30 @@ k_walk_coulomb(const double* __restrict__ targets, i64 m, const i64* __restrict_
         if (in) {
             double cx = c01.x, cy = c01.y, h = c23.x;
             double rx = xsub(tx, cx), ry = xsub(ty, cy);
-            double distance = xsqrt(xnorm2(rx, ry));
+            double d2 = xnorm2(rx, ry);
+            double distance = xsqrt(d2);
             if (!inside_cell(tx, ty, cx, cy, h) && xmul(2.0, h) < xmul(theta, distance)) {
-                if (!bad) {
+                if (!bad && MIXED) {
+                    // u = r / rho, p^ = p / rho, S^ = S / rho^2 (rho^2 = |r|^2 + eps^2):
+                    // phi = [q + p^.u + (3 u.S^u - tr S^) / 2] / rho and
+                    // E = [(q + 3 p^.u + 7.5 u.S^u - 1.5 tr S^) u - p^ - 3 S^u] / rho^2.
+                    double2 q45 = *reinterpret_cast<const double2*>(nd + 4);
+                    double2 q67 = *reinterpret_cast<const double2*>(nd + 6);
+                    double2 q89 = *reinterpret_cast<const double2*>(nd + 8);
+                    double ir = rsqrt(d2 + eps2), ir2 = ir * ir;
+                    float ux = (float)(rx * ir), uy = (float)(ry * ir);
+                    float q = (float)q45.x, px = (float)(q45.y * ir), py = (float)(q67.x * ir);
+                    float sxx = (float)(q67.y * ir2), sxy = (float)(q89.x * ir2),
+                          syy = (float)(q89.y * ir2);
+                    float pr = fmaf(px, ux, py * uy);
+                    float srx = fmaf(sxx, ux, sxy * uy), sry = fmaf(sxy, ux, syy * uy);
+                    float rsr = fmaf(ux, srx, uy * sry), trace = sxx + syy;
+                    double iru = ir * unit;  // 1 / rho in units of L
+                    if (POT) kp.add((float)((double)(q + pr + 0.5f * fmaf(3.0f, rsr, -trace)) * iru));
+                    float radial = q + 3.0f * pr + 7.5f * rsr - 1.5f * trace;
+                    kx.add((float)((double)(fmaf(radial, ux, -px) - 3.0f * srx) * (iru * iru)));
+                    ky.add((float)((double)(fmaf(radial, uy, -py) - 3.0f * sry) * (iru * iru)));
+                } else if (!bad) {
                     double2 q45 = *reinterpret_cast<const double2*>(nd + 4);
                     double2 q67 = *reinterpret_cast<const double2*>(nd + 6);
                     double2 q89 = *reinterpret_cast<const double2*>(nd + 8);
@@ -182,23 +227,35 @@ k_walk_coulomb(const double* __restrict__ targets, i64 m, const i64* __restrict_
     }
     if (!valid) return;
     if (bad) td3_report(status, i + 1);
+    if constexpr (MIXED) {
+        pot = kp.value() * inv_unit;
+        ex = kx.value() * inv_unit * inv_unit;
+        ey = ky.value() * inv_unit * inv_unit;
+    }
     phi[i] = POT ? pot : 0.0;
     field[i] = ex;
     field[m + i] = ey;
 }
 
-template <bool POT>
+// hat (MIXED only): the moments scaled by the cell size, hat_k = a_k / h^k as FP32 pairs,
+// (order_p + 1) per node.
+template <bool POT, bool MIXED>
 __global__ void __launch_bounds__(WALK_THREADS)
 k_walk_log(const double* __restrict__ targets, i64 m, const i64* __restrict__ exclude,
            const i64* __restrict__ order, const double* __restrict__ spos,
            const double* __restrict__ scharge, const i64* __restrict__ sindex, i64 n,
            const double4* __restrict__ geom, const int4* __restrict__ links,
            const int* __restrict__ depth, const double* __restrict__ moment_re,
-           const double* __restrict__ moment_im, int order_p, double theta, double eps2,
-           double* __restrict__ phi, double* __restrict__ field, i64* status) {
+           const double* __restrict__ moment_im, const float2* __restrict__ hat, int order_p,
+           double theta, double eps2, double* __restrict__ phi, double* __restrict__ field,
+           i64* status) {
     __shared__ unsigned masks[WALK_WARPS][MAX_DEPTH_WALK + 2];
     __shared__ double inv_n[TD3_MAX_ORDER + 1];
-    for (int k = threadIdx.x; k <= order_p; k += blockDim.x) inv_n[k] = k ? 1.0 / k : 0.0;
+    __shared__ float inv_nf[TD3_MAX_ORDER + 1];
+    for (int k = threadIdx.x; k <= order_p; k += blockDim.x) {
+        inv_n[k] = k ? 1.0 / k : 0.0;
+        inv_nf[k] = (float)inv_n[k];
+    }
     __syncthreads();
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     i64 t = ((i64)blockIdx.x * WALK_WARPS + wib) * 32 + lane;
@@ -207,6 +264,12 @@ k_walk_log(const double* __restrict__ targets, i64 m, const i64* __restrict__ ex
     double tx = valid ? targets[i] : 0.0, ty = valid ? targets[m + i] : 0.0;
     i64 skip = valid ? exclude[i] : -2;
     double pot = 0.0, ex = 0.0, ey = 0.0;
+    // MIXED: lengths in units of the root half-width L: -q ln r^2 = -q ln r'^2 - q ln L^2,
+    // the first summed in FP32, the charges of the second (qsum) in FP64; E = sum / L.
+    KahanF kp, kx, ky;
+    double unit = geom[0].z, inv_unit = 1.0 / unit, inv_unit2 = inv_unit * inv_unit;
+    double qsum = 0.0;
+    float eps2f = (float)(eps2 * inv_unit2);
     bool bad = false;
     unsigned* mk = masks[wib];
     unsigned active = __ballot_sync(0xffffffffu, valid);
@@ -232,6 +295,23 @@ k_walk_log(const double* __restrict__ targets, i64 m, const i64* __restrict__ ex
                     if (c == 0.0 || sindex[k] == skip) continue;
                     double dx = tx - spos[k];
                     double dy = ty - spos[n + k];
+                    if constexpr (MIXED) {
+                        if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) {
+                            bad = true;
+                            break;
+                        }
+                        float fx = (float)(dx * inv_unit), fy = (float)(dy * inv_unit);
+                        float qf = (float)c;
+                        float r2 = fmaf(fx, fx, fmaf(fy, fy, eps2f));
+                        if (POT) {
+                            kp.add(-qf * __logf(r2));
+                            qsum += c;
+                        }
+                        float f = __fdividef(2.0f * qf, r2);
+                        kx.add(f * fx);
+                        ky.add(f * fy);
+                        continue;
+                    }
                     double r2 = dx * dx + dy * dy + eps2;
                     if (r2 == 0.0) {
                         bad = true;
@@ -251,7 +331,41 @@ k_walk_log(const double* __restrict__ targets, i64 m, const i64* __restrict__ ex
             double rx = xsub(tx, g.x), ry = xsub(ty, g.y);
             double d2 = xnorm2(rx, ry);
             if (!inside_cell(tx, ty, g.x, g.y, g.z) && xmul(xmul(4.0, g.z), g.z) < xmul(theta2, d2)) {
-                if (!bad) {
+                if (!bad && MIXED) {
+                    // w = 1 / conj(r) = (rx, -ry) / |r|^2 and w^ = h w (|w^| < theta / 2):
+                    // sum_k a_k w^(k+1) = w sum_k hat_k w^^k and sum_k a_k w^k / k =
+                    // sum_k hat_k w^^k / k, both by Horner's rule from the highest order.
+                    double inv_d2 = 1.0 / d2;
+                    double wr64 = rx * inv_d2, wi64 = -ry * inv_d2;
+                    float wr = (float)(wr64 * g.z), wi = (float)(wi64 * g.z);
+                    wr64 *= unit;  // w in units of 1 / L
+                    wi64 *= unit;
+                    const float2* a = hat + (i64)node * w;
+                    float2 top = a[order_p];
+                    float gr = top.x, gi = top.y;
+                    float sr = top.x * inv_nf[order_p], si = top.y * inv_nf[order_p];
+                    for (int k = order_p - 1; k >= 0; --k) {
+                        float2 ak = a[k];
+                        float nr = fmaf(gr, wr, fmaf(-gi, wi, ak.x));
+                        gi = fmaf(gr, wi, fmaf(gi, wr, ak.y));
+                        gr = nr;
+                        if (POT) {
+                            float sk = k ? inv_nf[k] : 0.0f;
+                            float mr = fmaf(sr, wr, fmaf(-si, wi, ak.x * sk));
+                            si = fmaf(sr, wi, fmaf(si, wr, ak.y * sk));
+                            sr = mr;
+                        }
+                    }
+                    // after the k = 0 step s holds sum_{k>=1} hat_k w^^k / k (+ 0 w^^0)
+                    float fr = (float)wr64, fi = (float)wi64;
+                    float er = fmaf(fr, gr, -fi * gi), ei = fmaf(fr, gi, fi * gr);
+                    if (POT) {
+                        kp.add(fmaf(-a[0].x, log_split(d2 * inv_unit2), 2.0f * sr));
+                        qsum += moment_re[(i64)node * w];
+                    }
+                    kx.add(2.0f * er);
+                    ky.add(-2.0f * ei);
+                } else if (!bad) {
                     double inv_d2 = 1.0 / d2;
                     double w_re = rx * inv_d2, w_im = -ry * inv_d2;
                     double prev_re = 1.0, prev_im = 0.0, cur_re = w_re, cur_im = w_im;
@@ -288,9 +402,37 @@ k_walk_log(const double* __restrict__ targets, i64 m, const i64* __restrict__ ex
     }
     if (!valid) return;
     if (bad) td3_report(status, i + 1);
+    if constexpr (MIXED) {
+        pot = kp.value() - 2.0 * log(unit) * qsum;
+        ex = kx.value() * inv_unit;
+        ey = ky.value() * inv_unit;
+    }
     phi[i] = POT ? pot : 0.0;
     field[i] = ex;
     field[m + i] = ey;
+}
+
+template <bool POT, bool MIXED>
+void launch_walk_coulomb(unsigned blocks, cudaStream_t s, const double* targets, i64 m,
+                         const i64* exclude, const i64* order, const double* spos,
+                         const double* scharge, const i64* sindex, i64 n, const double* nodes,
+                         const int4* links, const int* depth, double theta, double eps2,
+                         double* phi, double* field, i64* status) {
+    k_walk_coulomb<POT, MIXED><<<blocks, WALK_THREADS, 0, s>>>(
+        targets, m, exclude, order, spos, scharge, sindex, n, nodes, links, depth, theta, eps2, phi,
+        field, status);
+}
+
+template <bool POT, bool MIXED>
+void launch_walk_log(unsigned blocks, cudaStream_t s, const double* targets, i64 m,
+                     const i64* exclude, const i64* order, const double* spos,
+                     const double* scharge, const i64* sindex, i64 n, const double4* geom,
+                     const int4* links, const int* depth, const double* moment_re,
+                     const double* moment_im, const float2* hat, int order_p, double theta,
+                     double eps2, double* phi, double* field, i64* status) {
+    k_walk_log<POT, MIXED><<<blocks, WALK_THREADS, 0, s>>>(
+        targets, m, exclude, order, spos, scharge, sindex, n, geom, links, depth, moment_re,
+        moment_im, hat, order_p, theta, eps2, phi, field, status);
 }
 
 // ------------------------------------------------------------------ target order
@@ -405,14 +547,15 @@ extern "C" int td3_evaluate_quadtree(int kernel, const double* targets, int64_t 
                                      int64_t tree_depth, const double* node_q, const double* node_qabs,
                                      const double* node_p, const double* node_s,
                                      const double* moment_re, const double* moment_im,
-                                     int order_p, double theta, double softening,
-                                     int with_potential, double* phi, double* field,
-                                     int64_t* status, void* workspace, size_t workspace_bytes,
-                                     void* stream) {
+                                     const float* moment_hat, int order_p, double theta,
+                                     double softening, int with_potential, int mixed, double* phi,
+                                     double* field, int64_t* status, void* workspace,
+                                     size_t workspace_bytes, void* stream) {
     if (m < 0 || n < 0 || node_count < 1 || node_count > 0x7fffffffLL || n > 0x7fffffffLL)
         return TD3_EINVAL;
     if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
     if (kernel == TD3_KERNEL_LOG && (order_p < 0 || order_p > TD3_MAX_ORDER)) return TD3_EINVAL;
+    if (kernel == TD3_KERNEL_LOG && mixed && !moment_hat) return TD3_EINVAL;
     if (tree_depth < 0) return TD3_EINVAL;
     if (tree_depth > MAX_DEPTH_WALK) return TD3_EDEPTH;
     if (m == 0) return TD3_OK;
@@ -434,27 +577,21 @@ extern "C" int td3_evaluate_quadtree(int kernel, const double* targets, int64_t 
         double* pk = static_cast<double*>(packed);
         k_pack_coulomb<<<nb, 256, 0, s>>>(node_count, node_center, node_half, node_qabs, node_q,
                                           node_p, node_s, pk);
-        if (with_potential)
-            k_walk_coulomb<true><<<tb, WALK_THREADS, 0, s>>>(targets, m, exclude, order, sorted_pos,
-                                                            sorted_charge, perm, n, pk, links, depth,
-                                                            theta, eps2, phi, field, status);
-        else
-            k_walk_coulomb<false><<<tb, WALK_THREADS, 0, s>>>(targets, m, exclude, order, sorted_pos,
-                                                             sorted_charge, perm, n, pk, links, depth,
-                                                             theta, eps2, phi, field, status);
+        auto go = with_potential ? (mixed ? launch_walk_coulomb<true, true>
+                                          : launch_walk_coulomb<true, false>)
+                                 : (mixed ? launch_walk_coulomb<false, true>
+                                          : launch_walk_coulomb<false, false>);
+        go(tb, s, targets, m, exclude, order, sorted_pos, sorted_charge, perm, n, pk, links, depth,
+           theta, eps2, phi, field, status);
     } else {
         double4* g = static_cast<double4*>(packed);
         k_pack_geometry<<<nb, 256, 0, s>>>(node_count, node_center, node_half, node_qabs, g);
-        if (with_potential)
-            k_walk_log<true><<<tb, WALK_THREADS, 0, s>>>(targets, m, exclude, order, sorted_pos,
-                                                        sorted_charge, perm, n, g, links, depth,
-                                                        moment_re, moment_im, order_p, theta, eps2,
-                                                        phi, field, status);
-        else
-            k_walk_log<false><<<tb, WALK_THREADS, 0, s>>>(targets, m, exclude, order, sorted_pos,
-                                                         sorted_charge, perm, n, g, links, depth,
-                                                         moment_re, moment_im, order_p, theta, eps2,
-                                                         phi, field, status);
+        auto go = with_potential ? (mixed ? launch_walk_log<true, true> : launch_walk_log<true, false>)
+                                 : (mixed ? launch_walk_log<false, true>
+                                          : launch_walk_log<false, false>);
+        go(tb, s, targets, m, exclude, order, sorted_pos, sorted_charge, perm, n, g, links, depth,
+           moment_re, moment_im, reinterpret_cast<const float2*>(moment_hat), order_p, theta, eps2,
+           phi, field, status);
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;

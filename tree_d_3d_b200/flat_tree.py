@@ -212,7 +212,9 @@ class FlatQuadtree:
     (2, N) and ``charges`` (N,) are copied.  ``kernel="coulomb"`` keeps signed moments
     through the quadrupole, ``kernel="log"`` complex multipole expansions of ``order``
     terms.  ``comm`` (MPI sharing of the moments) is not supported: one GPU holds the
-    whole tree.  ``precision="mixed"`` selects the mixed-precision FMM.
+    whole tree.  ``precision="mixed"`` selects the mixed-precision forms of the FMM and
+    of the Barnes-Hut walk: the same cells and pairs as FP64, near pairs and far-field
+    terms in FP32 with compensated sums, M2M/L2L and the results in FP64.
     """
 
     def __init__(self, positions, charges, root_quad: Quad, *, leaf_capacity: int = 8,
@@ -448,6 +450,9 @@ class FlatQuadtree:
         kernel = _kernel_code(self.kernel)
         ws = _lib.workspace(_lib.query("td3_walk_workspace_size", self.node_count, kernel),
                             self.device)
+        hat = None
+        if self._mixed and self.kernel == "log":
+            hat = self._scaled_moments((self.moment_re, self.moment_im))
         _lib.call(
             "td3_evaluate_quadtree", kernel, targets.data_ptr(), m, exclude.data_ptr(),
             order.data_ptr(), self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
@@ -456,9 +461,9 @@ class FlatQuadtree:
             self.node_child.data_ptr(), self.node_depth.data_ptr(), self.tree_depth,
             self.node_q.data_ptr(), self.node_qabs.data_ptr(), self.node_p.data_ptr(),
             self.node_s.data_ptr(), self.moment_re.data_ptr(), self.moment_im.data_ptr(),
-            self.order, float(theta), float(softening), 1 if potential else 0,
-            phi.data_ptr(), field.data_ptr(), status.data_ptr(), ws.data_ptr(), ws.numel(),
-            _lib.stream(self.device),
+            0 if hat is None else hat.data_ptr(), self.order, float(theta), float(softening),
+            1 if potential else 0, self._mixed, phi.data_ptr(), field.data_ptr(),
+            status.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream(self.device),
         )
 
     def evaluate(self, targets, *, exclude=None, theta=0.5, softening=0.0, potential=True):
@@ -621,11 +626,27 @@ class FlatQuadtree:
             local_b.data_ptr(), lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
             plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
             plan["partial"].data_ptr(), float(softening), 1 if potential else 0, self._mixed,
+            self._unit,
             phi.data_ptr(), field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
 
     @property
     def _mixed(self) -> int:
         return 1 if self.precision == "mixed" else 0
+
+    @property
+    def _unit(self) -> float:
+        """The length unit of the mixed-precision kernels: the root half-width."""
+        return self.root_quad.half
+
+    def _scaled_moments(self, moments):
+        """FP32 moments scaled by the cell size, hat_k = a_k / h^k (nodes, order + 1, 2)."""
+        mre, mim = moments
+        hat = torch.empty((self.node_count, self.order + 1, 2), dtype=torch.float32,
+                          device=self.device)
+        _lib.call("td3_scale_moments", self.node_count, self.order, mre.data_ptr(),
+                  mim.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(),
+                  _lib.stream(self.device))
+        return hat
 
     def _m2l_log(self, rows, partners, dst, moments, local_re, local_im):
         """Log-kernel M2L from this tree's cells into ``dst``'s: FP64, or FP32 on moments
@@ -633,16 +654,13 @@ class FlatQuadtree:
         stream = _lib.stream(self.device)
         mre, mim = moments
         if self.precision == "mixed" and self.order <= 20:
-            hat = torch.empty((self.node_count, self.order + 1, 2), dtype=torch.float32,
-                              device=self.device)
-            _lib.call("td3_scale_moments", self.node_count, self.order, mre.data_ptr(),
-                      mim.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(), stream)
+            hat = self._scaled_moments(moments)
             coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
             _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                       dst.node_center.data_ptr(), dst.node_half.data_ptr(),
                       self.node_center.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(),
-                      self.order, coeff.ctypes.data, local_re.data_ptr(), local_im.data_ptr(),
-                      stream)
+                      self.order, coeff.ctypes.data, self._unit, local_re.data_ptr(),
+                      local_im.data_ptr(), stream)
             return
         _lib.call("td3_fmm_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                   dst.node_center.data_ptr(), self.node_center.data_ptr(), mre.data_ptr(),
@@ -710,7 +728,8 @@ class FlatQuadtree:
                   adj_b.data_ptr(), lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
                   plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
                   partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), efield.data_ptr(),
-                  float(softening), self._mixed, qbar.data_ptr(), xbar.data_ptr(), stream)
+                  float(softening), self._mixed, self._unit, qbar.data_ptr(), xbar.data_ptr(),
+                  stream)
         return qbar, xbar
 
     def _move_within_cells(self, positions) -> None:
@@ -842,6 +861,7 @@ class FlatQuadtree:
             plan["partial"].data_ptr(), self._sorted_pos.data_ptr(),
             self._sorted_charge.data_ptr(), self.perm.data_ptr(), n, self.node_start.data_ptr(),
             self.node_end.data_ptr(), float(softening), 1 if with_pot else 0, self._mixed,
+            self._unit,
             phi.data_ptr(), field.data_ptr(), status.data_ptr(), stream)
         _check(status)
         if not potential:
