@@ -240,7 +240,8 @@ int td3_dual_traverse(const double* t_center, const double* t_half, const int64_
                       int64_t* sizes, void* workspace, size_t workspace_bytes, void* stream);
 
 /* Rows by node of the pairs (count, 2): row_start (n_nodes + 1) and partners, in pair
- * order; mutual != 0 lists b under a and a under b (once if a == b).  Replaces pair_csr
+ * order; mutual != 0 lists b under a and a under b (once if a == b).  partners holds
+ * count (mutual: 2 count) slots; those past row_start[n_nodes] are scratch.  Replaces pair_csr
  * (src/tree_d_3d/kernels/pair_csr/pair_csr_pyccel.py:12-45); identical rows. */
 size_t td3_pair_csr_workspace_size(int64_t count, int mutual, int64_t n_nodes);
 int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int64_t n_nodes,

@@ -139,6 +139,3 @@ size_t td3_sort_workspace(i64 n);
 int td3_radix_sort_u32(unsigned* keys, unsigned* keys_alt, unsigned* vals, unsigned* vals_alt,
                        i64 n, int bits, unsigned** keys_out, unsigned** vals_out, void* ws,
                        size_t ws_bytes, cudaStream_t stream);
-int td3_radix_sort_u64(unsigned long long* keys, unsigned long long* keys_alt, unsigned* vals,
-                       unsigned* vals_alt, i64 n, int bits, unsigned long long** keys_out,
-                       unsigned** vals_out, void* ws, size_t ws_bytes, cudaStream_t stream);

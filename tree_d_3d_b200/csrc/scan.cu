@@ -150,100 +150,118 @@ int exclusive_scan(const T* in, T* out, i64 n, T* total, void* ws, size_t ws_byt
 }
 
 // ------------------------------------------------------------------- radix sort
+// Stable LSD radix sort of uint32 keys with uint32 values, 8-bit digits.  A pass is a
+// per-tile digit histogram, an exclusive scan of the (digit-major) histograms, and a
+// scatter.  A tile is 8 warps x 512 consecutive items; a warp ranks its items round by
+// round (32 consecutive items per round) with __match_any_sync, so equal digits keep
+// input order; the tile is then reordered by digit in shared memory and written out in
+// runs of equal digits (coalesced stores).
 constexpr int SORT_THREADS = 256;
-constexpr int SORT_ITEMS = 8;
+constexpr int SORT_WARPS = SORT_THREADS / 32;
+constexpr int SORT_ITEMS = 16;
+constexpr int WARP_ITEMS = 32 * SORT_ITEMS;
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
-constexpr int RADIX_BITS = 4;
+constexpr int RADIX_BITS = 8;
 constexpr int RADIX = 1 << RADIX_BITS;
+static_assert(RADIX == SORT_THREADS, "one thread per digit in the tile totals");
 
-template <typename K>
-__global__ void k_sort_hist(const K* __restrict__ keys, i64 n, int shift, int n_tiles,
-                            int* __restrict__ hist) {
-    __shared__ int counts[RADIX];
-    if (threadIdx.x < RADIX) counts[threadIdx.x] = 0;
-    __syncthreads();
-    i64 base = (i64)blockIdx.x * SORT_TILE;
-    for (int i = threadIdx.x; i < SORT_TILE; i += SORT_THREADS) {
-        i64 k = base + i;
-        if (k < n) atomicAdd(&counts[(int)((keys[k] >> shift) & (RADIX - 1))], 1);
-    }
-    __syncthreads();
-    if (threadIdx.x < RADIX) hist[threadIdx.x * n_tiles + blockIdx.x] = counts[threadIdx.x];
+__device__ __forceinline__ unsigned lanes_below() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
 }
 
-// Each thread owns SORT_ITEMS consecutive items of the tile; an item's rank in the
-// tile is (items of smaller digits) + (same digit in earlier threads) + (same digit
-// earlier in this thread), which keeps equal keys in input order (stable).
-template <typename K>
-__global__ void k_sort_scatter(const K* __restrict__ keys, const unsigned* __restrict__ vals,
-                               K* __restrict__ keys_out, unsigned* __restrict__ vals_out,
-                               i64 n, int shift, int n_tiles, const int* __restrict__ offsets) {
-    __shared__ int table[RADIX * SORT_THREADS];
-    __shared__ K skeys[SORT_TILE];
+__global__ void __launch_bounds__(SORT_THREADS)
+k_sort_hist(const unsigned* __restrict__ keys, i64 n, int shift, unsigned mask, int n_tiles,
+            int* __restrict__ hist) {
+    __shared__ int counts[SORT_WARPS][RADIX];
+    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&counts[0][0])[i] = 0;
+    __syncthreads();
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    i64 base = (i64)blockIdx.x * SORT_TILE + (i64)wib * WARP_ITEMS;
+#pragma unroll 4
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        i64 k = base + r * 32 + lane;
+        bool live = k < n;
+        unsigned d = live ? (keys[k] >> shift) & mask : RADIX;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (live && (peers & lanes_below()) == 0) atomicAdd(&counts[wib][d], __popc(peers));
+    }
+    __syncthreads();
+    int d = threadIdx.x, sum = 0;
+#pragma unroll
+    for (int w = 0; w < SORT_WARPS; ++w) sum += counts[w][d];
+    hist[(i64)d * n_tiles + blockIdx.x] = sum;
+}
+
+__global__ void __launch_bounds__(SORT_THREADS)
+k_sort_scatter(const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
+               unsigned* __restrict__ keys_out, unsigned* __restrict__ vals_out, i64 n, int shift,
+               unsigned mask, int n_tiles, const int* __restrict__ offsets) {
+    __shared__ unsigned skeys[SORT_TILE];
     __shared__ unsigned svals[SORT_TILE];
-    i64 base = (i64)blockIdx.x * SORT_TILE;
-    for (int i = threadIdx.x; i < SORT_TILE; i += SORT_THREADS) {
-        i64 k = base + i;
-        if (k < n) {
-            skeys[i] = keys[k];
-            svals[i] = vals[k];
-        }
+    __shared__ int wcount[SORT_WARPS][RADIX];
+    __shared__ int tstart[RADIX];
+    __shared__ int goff[RADIX];
+    for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&wcount[0][0])[i] = 0;
+    __syncthreads();
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    i64 tile = (i64)blockIdx.x * SORT_TILE;
+    i64 base = tile + (i64)wib * WARP_ITEMS;
+    unsigned kr[SORT_ITEMS], vr[SORT_ITEMS];
+    int rank[SORT_ITEMS];
+    unsigned below = lanes_below();
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        i64 k = base + r * 32 + lane;
+        bool live = k < n;
+        kr[r] = live ? keys[k] : 0u;
+        vr[r] = live ? vals[k] : 0u;
+        unsigned d = live ? (kr[r] >> shift) & mask : RADIX;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        int before = __popc(peers & below);
+        int seen = live ? wcount[wib][d] : 0;
+        __syncwarp();
+        if (live && before == 0) wcount[wib][d] = seen + __popc(peers);
+        __syncwarp();
+        rank[r] = seen + before;
     }
     __syncthreads();
-    int local[RADIX];
+    // digit d (thread d): per-warp exclusive offsets within the digit, the tile total
+    int d = threadIdx.x, sum = 0;
 #pragma unroll
-    for (int d = 0; d < RADIX; ++d) local[d] = 0;
-    int first = threadIdx.x * SORT_ITEMS;
-#pragma unroll
-    for (int i = 0; i < SORT_ITEMS; ++i) {
-        if (base + first + i < n) {
-            int d = (int)((skeys[first + i] >> shift) & (RADIX - 1));
-#pragma unroll
-            for (int e = 0; e < RADIX; ++e) local[e] += (e == d);
-        }
-    }
-#pragma unroll
-    for (int d = 0; d < RADIX; ++d) table[d * SORT_THREADS + threadIdx.x] = local[d];
-    __syncthreads();
-    // exclusive scan of table (digit-major): thread t owns entries [16 t, 16 t + 16)
-    int run[RADIX];
-    int s = 0;
-#pragma unroll
-    for (int i = 0; i < RADIX; ++i) {
-        run[i] = table[threadIdx.x * RADIX + i];
-        s += run[i];
+    for (int w = 0; w < SORT_WARPS; ++w) {
+        int c = wcount[w][d];
+        wcount[w][d] = sum;
+        sum += c;
     }
     int total;
-    int off = block_exclusive(s, &total);
+    int start = block_exclusive(sum, &total);
+    tstart[d] = start;
+    goff[d] = offsets[(i64)d * n_tiles + blockIdx.x];
+    __syncthreads();
 #pragma unroll
-    for (int i = 0; i < RADIX; ++i) {
-        table[threadIdx.x * RADIX + i] = off;
-        off += run[i];
+    for (int r = 0; r < SORT_ITEMS; ++r) {
+        if (base + r * 32 + lane < n) {
+            int dg = (int)((kr[r] >> shift) & mask);
+            int at = tstart[dg] + wcount[wib][dg] + rank[r];
+            skeys[at] = kr[r];
+            svals[at] = vr[r];
+        }
     }
     __syncthreads();
-    int pos[RADIX];
-#pragma unroll
-    for (int d = 0; d < RADIX; ++d)
-        pos[d] = table[d * SORT_THREADS + threadIdx.x] - table[d * SORT_THREADS] +
-                 offsets[d * n_tiles + blockIdx.x];
-#pragma unroll
-    for (int i = 0; i < SORT_ITEMS; ++i) {
-        if (base + first + i < n) {
-            K key = skeys[first + i];
-            int d = (int)((key >> shift) & (RADIX - 1));
-            int p = 0;
-#pragma unroll
-            for (int e = 0; e < RADIX; ++e)
-                if (e == d) p = pos[e]++;
-            keys_out[p] = key;
-            vals_out[p] = svals[first + i];
-        }
+    int count = (int)(n - tile < SORT_TILE ? n - tile : SORT_TILE);
+    for (int i = threadIdx.x; i < count; i += SORT_THREADS) {
+        unsigned key = skeys[i];
+        int dg = (int)((key >> shift) & mask);
+        i64 p = (i64)goff[dg] + (i - tstart[dg]);
+        keys_out[p] = key;
+        vals_out[p] = svals[i];
     }
 }
 
-template <typename K>
-int radix_sort(K* keys, K* keys_alt, unsigned* vals, unsigned* vals_alt, i64 n, int bits,
-               K** keys_out, unsigned** vals_out, void* ws, size_t ws_bytes,
+int radix_sort(unsigned* keys, unsigned* keys_alt, unsigned* vals, unsigned* vals_alt, i64 n,
+               int bits, unsigned** keys_out, unsigned** vals_out, void* ws, size_t ws_bytes,
                cudaStream_t stream) {
     *keys_out = keys;
     *vals_out = vals;
@@ -251,22 +269,23 @@ int radix_sort(K* keys, K* keys_alt, unsigned* vals, unsigned* vals_alt, i64 n, 
     if (n > 0x7fffffffLL) return TD3_EINVAL;
     int n_tiles = (int)((n + SORT_TILE - 1) / SORT_TILE);
     i64 n_hist = (i64)RADIX * n_tiles;
+    if (n_hist > 0x7fffffffLL) return TD3_EINVAL;
     Workspace w(ws, ws_bytes);
     int* hist = w.take<int>(n_hist);
     void* scan_ws = w.base + w.used;
     size_t scan_bytes = w.size - w.used;
     if (!hist) return TD3_EWORKSPACE;
-    K* src_k = keys;
-    K* dst_k = keys_alt;
-    unsigned* src_v = vals;
-    unsigned* dst_v = vals_alt;
+    unsigned *src_k = keys, *dst_k = keys_alt, *src_v = vals, *dst_v = vals_alt;
+    if (bits > 32) bits = 32;
     for (int shift = 0; shift < bits; shift += RADIX_BITS) {
-        k_sort_hist<K><<<n_tiles, SORT_THREADS, 0, stream>>>(src_k, n, shift, n_tiles, hist);
+        int digit_bits = bits - shift < RADIX_BITS ? bits - shift : RADIX_BITS;
+        unsigned mask = (1u << digit_bits) - 1u;
+        k_sort_hist<<<n_tiles, SORT_THREADS, 0, stream>>>(src_k, n, shift, mask, n_tiles, hist);
         TD3_TRY_RC(td3_exclusive_scan_i32(hist, hist, n_hist, nullptr, scan_ws, scan_bytes, stream));
-        k_sort_scatter<K><<<n_tiles, SORT_THREADS, 0, stream>>>(src_k, src_v, dst_k, dst_v, n,
-                                                                shift, n_tiles, hist);
+        k_sort_scatter<<<n_tiles, SORT_THREADS, 0, stream>>>(src_k, src_v, dst_k, dst_v, n, shift,
+                                                             mask, n_tiles, hist);
         TD3_CHECK_LAUNCH();
-        K* tk = src_k;
+        unsigned* tk = src_k;
         src_k = dst_k;
         dst_k = tk;
         unsigned* tv = src_v;
@@ -309,15 +328,8 @@ size_t td3_sort_workspace(i64 n) {
 int td3_radix_sort_u32(unsigned* keys, unsigned* keys_alt, unsigned* vals, unsigned* vals_alt,
                        i64 n, int bits, unsigned** keys_out, unsigned** vals_out, void* ws,
                        size_t ws_bytes, cudaStream_t stream) {
-    return radix_sort<unsigned>(keys, keys_alt, vals, vals_alt, n, bits, keys_out, vals_out, ws,
-                                ws_bytes, stream);
-}
-
-int td3_radix_sort_u64(unsigned long long* keys, unsigned long long* keys_alt, unsigned* vals,
-                       unsigned* vals_alt, i64 n, int bits, unsigned long long** keys_out,
-                       unsigned** vals_out, void* ws, size_t ws_bytes, cudaStream_t stream) {
-    return radix_sort<unsigned long long>(keys, keys_alt, vals, vals_alt, n, bits, keys_out,
-                                          vals_out, ws, ws_bytes, stream);
+    return radix_sort(keys, keys_alt, vals, vals_alt, n, bits, keys_out, vals_out, ws, ws_bytes,
+                      stream);
 }
 
 // ------------------------------------------------------------------- C ABI

@@ -364,13 +364,9 @@ extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int
                                   w.size - w.used, s));
     TD3_TRY_RC(td3_exclusive_scan_i64(row_start, row_start, n_nodes + 1, nullptr, w.base + w.used,
                                       w.size - w.used, s));
-    // valid entries sort before the invalid key n_nodes; their number is row_start[n_nodes]
-    i64 valid = mutual ? -1 : count;
-    if (valid < 0) {
-        TD3_TRY(cudaMemcpyAsync(&valid, row_start + n_nodes, sizeof(i64), cudaMemcpyDeviceToHost, s));
-        TD3_TRY(cudaStreamSynchronize(s));
-    }
-    k_widen_vals<<<td3_blocks(valid, 256), 256, 0, s>>>(vo, valid, partners);
+    // valid entries sort before the invalid key n_nodes (row_start[n_nodes] of them); the
+    // entries after them are widened too (partners holds e slots), so no host read
+    k_widen_vals<<<td3_blocks(e, 256), 256, 0, s>>>(vo, e, partners);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
