@@ -159,3 +159,24 @@ def test_large_build_is_a_valid_tree():
     leaves = ~split
     assert int(((end - start)[leaves] > 8).sum()) == 0
     assert torch.equal(tree._sorted_pos, tree.pos[:, perm])
+
+
+@pytest.mark.parametrize("scale,depth", [(1e-5, 48), (1e-8, 48), (1e-8, 20), (1e-12, 48)])
+def test_build_of_fine_clusters_matches_the_oracle(oracle, scale, depth):
+    """Clusters 2^-17 to 2^-40 of the root: trees whose splits go past the first 16
+    levels of the quadrant paths, past 32 levels, or stop at max_depth."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad
+
+    rng = np.random.default_rng(int(-np.log10(scale)) + depth)
+    pos = np.concatenate([rng.uniform(-1, 1, (2, 3000)),
+                          0.3 + scale * rng.normal(size=(2, 2000)),
+                          -0.51 + scale * rng.uniform(-1, 1, (2, 500))], axis=1)
+    ref = oracle.OracleTree(pos, np.ones(pos.shape[1]), (0.0, 0.0, 1.0), leaf_capacity=5,
+                            max_depth=depth)
+    tree = FlatQuadtree(pos, np.ones(pos.shape[1]), Quad(0, 0, 1), leaf_capacity=5,
+                        max_depth=depth)
+    assert tree.node_count == ref.node_count
+    for name in TREE_ARRAYS:
+        np.testing.assert_array_equal(_np(getattr(tree, name)), getattr(ref, name)[: ref.node_count]
+                                      if name != "perm" else ref.perm, err_msg=name)
+    np.testing.assert_array_equal(tree.levels, ref.levels)

@@ -169,7 +169,7 @@ def _m2l_coefficients(order: int, symmetric: bool) -> np.ndarray:
 
 
 #: partners per near-field work segment (one warp each)
-NEAR_SEGMENT = 32
+NEAR_SEGMENT = 256
 
 
 def _nearfield_plan(rows: torch.Tensor, tree) -> dict:
@@ -332,7 +332,7 @@ class FlatQuadtree:
             if rc == _lib.OK:
                 break
             self.build_restarts += 1
-            capacity *= 2
+            capacity = max(2 * capacity, int(sizes[0]))
         self.levels = levels[: sizes[1] + 1].copy()
         self._sorted_charge = self.charge[self.perm].contiguous()
         return int(sizes[0])
