@@ -216,7 +216,7 @@ int td3_evaluate_quadtree(int kernel, const double* targets, int64_t m, const in
  * the reference's serial order (generation by generation, frontier order); sizes
  * (HOST, 4) = n_m2l, n_p2p, next frontier, -1 on overflow, when TD3_ENEEDMORE is
  * returned (retry with larger buffers).  frontier_capacity bounds one generation.
- * Synchronises `stream` once per generation.  Replaces fmm_traverse
+ * Synchronises `stream` once per 8 generations.  Replaces fmm_traverse
  * (src/tree_d_3d/kernels/fmm_traverse/fmm_traverse_pyccel.py:15-106,
  * fmm_traverse_cuda.cu:14-97) driven by FlatQuadtree._traverse
  * (src/tree_d_3d/flat_tree.py:1318-1358); identical lists. */

@@ -9,6 +9,7 @@
 // A generation classifies every frontier pair (M2L, P2P, its 4 or 10 child pairs, or
 // dropped), an exclusive scan of the per-pair counts gives each output its slot, and a
 // second pass writes them: the lists come out in the reference's serial order.  The
+// frontier sizes stay on the device; the host looks at them every few generations.  The
 // predicates use exactly rounded operations (this file is compiled with --fmad=false).
 #include "common.cuh"
 
@@ -53,139 +54,271 @@ __device__ __forceinline__ td3_i64x2 action_counts(int act) {
     }
 }
 
-__global__ void k_trav_classify(const Pair* __restrict__ frontier, i64 nf,
-                                const double* __restrict__ center, const double* __restrict__ half,
-                                const i64* __restrict__ start, const i64* __restrict__ end,
-                                const i64* __restrict__ child, double theta,
-                                signed char* __restrict__ action, td3_i64x2* __restrict__ counts) {
-    i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nf) return;
-    Pair pr = frontier[k];
-    int act = classify_mutual(pr.a, pr.b, center, half, start, end, child, theta);
-    action[k] = (signed char)act;
-    counts[k] = action_counts(act);
+// The one-way decision for (target cell a, source cell b) (dual_traverse_pyccel.py:46-86).
+__device__ __forceinline__ int classify_dual(i64 a, i64 b, const double* __restrict__ t_center,
+                                             const double* __restrict__ t_half,
+                                             const i64* __restrict__ t_start,
+                                             const i64* __restrict__ t_end,
+                                             const i64* __restrict__ t_child,
+                                             const double* __restrict__ s_center,
+                                             const double* __restrict__ s_half,
+                                             const i64* __restrict__ s_start,
+                                             const i64* __restrict__ s_end,
+                                             const i64* __restrict__ s_child, double theta) {
+    if (t_end[a] == t_start[a] || s_end[b] == s_start[b]) return ACT_NONE;
+    double dx = xsub(t_center[2 * a], s_center[2 * b]);
+    double dy = xsub(t_center[2 * a + 1], s_center[2 * b + 1]);
+    if (xmul(TD3_ROOT2, xadd(t_half[a], s_half[b])) < xmul(theta, xsqrt(xnorm2(dx, dy))))
+        return ACT_M2L;
+    bool leaf_a = t_child[a] < 0, leaf_b = s_child[b] < 0;
+    if (leaf_a && leaf_b) return ACT_P2P;
+    if (leaf_b || (!leaf_a && t_half[a] >= s_half[b])) return ACT_SPLIT_A;
+    return ACT_SPLIT_B;
 }
 
-__global__ void k_trav_emit(const Pair* __restrict__ frontier, i64 nf,
-                            const signed char* __restrict__ action,
-                            const td3_i64x2* __restrict__ offsets, const i64* __restrict__ child,
-                            i64 base_m2l, i64 base_p2p, Pair* __restrict__ m2l,
-                            Pair* __restrict__ p2p, Pair* __restrict__ next) {
-    i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nf) return;
-    int act = action[k];
-    if (act == ACT_NONE) return;
-    Pair pr = frontier[k];
-    td3_i64x2 off = offsets[k];
-    switch (act) {
-        case ACT_M2L: m2l[base_m2l + (off.a & 0xffffffffLL)] = pr; break;
-        case ACT_P2P: p2p[base_p2p + (off.a >> 32)] = pr; break;
-        case ACT_SELF: {
-            i64 first = child[pr.a], i = off.b;
-            for (int c = 0; c < 4; ++c)
-                for (int d = c; d < 4; ++d) next[i++] = Pair{first + c, first + d};
-            break;
+// ------------------------------------------------------------------ generations
+// A generation is three launches of fixed size that read the frontier size from device
+// memory: classify (action per pair, counts per tile of GEN_TILE pairs), an exclusive
+// scan of the tile counts (one block; it also checks the buffers and advances the
+// totals), and emit (per tile, block scans of the pairs' counts in frontier order give
+// every output its slot).  The host reads the state once per GEN_BATCH generations.
+constexpr int GEN_ITEMS = 8;
+constexpr int GEN_TILE = TRAV_THREADS * GEN_ITEMS;
+constexpr int GEN_BATCH = 8;
+constexpr int GEN_SCAN_THREADS = 1024;
+
+struct TravState {
+    i64 nf[2];          // frontier size of even / odd generations
+    i64 emit_nf;        // frontier size the current emit pass writes (0 after overflow)
+    i64 n_m2l, n_p2p;   // pairs listed so far
+    i64 base_m2l, base_p2p;
+    i64 overflow;       // a list or the next frontier outgrew its buffer
+    i64 need_m2l, need_p2p, need_frontier;
+};
+
+struct TreeView {
+    const double* center;
+    const double* half;
+    const i64* start;
+    const i64* end;
+    const i64* child;
+};
+
+template <bool DUAL>
+__device__ __forceinline__ int classify_pair(const TreeView& t, const TreeView& s, double theta,
+                                             Pair pr) {
+    if (DUAL)
+        return classify_dual(pr.a, pr.b, t.center, t.half, t.start, t.end, t.child, s.center,
+                             s.half, s.start, s.end, s.child, theta);
+    return classify_mutual(pr.a, pr.b, t.center, t.half, t.start, t.end, t.child, theta);
+}
+
+__device__ __forceinline__ td3_i64x2 warp_inclusive_x2(td3_i64x2 v, int lane) {
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        long long a = __shfl_up_sync(0xffffffffu, (long long)v.a, d);
+        long long b = __shfl_up_sync(0xffffffffu, (long long)v.b, d);
+        if (lane >= d) {
+            v.a += a;
+            v.b += b;
         }
-        case ACT_SPLIT_A: {
-            i64 first = child[pr.a];
-            for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{first + c, pr.b};
-            break;
+    }
+    return v;
+}
+
+// Exclusive scan over the block (blockDim.x a multiple of 32, at most 1024 threads).
+__device__ __forceinline__ td3_i64x2 block_exclusive_x2(td3_i64x2 v, td3_i64x2* total) {
+    __shared__ td3_i64x2 sums[32];
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    td3_i64x2 inc = warp_inclusive_x2(v, lane);
+    if (lane == 31) sums[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        td3_i64x2 x = lane < nw ? sums[lane] : td3_i64x2(0);
+        x = warp_inclusive_x2(x, lane);
+        if (lane < nw) sums[lane] = x;
+    }
+    __syncthreads();
+    td3_i64x2 off = warp ? sums[warp - 1] : td3_i64x2(0);
+    *total = sums[nw - 1];
+    __syncthreads();
+    return off + inc - v;
+}
+
+__global__ void k_gen_init(TravState* st, Pair* frontier) {
+    st->nf[0] = 1;
+    st->nf[1] = 0;
+    st->emit_nf = 0;
+    st->n_m2l = st->n_p2p = st->base_m2l = st->base_p2p = 0;
+    st->overflow = st->need_m2l = st->need_p2p = st->need_frontier = 0;
+    frontier[0] = Pair{0, 0};
+}
+
+template <bool DUAL>
+__global__ void __launch_bounds__(TRAV_THREADS)
+k_gen_classify(const Pair* __restrict__ frontier, const TravState* st, int parity, TreeView t,
+               TreeView s, double theta, signed char* __restrict__ action,
+               td3_i64x2* __restrict__ tile_sum) {
+    i64 nf = st->nf[parity];
+    i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
+    for (i64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        td3_i64x2 sum(0);
+#pragma unroll
+        for (int i = 0; i < GEN_ITEMS; ++i) {
+            i64 k = tile * GEN_TILE + i * TRAV_THREADS + threadIdx.x;
+            if (k < nf) {
+                int act = classify_pair<DUAL>(t, s, theta, frontier[k]);
+                action[k] = (signed char)act;
+                sum += action_counts(act);
+            }
         }
-        case ACT_SPLIT_B: {
-            i64 first = child[pr.b];
-            for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{pr.a, first + c};
-            break;
-        }
+        td3_i64x2 total;
+        block_exclusive_x2(sum, &total);
+        if (threadIdx.x == 0) tile_sum[tile] = total;
     }
 }
 
-__global__ void k_root_pair(Pair* frontier) { frontier[0] = Pair{0, 0}; }
-
-// ------------------------------------------------------------------ dual traversal
-// One-way decision for (target cell a, source cell b) (dual_traverse_pyccel.py:46-86).
-__global__ void k_dual_classify(const Pair* __restrict__ frontier, i64 nf,
-                                const double* __restrict__ t_center, const double* __restrict__ t_half,
-                                const i64* __restrict__ t_start, const i64* __restrict__ t_end,
-                                const i64* __restrict__ t_child,
-                                const double* __restrict__ s_center, const double* __restrict__ s_half,
-                                const i64* __restrict__ s_start, const i64* __restrict__ s_end,
-                                const i64* __restrict__ s_child, double theta,
-                                signed char* __restrict__ action, td3_i64x2* __restrict__ counts) {
-    i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nf) return;
-    Pair pr = frontier[k];
-    i64 a = pr.a, b = pr.b;
-    int act;
-    if (t_end[a] == t_start[a] || s_end[b] == s_start[b]) {
-        act = ACT_NONE;
-    } else {
-        double dx = xsub(t_center[2 * a], s_center[2 * b]);
-        double dy = xsub(t_center[2 * a + 1], s_center[2 * b + 1]);
-        if (xmul(TD3_ROOT2, xadd(t_half[a], s_half[b])) < xmul(theta, xsqrt(xnorm2(dx, dy)))) {
-            act = ACT_M2L;
+__global__ void __launch_bounds__(GEN_SCAN_THREADS)
+k_gen_scan(TravState* st, int parity, td3_i64x2* __restrict__ tile_sum, i64 m2l_capacity,
+           i64 p2p_capacity, i64 frontier_capacity) {
+    i64 nf = st->nf[parity];
+    i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
+    td3_i64x2 carry(0);
+    for (i64 c = 0; c < tiles; c += GEN_SCAN_THREADS) {
+        i64 tile = c + threadIdx.x;
+        td3_i64x2 v = tile < tiles ? tile_sum[tile] : td3_i64x2(0);
+        td3_i64x2 total;
+        td3_i64x2 ex = block_exclusive_x2(v, &total);
+        if (tile < tiles) tile_sum[tile] = carry + ex;
+        carry += total;
+    }
+    if (threadIdx.x == 0) {
+        i64 add_m2l = carry.a & 0xffffffffLL, add_p2p = carry.a >> 32, nn = carry.b;
+        st->base_m2l = st->n_m2l;
+        st->base_p2p = st->n_p2p;
+        if (st->n_m2l + add_m2l > m2l_capacity || st->n_p2p + add_p2p > p2p_capacity ||
+            nn > frontier_capacity) {
+            st->overflow = 1;
+            st->need_m2l = st->n_m2l + add_m2l;
+            st->need_p2p = st->n_p2p + add_p2p;
+            st->need_frontier = nn;
+            st->emit_nf = 0;
+            st->nf[parity ^ 1] = 0;
         } else {
-            bool leaf_a = t_child[a] < 0, leaf_b = s_child[b] < 0;
-            if (leaf_a && leaf_b)
-                act = ACT_P2P;
-            else if (leaf_b || (!leaf_a && t_half[a] >= s_half[b]))
-                act = ACT_SPLIT_A;
-            else
-                act = ACT_SPLIT_B;
+            st->n_m2l += add_m2l;
+            st->n_p2p += add_p2p;
+            st->emit_nf = nf;
+            st->nf[parity ^ 1] = nn;
         }
     }
-    action[k] = (signed char)act;
-    counts[k] = action_counts(act);
 }
 
-__global__ void k_dual_emit(const Pair* __restrict__ frontier, i64 nf,
-                            const signed char* __restrict__ action,
-                            const td3_i64x2* __restrict__ offsets, const i64* __restrict__ t_child,
-                            const i64* __restrict__ s_child, i64 base_m2l, i64 base_p2p,
-                            Pair* __restrict__ m2l, Pair* __restrict__ p2p, Pair* __restrict__ next) {
-    i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nf) return;
-    int act = action[k];
-    if (act == ACT_NONE) return;
-    Pair pr = frontier[k];
-    td3_i64x2 off = offsets[k];
-    if (act == ACT_M2L) {
-        m2l[base_m2l + (off.a & 0xffffffffLL)] = pr;
-    } else if (act == ACT_P2P) {
-        p2p[base_p2p + (off.a >> 32)] = pr;
-    } else if (act == ACT_SPLIT_A) {
-        i64 first = t_child[pr.a];
-        for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{first + c, pr.b};
-    } else {
-        i64 first = s_child[pr.b];
-        for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{pr.a, first + c};
+template <bool DUAL>
+__global__ void __launch_bounds__(TRAV_THREADS)
+k_gen_emit(const Pair* __restrict__ frontier, const TravState* st,
+           const signed char* __restrict__ action, const td3_i64x2* __restrict__ tile_off,
+           const i64* __restrict__ t_child, const i64* __restrict__ s_child,
+           Pair* __restrict__ m2l, Pair* __restrict__ p2p, Pair* __restrict__ next) {
+    i64 nf = st->emit_nf;
+    i64 base_m2l = st->base_m2l, base_p2p = st->base_p2p;
+    i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
+    for (i64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        td3_i64x2 carry = tile_off[tile];
+        for (int i = 0; i < GEN_ITEMS; ++i) {
+            i64 k = tile * GEN_TILE + i * TRAV_THREADS + threadIdx.x;
+            int act = k < nf ? action[k] : ACT_NONE;
+            td3_i64x2 total;
+            td3_i64x2 off = carry + block_exclusive_x2(action_counts(act), &total);
+            carry += total;
+            if (act == ACT_NONE) continue;
+            Pair pr = frontier[k];
+            switch (act) {
+                case ACT_M2L: m2l[base_m2l + (off.a & 0xffffffffLL)] = pr; break;
+                case ACT_P2P: p2p[base_p2p + (off.a >> 32)] = pr; break;
+                case ACT_SELF: {
+                    i64 first = t_child[pr.a], j = off.b;
+                    for (int c = 0; c < 4; ++c)
+                        for (int d = c; d < 4; ++d) next[j++] = Pair{first + c, first + d};
+                    break;
+                }
+                case ACT_SPLIT_A: {
+                    i64 first = t_child[pr.a];
+                    for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{first + c, pr.b};
+                    break;
+                }
+                default: {
+                    i64 first = (DUAL ? s_child : t_child)[pr.b];
+                    for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{pr.a, first + c};
+                    break;
+                }
+            }
+        }
     }
 }
 
 struct TraverseBuffers {
     Pair* frontier[2];
     signed char* action;
-    td3_i64x2* counts;
-    td3_i64x2* total;
-    void* scan_ws;
-    size_t scan_bytes;
+    td3_i64x2* tile_sum;
+    TravState* state;
 };
+
+i64 gen_tiles(i64 frontier_cap) { return (frontier_cap + GEN_TILE - 1) / GEN_TILE; }
 
 size_t traverse_workspace(i64 frontier_cap) {
     return 2 * td3_ws_bytes<Pair>(frontier_cap) + td3_ws_bytes<signed char>(frontier_cap) +
-           td3_ws_bytes<td3_i64x2>(frontier_cap) + td3_ws_bytes<td3_i64x2>(1) +
-           td3_scan_workspace(frontier_cap) + 256;
+           td3_ws_bytes<td3_i64x2>(gen_tiles(frontier_cap)) + td3_ws_bytes<TravState>(1) + 256;
 }
 
 bool take_traverse(Workspace& w, i64 frontier_cap, TraverseBuffers& b) {
     b.frontier[0] = w.take<Pair>(frontier_cap);
     b.frontier[1] = w.take<Pair>(frontier_cap);
     b.action = w.take<signed char>(frontier_cap);
-    b.counts = w.take<td3_i64x2>(frontier_cap);
-    b.total = w.take<td3_i64x2>(1);
-    if (!b.total) return false;
-    b.scan_ws = w.base + w.used;
-    b.scan_bytes = w.size - w.used;
-    return true;
+    b.tile_sum = w.take<td3_i64x2>(gen_tiles(frontier_cap));
+    b.state = w.take<TravState>(1);
+    return b.state != nullptr;
+}
+
+// The generations from (root, root) until the frontier is empty; sizes as the entry
+// points document them.
+template <bool DUAL>
+int run_generations(const TreeView& t, const TreeView& s, double theta, Pair* m2l,
+                    i64 m2l_capacity, Pair* p2p, i64 p2p_capacity, i64 frontier_capacity,
+                    int64_t* sizes, const TraverseBuffers& b, cudaStream_t stream) {
+    i64 tiles = gen_tiles(frontier_capacity);
+    unsigned grid = (unsigned)(tiles < 148 * 4 ? tiles : 148 * 4);
+    k_gen_init<<<1, 1, 0, stream>>>(b.state, b.frontier[0]);
+    TD3_CHECK_LAUNCH();
+    sizes[0] = sizes[1] = sizes[2] = sizes[3] = 0;
+    for (int gen = 0;;) {
+        for (int k = 0; k < GEN_BATCH; ++k, ++gen) {
+            int parity = gen & 1;
+            k_gen_classify<DUAL><<<grid, TRAV_THREADS, 0, stream>>>(
+                b.frontier[parity], b.state, parity, t, s, theta, b.action, b.tile_sum);
+            k_gen_scan<<<1, GEN_SCAN_THREADS, 0, stream>>>(b.state, parity, b.tile_sum,
+                                                            m2l_capacity, p2p_capacity,
+                                                            frontier_capacity);
+            k_gen_emit<DUAL><<<grid, TRAV_THREADS, 0, stream>>>(
+                b.frontier[parity], b.state, b.action, b.tile_sum, t.child, s.child, m2l, p2p,
+                b.frontier[parity ^ 1]);
+            TD3_CHECK_LAUNCH();
+        }
+        TravState h;
+        TD3_TRY(cudaMemcpyAsync(&h, b.state, sizeof(h), cudaMemcpyDeviceToHost, stream));
+        TD3_TRY(cudaStreamSynchronize(stream));
+        if (h.overflow) {
+            sizes[0] = h.need_m2l;
+            sizes[1] = h.need_p2p;
+            sizes[2] = h.need_frontier;
+            sizes[3] = -1;
+            return TD3_ENEEDMORE;
+        }
+        if (h.nf[gen & 1] == 0) {
+            sizes[0] = h.n_m2l;
+            sizes[1] = h.n_p2p;
+            return TD3_OK;
+        }
+    }
 }
 
 // ------------------------------------------------------------------ pair CSR
@@ -238,48 +371,13 @@ extern "C" int td3_fmm_traverse(const double* node_center, const double* node_ha
                                 int64_t frontier_capacity, int64_t* sizes, void* workspace,
                                 size_t workspace_bytes, void* stream) {
     if (frontier_capacity < 1 || m2l_capacity < 0 || p2p_capacity < 0) return TD3_EINVAL;
-    cudaStream_t s = td3_stream(stream);
     Workspace w(workspace, workspace_bytes);
     TraverseBuffers b;
     if (!take_traverse(w, frontier_capacity, b)) return TD3_EWORKSPACE;
-    Pair* pm2l = reinterpret_cast<Pair*>(m2l);
-    Pair* pp2p = reinterpret_cast<Pair*>(p2p);
-    k_root_pair<<<1, 1, 0, s>>>(b.frontier[0]);
-    TD3_CHECK_LAUNCH();
-    i64 nf = 1, n_m2l = 0, n_p2p = 0;
-    int cur = 0;
-    sizes[0] = sizes[1] = sizes[2] = sizes[3] = 0;
-    while (nf > 0) {
-        unsigned nb = td3_blocks(nf, TRAV_THREADS);
-        k_trav_classify<<<nb, TRAV_THREADS, 0, s>>>(b.frontier[cur], nf, node_center, node_half,
-                                                    node_start, node_end, node_child, theta,
-                                                    b.action, b.counts);
-        TD3_TRY_RC(td3_exclusive_scan_i64x2(b.counts, b.counts, nf, b.total, b.scan_ws,
-                                            b.scan_bytes, s));
-        td3_i64x2 tot;
-        TD3_TRY(cudaMemcpyAsync(&tot, b.total, sizeof(tot), cudaMemcpyDeviceToHost, s));
-        TD3_TRY(cudaStreamSynchronize(s));
-        i64 add_m2l = tot.a & 0xffffffffLL, add_p2p = tot.a >> 32, nn = tot.b;
-        if (n_m2l + add_m2l > m2l_capacity || n_p2p + add_p2p > p2p_capacity ||
-            nn > frontier_capacity) {
-            sizes[0] = n_m2l + add_m2l;
-            sizes[1] = n_p2p + add_p2p;
-            sizes[2] = nn;
-            sizes[3] = -1;
-            return TD3_ENEEDMORE;
-        }
-        k_trav_emit<<<nb, TRAV_THREADS, 0, s>>>(b.frontier[cur], nf, b.action, b.counts,
-                                                node_child, n_m2l, n_p2p, pm2l, pp2p,
-                                                b.frontier[cur ^ 1]);
-        TD3_CHECK_LAUNCH();
-        n_m2l += add_m2l;
-        n_p2p += add_p2p;
-        nf = nn;
-        cur ^= 1;
-    }
-    sizes[0] = n_m2l;
-    sizes[1] = n_p2p;
-    return TD3_OK;
+    TreeView t{node_center, node_half, node_start, node_end, node_child};
+    return run_generations<false>(t, t, theta, reinterpret_cast<Pair*>(m2l), m2l_capacity,
+                                  reinterpret_cast<Pair*>(p2p), p2p_capacity, frontier_capacity,
+                                  sizes, b, td3_stream(stream));
 }
 
 extern "C" int td3_dual_traverse(const double* t_center, const double* t_half,
@@ -291,48 +389,14 @@ extern "C" int td3_dual_traverse(const double* t_center, const double* t_half,
                                  int64_t p2p_capacity, int64_t frontier_capacity, int64_t* sizes,
                                  void* workspace, size_t workspace_bytes, void* stream) {
     if (frontier_capacity < 1 || m2l_capacity < 0 || p2p_capacity < 0) return TD3_EINVAL;
-    cudaStream_t s = td3_stream(stream);
     Workspace w(workspace, workspace_bytes);
     TraverseBuffers b;
     if (!take_traverse(w, frontier_capacity, b)) return TD3_EWORKSPACE;
-    Pair* pm2l = reinterpret_cast<Pair*>(m2l);
-    Pair* pp2p = reinterpret_cast<Pair*>(p2p);
-    k_root_pair<<<1, 1, 0, s>>>(b.frontier[0]);
-    TD3_CHECK_LAUNCH();
-    i64 nf = 1, n_m2l = 0, n_p2p = 0;
-    int cur = 0;
-    sizes[0] = sizes[1] = sizes[2] = sizes[3] = 0;
-    while (nf > 0) {
-        unsigned nb = td3_blocks(nf, TRAV_THREADS);
-        k_dual_classify<<<nb, TRAV_THREADS, 0, s>>>(b.frontier[cur], nf, t_center, t_half, t_start,
-                                                    t_end, t_child, s_center, s_half, s_start,
-                                                    s_end, s_child, theta, b.action, b.counts);
-        TD3_TRY_RC(td3_exclusive_scan_i64x2(b.counts, b.counts, nf, b.total, b.scan_ws,
-                                            b.scan_bytes, s));
-        td3_i64x2 tot;
-        TD3_TRY(cudaMemcpyAsync(&tot, b.total, sizeof(tot), cudaMemcpyDeviceToHost, s));
-        TD3_TRY(cudaStreamSynchronize(s));
-        i64 add_m2l = tot.a & 0xffffffffLL, add_p2p = tot.a >> 32, nn = tot.b;
-        if (n_m2l + add_m2l > m2l_capacity || n_p2p + add_p2p > p2p_capacity ||
-            nn > frontier_capacity) {
-            sizes[0] = n_m2l + add_m2l;
-            sizes[1] = n_p2p + add_p2p;
-            sizes[2] = nn;
-            sizes[3] = -1;
-            return TD3_ENEEDMORE;
-        }
-        k_dual_emit<<<nb, TRAV_THREADS, 0, s>>>(b.frontier[cur], nf, b.action, b.counts, t_child,
-                                                s_child, n_m2l, n_p2p, pm2l, pp2p,
-                                                b.frontier[cur ^ 1]);
-        TD3_CHECK_LAUNCH();
-        n_m2l += add_m2l;
-        n_p2p += add_p2p;
-        nf = nn;
-        cur ^= 1;
-    }
-    sizes[0] = n_m2l;
-    sizes[1] = n_p2p;
-    return TD3_OK;
+    TreeView t{t_center, t_half, t_start, t_end, t_child};
+    TreeView s{s_center, s_half, s_start, s_end, s_child};
+    return run_generations<true>(t, s, theta, reinterpret_cast<Pair*>(m2l), m2l_capacity,
+                                 reinterpret_cast<Pair*>(p2p), p2p_capacity, frontier_capacity,
+                                 sizes, b, td3_stream(stream));
 }
 
 extern "C" size_t td3_pair_csr_workspace_size(int64_t count, int mutual, int64_t n_nodes) {

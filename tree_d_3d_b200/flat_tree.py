@@ -172,13 +172,12 @@ def _m2l_coefficients(order: int, symmetric: bool) -> np.ndarray:
 NEAR_SEGMENT = 256
 
 
-def _nearfield_plan(rows: torch.Tensor, tree) -> dict:
+def _nearfield_plan(rows: torch.Tensor, tree, entries: int) -> dict:
     """The near-field work plan of one tree's leaf rows (td3_nearfield_plan): leaf rows
     cut into segments of at most NEAR_SEGMENT partners, and the partial-sum buffer of
-    the rows that take several segments."""
+    the rows that take several segments.  ``entries`` bounds the rows' partner count."""
     dev = rows.device
     n_nodes = rows.shape[0] - 1
-    entries = int(rows[-1].item())
     capacity = n_nodes + entries // NEAR_SEGMENT + 1
     seg_leaf = torch.empty(capacity, dtype=torch.int32, device=dev)
     seg_range = torch.empty((capacity, 2), dtype=torch.int64, device=dev)
@@ -531,7 +530,7 @@ class FlatQuadtree:
                 float(theta), m2l.data_ptr(), int(capacity[0]), p2p.data_ptr(), int(capacity[1]),
                 int(capacity[2]), sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
             if rc == _lib.OK:
-                return m2l[: sizes[0]].clone(), p2p[: sizes[1]].clone()
+                return m2l[: sizes[0]], p2p[: sizes[1]]
             capacity = np.maximum(2 * capacity, sizes[:3] + 64)
 
     def _rows(self, pairs: torch.Tensor, mutual: bool, n_nodes: int | None = None):
@@ -558,7 +557,7 @@ class FlatQuadtree:
                 "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
                 "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
             }
-            lists["plan"] = _nearfield_plan(p2p_rows, self)
+            lists["plan"] = _nearfield_plan(p2p_rows, self, 2 * p2p.shape[0])
             self._traversals[theta] = lists
         return self._traversals[theta]
 
@@ -774,13 +773,13 @@ class FlatQuadtree:
             if rc == _lib.OK:
                 break
             capacity = np.maximum(2 * capacity, sizes[:3] + 64)
-        m2l, p2p = m2l[: sizes[0]].clone(), p2p[: sizes[1]].clone()
+        m2l, p2p = m2l[: sizes[0]], p2p[: sizes[1]]
         m2l_rows, m2l_partners = self._rows(m2l, mutual=False, n_nodes=tree.node_count)
         p2p_rows, p2p_partners = self._rows(p2p, mutual=False, n_nodes=tree.node_count)
         return {
             "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
             "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
-            "plan": _nearfield_plan(p2p_rows, tree),
+            "plan": _nearfield_plan(p2p_rows, tree, p2p.shape[0]),
         }
 
     def _target_plan(self, targets: torch.Tensor, theta: float, leaf: int):
