@@ -257,8 +257,9 @@ def count_our_launches(fn, torch):
     return counts
 
 
-def time_m2l_mixed(tree, torch, reps):
-    """The mixed M2L kernel alone (CUDA events on its stream), average ms per launch."""
+def time_m2l_mixed(tree, torch, reps, tensor=1):
+    """The mixed M2L kernel alone (CUDA events on its stream), average ms per launch;
+    tensor=1 the tensor-core form, 0 the FP32 CUDA-core form."""
     from tree_d_3d_b200 import _lib
     from tree_d_3d_b200.flat_tree import _m2l_coefficients
 
@@ -269,10 +270,12 @@ def time_m2l_mixed(tree, torch, reps):
     hat = tree._scaled_moments((tree.moment_re, tree.moment_im))
     stream = _lib.stream(tree.device)
     coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
-    args = (lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(), count,
+    status = torch.zeros(1, dtype=torch.int64, device=tree.device)
+    args = (lists["m2l_rows"].data_ptr(), lists["m2l_entry_row"].data_ptr(),
+            lists["m2l_partners"].data_ptr(), count,
             tree.node_center.data_ptr(), tree.node_half.data_ptr(), tree.node_center.data_ptr(),
             tree.node_half.data_ptr(), hat.data_ptr(), tree.order, coeff.ctypes.data,
-            tree._unit, lre.data_ptr(), lim.data_ptr(), stream)
+            tree._unit, tensor, lre.data_ptr(), lim.data_ptr(), status.data_ptr(), stream)
     _lib.call("td3_fmm_m2l_mixed", *args)
     cur = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -282,6 +285,8 @@ def time_m2l_mixed(tree, torch, reps):
         _lib.call("td3_fmm_m2l_mixed", *args)
     stop.record(cur)
     torch.cuda.synchronize()
+    if int(status.item()):
+        raise RuntimeError("the tensor-core M2L timed out")
     return start.elapsed_time(stop) / reps, int(lists["m2l"].shape[0])
 
 

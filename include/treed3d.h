@@ -243,12 +243,14 @@ int td3_dual_traverse(const double* t_center, const double* t_half, const int64_
 
 /* Rows by node of the pairs (count, 2): row_start (n_nodes + 1) and partners, in pair
  * order; mutual != 0 lists b under a and a under b (once if a == b).  partners holds
- * count (mutual: 2 count) slots; those past row_start[n_nodes] are scratch.  Replaces pair_csr
+ * count (mutual: 2 count) slots; those past row_start[n_nodes] are scratch.  entry_row
+ * (may be NULL; as many slots as partners) receives the row of every entry (n_nodes in
+ * the scratch slots), for kernels that walk the entries rather than the rows.  Replaces pair_csr
  * (src/tree_d_3d/kernels/pair_csr/pair_csr_pyccel.py:12-45); identical rows. */
 size_t td3_pair_csr_workspace_size(int64_t count, int mutual, int64_t n_nodes);
 int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int64_t n_nodes,
-                 int64_t* row_start, int64_t* partners, void* workspace, size_t workspace_bytes,
-                 void* stream);
+                 int64_t* row_start, int64_t* partners, int32_t* entry_row, void* workspace,
+                 size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------------------------ log-kernel FMM */
 
@@ -273,15 +275,22 @@ int td3_fmm_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst
  * and local_re / local_im (FP64) += bhat_l / h_dst^l.  ln|t| is formed as ln|t / unit|
  * in FP32 plus ln(unit) sum a_0 in FP64 (unit > 0: a length of the problem, e.g. the
  * root half-width).  coeff is a HOST (order + 1)^2 array (the reference's M2L matrix);
- * order <= 20.  The FP32 counterpart of
- * td3_fmm_m2l (reference: fmm_m2l_host, src/tree_d_3d/kernels/fmm_m2l_host/
- * fmm_m2l_host_pyccel.py:16-105). */
+ * order <= 20.  entry_row: the row of every entry of partners (td3_pair_csr); a warp
+ * takes 32 consecutive entries at a time across row boundaries.  tensor_cores != 0 (orders <= 15) takes the matrix products s_l on the
+ * tensor cores (tcgen05.mma, 3xTF32 with FP32 accumulation) and needs status, a device
+ * int64 the caller zeroed: it becomes nonzero if a wait for the tensor cores ran out (the
+ * locals are then incomplete); otherwise FP32 CUDA-core arithmetic, status unused.  The
+ * rows of one destination are summed in row order either way (deterministic).  The
+ * FP32 counterpart of td3_fmm_m2l (reference: fmm_m2l_host,
+ * src/tree_d_3d/kernels/fmm_m2l_host/fmm_m2l_host_pyccel.py:16-105). */
 int td3_scale_moments(int64_t count, int order, const double* moment_re,
                       const double* moment_im, const double* node_half, float* hat, void* stream);
-int td3_fmm_m2l_mixed(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
+                      const int64_t* partners, int64_t n_dst,
                       const double* dst_center, const double* dst_half, const double* src_center,
                       const double* src_half, const float* hat, int order, const double* coeff,
-                      double unit, double* local_re, double* local_im, void* stream);
+                      double unit, int tensor_cores, double* local_re, double* local_im,
+                      int64_t* status, void* stream);
 
 /* L2L from the root down, level by level (levels HOST, n_levels + 1): every local
  * expansion shifted into its children, b_m(child) += sum_{l>=m} C(l, m) b_l s^(l-m).

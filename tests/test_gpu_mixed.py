@@ -134,3 +134,30 @@ def test_mixed_fmm_and_backward_at_extreme_length_scales(kernel, scale):
         out[precision] = [t.detach().cpu().numpy() for t in (phi, field, Q.grad, P.grad)]
     for a, b in zip(out["mixed"], out["fp64"]):
         assert relative(a, b) < TOL
+
+
+@pytest.mark.parametrize("order", [4, 8, 12, 15])
+def test_tensor_core_m2l_matches_cuda_core_m2l_and_fp64(order, monkeypatch):
+    """The M2L matrix products on the tensor cores (3xTF32, tcgen05) give the locals of
+    the FP32 CUDA-core form and of FP64 to FP32 accuracy, and the same bits every run
+    (fixed summation order per destination)."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, flat_tree, synthetic
+
+    pos, q = synthetic.mixture8(150_000, seed=40 + order)
+    P, Q = torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda")
+    ref = FlatQuadtree(P, Q, Quad(0, 0, 1), kernel="log", order=order)
+    lists = ref._lists(0.5)
+    fp64 = [t.cpu().numpy() for t in ref._log_locals(lists)]
+    tree = FlatQuadtree(P, Q, Quad(0, 0, 1), kernel="log", order=order, precision="mixed")
+    lists = tree._lists(0.5)
+    runs = {}
+    for tensor in (True, False):
+        monkeypatch.setattr(flat_tree, "M2L_TENSOR_CORES", tensor)
+        runs[tensor] = [t.cpu().numpy() for t in tree._log_locals(lists)]
+        tree._check_tensor_cores()
+    monkeypatch.setattr(flat_tree, "M2L_TENSOR_CORES", True)
+    again = [t.cpu().numpy() for t in tree._log_locals(lists)]
+    for part in (0, 1):
+        assert relative(runs[True][part], fp64[part]) < 1e-6
+        assert relative(runs[True][part], runs[False][part]) < 1e-6
+        assert np.array_equal(again[part], runs[True][part])

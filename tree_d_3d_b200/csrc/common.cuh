@@ -132,6 +132,14 @@ int td3_exclusive_scan_i32(const int* in, int* out, i64 n, int* total, void* ws,
 int td3_exclusive_scan_i64x2(const td3_i64x2* in, td3_i64x2* out, i64 n, td3_i64x2* total,
                              void* ws, size_t ws_bytes, cudaStream_t stream);
 
+// The mixed-precision log M2L with its matrix products on the tensor cores, orders up
+// to 15 (m2l_tc.cu); arguments as td3_fmm_m2l_mixed, coeff on the host.
+int td3_m2l_tensor(const i64* row_start, const int* entry_row, const i64* partners, i64 n_dst,
+                   const double* dst_center,
+                   const double* dst_half, const double* src_center, const double* src_half,
+                   const float2* hat, int order, const double* coeff, double unit,
+                   double* local_re, double* local_im, i64* status, cudaStream_t s);
+
 // Stable LSD radix sort of (key, value) pairs by the low `bits` bits of the key
 // (scan.cu).  Keys and values are ping-ponged between the in and alt buffers; the
 // sorted result is returned in *keys_out / *vals_out (one of the two buffers).

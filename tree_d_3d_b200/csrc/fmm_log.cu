@@ -9,6 +9,7 @@
 // s_l = sum_k coeff[k, l] a'_k is the real matrix product of the reference.  The
 // partial locals of the groups are summed by shuffles and added once per cell.
 #include "common.cuh"
+#include "m2l_rows.cuh"
 
 namespace {
 
@@ -166,46 +167,47 @@ struct CoefTable {
     float c[(P + 1) * (P + 1)];
 };
 
-// M2L in FP32, one lane per translation (partner), one warp per destination cell.
+// M2L in FP32 on the CUDA cores, one lane per translation (CSR entry), the entries of
+// a warp's run of rows taken 32 at a time across row boundaries (m2l_rows.cuh).
 // With w = 1/t, ws = h_src w and wd = h_dst w (|ws|, |wd| < 1 for separated cells):
 //   a'_k = hat_k ws^k,  s_l = sum_k coeff[k, l] a'_k,
 //   bhat_0 = a_0 ln|t| - s_0,  bhat_l = -(-1)^l s_l wd^l  (b_l = bhat_l / h_dst^l),
 // the reference's translation with every quantity O(1).  ln|t| is taken in units of
 // `unit` (L): a_0 ln|t| = a_0 ln|t / L| + a_0 ln L, the second summed over the partners
-// (a0r, a0i) and added in FP64.  The coefficient matrix is a kernel parameter (constant
-// bank), the sums over the partners are warp reductions, and the locals are added in FP64.
+// and added in FP64.  The coefficient matrix is a kernel parameter (constant bank).
 template <int P>
 __global__ void __launch_bounds__(32 * M2L_WARPS)
-k_m2l_mixed(const i64* __restrict__ row_start, const i64* __restrict__ partners, i64 n_dst,
-            const double* __restrict__ dst_center, const double* __restrict__ dst_half,
-            const double* __restrict__ src_center, const double* __restrict__ src_half,
-            const float2* __restrict__ hat, int order, const CoefTable<P> C, double unit,
-            double* __restrict__ local_re, double* __restrict__ local_im) {
-    constexpr int W = P + 1;
+k_m2l_mixed(const i64* __restrict__ row_start, const int* __restrict__ entry_row,
+            const i64* __restrict__ partners, i64 n_dst, const double* __restrict__ dst_center,
+            const double* __restrict__ dst_half, const double* __restrict__ src_center,
+            const double* __restrict__ src_half, const float2* __restrict__ hat, int order,
+            const CoefTable<P> C, double unit, double* __restrict__ local_re,
+            double* __restrict__ local_im) {
+    constexpr int W = P + 1, V = 2 * W + 2;
+    __shared__ float carry[M2L_WARPS][V];
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int w = order + 1;
     double inv_unit2 = 1.0 / (unit * unit), ln_unit = log(unit);
-    for (i64 dst = (i64)blockIdx.x * M2L_WARPS + wib; dst < n_dst; dst += (i64)gridDim.x * M2L_WARPS) {
-        i64 e0 = row_start[dst], e1 = row_start[dst + 1];
-        if (e0 == e1) continue;
-        double cx = dst_center[2 * dst], cy = dst_center[2 * dst + 1], hd = dst_half[dst];
-        float br[W], bi[W];
-        float a0r = 0.0f, a0i = 0.0f;
+    i64 e0, e1;
+    td3m2l::warp_entries(row_start, n_dst, (i64)blockIdx.x * M2L_WARPS + wib,
+                         (i64)gridDim.x * M2L_WARPS, e0, e1);
+    int carry_d = -1;
+    for (i64 base = e0; base < e1; base += 32) {
+        i64 e = base + lane;
+        bool live = e < e1;
+        int d = live ? entry_row[e] : -1;
+        float v[V];
 #pragma unroll
-        for (int l = 0; l < W; ++l) br[l] = bi[l] = 0.0f;
-        for (i64 base = e0; base < e1; base += 32) {
-            i64 e = base + lane;
-            if (e >= e1) continue;
+        for (int j = 0; j < V; ++j) v[j] = 0.0f;
+        if (live) {
             i64 src = partners[e];
+            double cx = dst_center[2 * d], cy = dst_center[2 * d + 1], hd = dst_half[d];
             double tr = cx - src_center[2 * src], ti = cy - src_center[2 * src + 1];
             double t2 = tr * tr + ti * ti, inv = 1.0 / t2, hs = src_half[src];
             float wsr = (float)(hs * tr * inv), wsi = (float)(-hs * ti * inv);
             float wdr = (float)(hd * tr * inv), wdi = (float)(-hd * ti * inv);
             float lnt = 0.5f * log_split(t2 * inv_unit2);
             const float2* a = hat + src * w;
-            float2 m0 = a[0];
-            a0r += m0.x;
-            a0i += m0.y;
             float ar[W], ai[W];
             float pr = 1.0f, pi = 0.0f;
 #pragma unroll
@@ -227,56 +229,39 @@ k_m2l_mixed(const i64* __restrict__ row_start, const i64* __restrict__ partners,
                     si += C.c[k * W + l] * ai[k];
                 }
                 if (l == 0) {
-                    br[0] += ar[0] * lnt - sr;
-                    bi[0] += ai[0] * lnt - si;
+                    v[0] = ar[0] * lnt - sr;
+                    v[1] = ai[0] * lnt - si;
                 } else {
                     float sign = (l & 1) ? 1.0f : -1.0f;
-                    br[l] += sign * (sr * qr - si * qi);
-                    bi[l] += sign * (sr * qi + si * qr);
+                    v[2 * l] = sign * (sr * qr - si * qi);
+                    v[2 * l + 1] = sign * (sr * qi + si * qr);
                 }
                 float nr = qr * wdr - qi * wdi;
                 qi = qr * wdi + qi * wdr;
                 qr = nr;
             }
+            v[2 * W] = ar[0];
+            v[2 * W + 1] = ai[0];
         }
-        for (int off = 16; off > 0; off >>= 1) {
-            a0r += __shfl_xor_sync(0xffffffffu, a0r, off);
-            a0i += __shfl_xor_sync(0xffffffffu, a0i, off);
-        }
-        double inv_h = 1.0 / hd, scale = 1.0;
-#pragma unroll
-        for (int l = 0; l < W; ++l) {
-            float vr = br[l], vi = bi[l];
-            for (int off = 16; off > 0; off >>= 1) {
-                vr += __shfl_xor_sync(0xffffffffu, vr, off);
-                vi += __shfl_xor_sync(0xffffffffu, vi, off);
-            }
-            if (lane == 0 && l < w) {
-                double ur = l ? 0.0 : ln_unit * a0r, ui = l ? 0.0 : ln_unit * a0i;
-                local_re[dst * w + l] += (double)vr * scale + ur;
-                local_im[dst * w + l] += (double)vi * scale + ui;
-            }
-            scale *= inv_h;
-        }
+        td3m2l::finish_round<W>(v, d, live, lane, base + 32, e1, entry_row, w, dst_half, ln_unit,
+                                local_re, local_im, carry[wib], carry_d);
     }
 }
 
 template <int P>
-int launch_m2l_mixed(const i64* row_start, const i64* partners, i64 n_dst, const double* dst_center,
-                     const double* dst_half, const double* src_center, const double* src_half,
-                     const float2* hat, int order, const double* coeff, double unit, double* lre,
-                     double* lim, cudaStream_t s) {
+int launch_m2l_mixed(const i64* row_start, const int* entry_row, const i64* partners, i64 n_dst,
+                     const double* dst_center, const double* dst_half, const double* src_center,
+                     const double* src_half, const float2* hat, int order, const double* coeff,
+                     double unit, double* lre, double* lim, cudaStream_t s) {
     // the reference's matrix, zero-padded from (order + 1)^2 to (P + 1)^2
     CoefTable<P> C;
     int w = order + 1;
     for (int k = 0; k <= P; ++k)
         for (int l = 0; l <= P; ++l)
             C.c[k * (P + 1) + l] = (k < w && l < w) ? (float)coeff[k * w + l] : 0.0f;
-    i64 blocks = (n_dst + M2L_WARPS - 1) / M2L_WARPS;
-    if (blocks > 148 * 64) blocks = 148 * 64;
-    k_m2l_mixed<P><<<(unsigned)blocks, 32 * M2L_WARPS, 0, s>>>(row_start, partners, n_dst,
-                                                                dst_center, dst_half, src_center,
-                                                                src_half, hat, order, C, unit, lre, lim);
+    k_m2l_mixed<P><<<148 * 16, 32 * M2L_WARPS, 0, s>>>(row_start, entry_row, partners, n_dst,
+                                                       dst_center, dst_half, src_center, src_half,
+                                                       hat, order, C, unit, lre, lim);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
@@ -329,29 +314,35 @@ extern "C" int td3_scale_moments(int64_t count, int order, const double* moment_
     return TD3_OK;
 }
 
-extern "C" int td3_fmm_m2l_mixed(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+extern "C" int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
+                                 const int64_t* partners, int64_t n_dst,
                                  const double* dst_center, const double* dst_half,
                                  const double* src_center, const double* src_half,
                                  const float* hat, int order, const double* coeff, double unit,
-                                 double* local_re, double* local_im, void* stream) {
+                                 int tensor_cores, double* local_re, double* local_im,
+                                 int64_t* status, void* stream) {
     if (n_dst < 0 || order < 0 || order > 20) return TD3_EINVAL;
     if (!(unit > 0.0 && unit < INFINITY)) return TD3_EINVAL;
+    if (tensor_cores && !status) return TD3_EINVAL;
     if (n_dst == 0) return TD3_OK;
     cudaStream_t s = td3_stream(stream);
     const float2* h = reinterpret_cast<const float2*>(hat);
+    if (tensor_cores && order <= 15)
+        return td3_m2l_tensor(row_start, entry_row, partners, n_dst, dst_center, dst_half, src_center,
+                              src_half, h, order, coeff, unit, local_re, local_im, status, s);
     if (order <= 4)
-        return launch_m2l_mixed<4>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+        return launch_m2l_mixed<4>(row_start, entry_row, partners, n_dst, dst_center, dst_half, src_center,
                                    src_half, h, order, coeff, unit, local_re, local_im, s);
     if (order <= 8)
-        return launch_m2l_mixed<8>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+        return launch_m2l_mixed<8>(row_start, entry_row, partners, n_dst, dst_center, dst_half, src_center,
                                    src_half, h, order, coeff, unit, local_re, local_im, s);
     if (order <= 12)
-        return launch_m2l_mixed<12>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+        return launch_m2l_mixed<12>(row_start, entry_row, partners, n_dst, dst_center, dst_half, src_center,
                                     src_half, h, order, coeff, unit, local_re, local_im, s);
     if (order <= 16)
-        return launch_m2l_mixed<16>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+        return launch_m2l_mixed<16>(row_start, entry_row, partners, n_dst, dst_center, dst_half, src_center,
                                     src_half, h, order, coeff, unit, local_re, local_im, s);
-    return launch_m2l_mixed<20>(row_start, partners, n_dst, dst_center, dst_half, src_center,
+    return launch_m2l_mixed<20>(row_start, entry_row, partners, n_dst, dst_center, dst_half, src_center,
                                 src_half, h, order, coeff, unit, local_re, local_im, s);
 }
 

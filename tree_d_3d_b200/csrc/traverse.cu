@@ -347,9 +347,13 @@ __global__ void k_csr_keys(const Pair* __restrict__ pairs, i64 count, int mutual
     }
 }
 
-__global__ void k_widen_vals(const unsigned* __restrict__ in, i64 count, i64* __restrict__ out) {
+// partners (int64) and, when asked, the row of every entry (int32)
+__global__ void k_csr_out(const unsigned* __restrict__ vals, const unsigned* __restrict__ keys,
+                          i64 count, i64* __restrict__ partners, int* __restrict__ entry_row) {
     i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k < count) out[k] = in[k];
+    if (k >= count) return;
+    partners[k] = vals[k];
+    if (entry_row) entry_row[k] = (int)keys[k];
 }
 
 int bits_for(i64 v) {
@@ -406,8 +410,8 @@ extern "C" size_t td3_pair_csr_workspace_size(int64_t count, int mutual, int64_t
 }
 
 extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int64_t n_nodes,
-                            int64_t* row_start, int64_t* partners, void* workspace,
-                            size_t workspace_bytes, void* stream) {
+                            int64_t* row_start, int64_t* partners, int32_t* entry_row,
+                            void* workspace, size_t workspace_bytes, void* stream) {
     if (count < 0 || n_nodes < 1 || n_nodes >= 0x7fffffffLL) return TD3_EINVAL;
     cudaStream_t s = td3_stream(stream);
     TD3_TRY(cudaMemsetAsync(row_start, 0, sizeof(i64) * (n_nodes + 1), s));
@@ -430,7 +434,7 @@ extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int
                                       w.size - w.used, s));
     // valid entries sort before the invalid key n_nodes (row_start[n_nodes] of them); the
     // entries after them are widened too (partners holds e slots), so no host read
-    k_widen_vals<<<td3_blocks(e, 256), 256, 0, s>>>(vo, e, partners);
+    k_csr_out<<<td3_blocks(e, 256), 256, 0, s>>>(vo, ko, e, partners, entry_row);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }

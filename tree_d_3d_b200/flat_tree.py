@@ -171,6 +171,11 @@ def _m2l_coefficients(order: int, symmetric: bool) -> np.ndarray:
 #: partners per near-field work segment (one warp each)
 NEAR_SEGMENT = 256
 
+#: mixed-precision M2L matrix products on the tensor cores (tcgen05, 3xTF32; orders up
+#: to 15) instead of FP32 CUDA-core arithmetic.  Off by default: the tensor-core form is
+#: correct but, waiting on each 128-row tile, still slower than the CUDA-core form.
+M2L_TENSOR_CORES = False
+
 
 def _nearfield_plan(rows: torch.Tensor, tree, entries: int) -> dict:
     """The near-field work plan of one tree's leaf rows (td3_nearfield_plan): leaf rows
@@ -533,29 +538,34 @@ class FlatQuadtree:
                 return m2l[: sizes[0]], p2p[: sizes[1]]
             capacity = np.maximum(2 * capacity, sizes[:3] + 64)
 
-    def _rows(self, pairs: torch.Tensor, mutual: bool, n_nodes: int | None = None):
-        """pair_csr (K/pair_csr/pair_csr_pyccel.py:12-45): rows by node of ``pairs``."""
+    def _rows(self, pairs: torch.Tensor, mutual: bool, n_nodes: int | None = None,
+              entry_rows: bool = False):
+        """pair_csr (K/pair_csr/pair_csr_pyccel.py:12-45): rows by node of ``pairs``;
+        with ``entry_rows`` also the row of every entry (int32)."""
         dev = self.device
         n_nodes = self.node_count if n_nodes is None else n_nodes
         count = pairs.shape[0]
         rows = torch.zeros(n_nodes + 1, dtype=torch.int64, device=dev)
-        partners = torch.empty(max((2 if mutual else 1) * count, 1), dtype=torch.int64, device=dev)
+        slots = max((2 if mutual else 1) * count, 1)
+        partners = torch.empty(slots, dtype=torch.int64, device=dev)
+        entry = torch.empty(slots, dtype=torch.int32, device=dev) if entry_rows else None
         ws = _lib.workspace(_lib.query("td3_pair_csr_workspace_size", count, int(mutual), n_nodes),
                             dev)
         _lib.call("td3_pair_csr", pairs.data_ptr(), count, int(mutual), n_nodes, rows.data_ptr(),
-                  partners.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream(dev))
-        return rows, partners
+                  partners.data_ptr(), 0 if entry is None else entry.data_ptr(), ws.data_ptr(),
+                  ws.numel(), _lib.stream(dev))
+        return (rows, partners, entry) if entry_rows else (rows, partners)
 
     def _lists(self, theta: float) -> dict:
         """The interaction lists of ``theta``, their rows and the near-field plan, kept
         across set_charges (ft:1496-1498): they depend on the cells only."""
         if theta not in self._traversals:
             m2l, p2p = self._traverse(theta)
-            m2l_rows, m2l_partners = self._rows(m2l, mutual=True)
+            m2l_rows, m2l_partners, m2l_entry = self._rows(m2l, mutual=True, entry_rows=True)
             p2p_rows, p2p_partners = self._rows(p2p, mutual=True)
             lists = {
                 "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
-                "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
+                "m2l_entry_row": m2l_entry, "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
             }
             lists["plan"] = _nearfield_plan(p2p_rows, self, 2 * p2p.shape[0])
             self._traversals[theta] = lists
@@ -591,6 +601,7 @@ class FlatQuadtree:
         self._evaluate_near(lists, _lib.KERNEL_LOG, local_re, local_im, softening, potential,
                             phi, field, status)
         _check(status)
+        self._check_tensor_cores()
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
         return out((phi, field), self._numpy)
 
@@ -603,8 +614,7 @@ class FlatQuadtree:
         local_im = torch.zeros((count, w), dtype=torch.float64, device=dev)
         stream = _lib.stream(dev)
         if lists["m2l"].shape[0]:
-            self._m2l_log(lists["m2l_rows"], lists["m2l_partners"], self, (mre, mim), local_re,
-                          local_im)
+            self._m2l_log(lists, self, (mre, mim), local_re, local_im)
         levels = np.ascontiguousarray(self.levels, dtype=np.int64)
         binom = self._binomial()
         _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
@@ -647,19 +657,39 @@ class FlatQuadtree:
                   _lib.stream(self.device))
         return hat
 
-    def _m2l_log(self, rows, partners, dst, moments, local_re, local_im):
-        """Log-kernel M2L from this tree's cells into ``dst``'s: FP64, or FP32 on moments
-        scaled by the cell size for ``precision="mixed"`` (orders up to 20)."""
+    def _tensor_status(self) -> torch.Tensor:
+        """The device word the tensor-core M2L raises when a wait for the tensor cores
+        runs out (checked by _check_tensor_cores)."""
+        if getattr(self, "_tc_status", None) is None:
+            self._tc_status = status_word(self.device)
+        return self._tc_status
+
+    def _check_tensor_cores(self) -> None:
+        """Raise if a tensor-core M2L of this tree did not complete (reads the word)."""
+        word = getattr(self, "_tc_status", None)
+        if word is not None and int(word.item()) != 0:
+            word.zero_()
+            raise RuntimeError("the tensor cores did not complete an M2L (a bounded wait ran "
+                               "out); the local expansions are incomplete")
+
+    def _m2l_log(self, lists, dst, moments, local_re, local_im):
+        """Log-kernel M2L from this tree's cells into ``dst``'s over the rows of
+        ``lists``: FP64, or FP32 on moments scaled by the cell size for
+        ``precision="mixed"`` (orders up to 20), the matrix products on the tensor cores
+        for orders up to 15 (M2L_TENSOR_CORES)."""
         stream = _lib.stream(self.device)
         mre, mim = moments
+        rows, partners = lists["m2l_rows"], lists["m2l_partners"]
         if self.precision == "mixed" and self.order <= 20:
             hat = self._scaled_moments(moments)
             coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
-            _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), partners.data_ptr(), dst.node_count,
+            tensor = 1 if M2L_TENSOR_CORES and self.order <= 15 else 0
+            _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), lists["m2l_entry_row"].data_ptr(),
+                      partners.data_ptr(), dst.node_count,
                       dst.node_center.data_ptr(), dst.node_half.data_ptr(),
                       self.node_center.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(),
-                      self.order, coeff.ctypes.data, self._unit, local_re.data_ptr(),
-                      local_im.data_ptr(), stream)
+                      self.order, coeff.ctypes.data, self._unit, tensor, local_re.data_ptr(),
+                      local_im.data_ptr(), self._tensor_status().data_ptr(), stream)
             return
         _lib.call("td3_fmm_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                   dst.node_center.data_ptr(), self.node_center.data_ptr(), mre.data_ptr(),
@@ -729,6 +759,7 @@ class FlatQuadtree:
                   partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), efield.data_ptr(),
                   float(softening), self._mixed, self._unit, qbar.data_ptr(), xbar.data_ptr(),
                   stream)
+        self._check_tensor_cores()
         return qbar, xbar
 
     def _move_within_cells(self, positions) -> None:
@@ -774,11 +805,12 @@ class FlatQuadtree:
                 break
             capacity = np.maximum(2 * capacity, sizes[:3] + 64)
         m2l, p2p = m2l[: sizes[0]], p2p[: sizes[1]]
-        m2l_rows, m2l_partners = self._rows(m2l, mutual=False, n_nodes=tree.node_count)
+        m2l_rows, m2l_partners, m2l_entry = self._rows(m2l, mutual=False,
+                                                       n_nodes=tree.node_count, entry_rows=True)
         p2p_rows, p2p_partners = self._rows(p2p, mutual=False, n_nodes=tree.node_count)
         return {
             "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
-            "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
+            "m2l_entry_row": m2l_entry, "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
             "plan": _nearfield_plan(p2p_rows, tree, p2p.shape[0]),
         }
 
@@ -835,8 +867,7 @@ class FlatQuadtree:
             local_a = torch.zeros((tree.node_count, w), dtype=torch.float64, device=dev)
             local_b = torch.zeros_like(local_a)
             if n_m2l:
-                self._m2l_log(lists["m2l_rows"], lists["m2l_partners"], tree,
-                              (self.moment_re, self.moment_im), local_a, local_b)
+                self._m2l_log(lists, tree, (self.moment_re, self.moment_im), local_a, local_b)
             levels = np.ascontiguousarray(tree.levels, dtype=np.int64)
             binom = self._binomial()
             _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
@@ -863,6 +894,7 @@ class FlatQuadtree:
             self._unit,
             phi.data_ptr(), field.data_ptr(), status.data_ptr(), stream)
         _check(status)
+        self._check_tensor_cores()
         if not potential:
             phi.zero_()
         return out((phi, field), as_numpy)
