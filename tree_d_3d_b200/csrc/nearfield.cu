@@ -194,61 +194,91 @@ struct Targets {
     i64 m;
 };
 
-// The mixed-precision near field of one target over a run of partner leaves: the pair
-// difference in FP64 (exact enough for close pairs far from the origin), in units of
-// S.unit = L and rounded to FP32, then FP32 kernel arithmetic with compensated
-// accumulation.  Coulomb: phi = sum q / r' / L, E = sum q d' / r'^3 / L^2; log:
-// phi = sum -q ln r'^2 - ln L^2 sum q (the charge sum in FP64), E = sum 2 q d' / r'^2 / L.
-template <int KERNEL, bool POT, bool OTHER>
-__device__ __forceinline__ void near_mixed(const Sources& S, const i64* __restrict__ partners,
-                                           i64 e_begin, i64 e_end, int step, double xi, double yi,
-                                           double qi, i64 k, i64 skip, double eps2, double& pot,
-                                           double& ex, double& ey, bool& bad) {
-    KahanF p, x, y;
-    double inv_unit = 1.0 / S.unit, qsum = 0.0;
-    float eps2f = (float)(eps2 * inv_unit * inv_unit);
-    for (i64 e = e_begin; e < e_end; e += step) {
-        i64 b = partners[e];
-        i64 b1 = S.end[b];
-        for (i64 j = S.start[b]; j < b1; ++j) {
-            double qj = S.charge[j];
-            if (OTHER) {
-                if (qj == 0.0 || S.index[j] == skip) continue;
-            } else if (j == k) {
-                continue;
-            }
-            double dx64 = xi - S.pos[j], dy64 = yi - S.pos[S.n + j];
-            if (dx64 == 0.0 && dy64 == 0.0 && eps2 == 0.0) {
-                bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
-                continue;
-            }
-            float dx = (float)(dx64 * inv_unit), dy = (float)(dy64 * inv_unit), q = (float)qj;
-            float r2 = dx * dx + dy * dy + eps2f;
-            if (KERNEL == TD3_KERNEL_LOG) {
-                if (POT) {
-                    p.add(-q * __logf(r2));
-                    qsum += qj;
+// ------------------------------------------------------------------ staged sources
+// The source particles of a segment's partner leaves pass through shared memory: the
+// warp takes 32 partner leaves at a time (lane i reads leaf i's range; a warp scan of
+// the counts places them), copies their particles in windows of up to CAP (every lane
+// loads independent particles, so the loads overlap), and then every (target, slice)
+// lane sums over the window.  Each target still meets every source once, in a fixed
+// order (window by window, slice-strided inside a window, slices added last).
+//
+// stage(p, j): store source slot j at window position p (called by one lane);
+// body(wn): sum over the window's wn staged particles (called by every lane).
+template <int CAP, class Stage, class Body>
+__device__ __forceinline__ void for_source_windows(const Sources& S,
+                                                   const i64* __restrict__ partners, i64 e0,
+                                                   i64 e1, int lane, Stage stage, Body body) {
+    for (i64 g = e0; g < e1; g += 32) {
+        i64 i = g + lane;
+        i64 st = 0;
+        int cnt = 0;
+        if (i < e1) {
+            i64 b = partners[i];
+            st = S.start[b];
+            cnt = (int)(S.end[b] - st);
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        int total = __shfl_sync(0xffffffffu, incl, 31);
+        int excl = incl - cnt;
+        for (int w0 = 0; w0 < total; w0 += CAP) {
+            int wn = total - w0 < CAP ? total - w0 : CAP;
+            for (int p0 = 0; p0 < wn; p0 += 32) {
+                int p = p0 + lane;
+                int at = w0 + (p < wn ? p : 0);
+                // the leaf holding position `at`: the last lane whose offset is <= at
+                int L = 0;
+#pragma unroll
+                for (int s = 16; s > 0; s >>= 1) {
+                    int v = __shfl_sync(0xffffffffu, excl, L + s);
+                    if (v <= at) L += s;
                 }
-                float f = __fdividef(2.0f * q, r2);
-                x.add(f * dx);
-                y.add(f * dy);
-            } else {
-                float inv_r = rsqrtf(r2);
-                float qr3 = q * inv_r * inv_r * inv_r;
-                p.add(q * inv_r);
-                x.add(qr3 * dx);
-                y.add(qr3 * dy);
+                i64 stL = __shfl_sync(0xffffffffu, st, L);
+                int exL = __shfl_sync(0xffffffffu, excl, L);
+                if (p < wn) stage(p, stL + (at - exL));
             }
+            __syncwarp();
+            body(wn);
+            __syncwarp();
         }
     }
+}
+
+constexpr int NF_CAP = 256;  // staged sources per warp window (forward)
+
+struct NearWindow {
+    double x[NF_CAP], y[NF_CAP], q[NF_CAP];
+    int tag[NF_CAP];  // slot j (self-exclusion) or the source's input index (OTHER)
+};
+
+// One mixed-precision pair: the difference in FP64 (exact enough for close pairs far
+// from the origin), in units of L = S.unit and rounded to FP32, then FP32 arithmetic with
+// compensated accumulation.  Coulomb sums q / r' and q d' / r'^3; log sums -q ln r'^2
+// (with the charges in FP64, qsum) and 2 q d' / r'^2.
+template <int KERNEL, bool POT>
+__device__ __forceinline__ void pair_mixed(double dx64, double dy64, double qj, double inv_unit,
+                                           float eps2f, KahanF& p, KahanF& x, KahanF& y,
+                                           double& qsum) {
+    float dx = (float)(dx64 * inv_unit), dy = (float)(dy64 * inv_unit), q = (float)qj;
+    float r2 = dx * dx + dy * dy + eps2f;
     if (KERNEL == TD3_KERNEL_LOG) {
-        pot = p.value() - 2.0 * log(S.unit) * qsum;
-        ex = x.value() * inv_unit;
-        ey = y.value() * inv_unit;
+        if (POT) {
+            p.add(-q * __logf(r2));
+            qsum += qj;
+        }
+        float f = __fdividef(2.0f * q, r2);
+        x.add(f * dx);
+        y.add(f * dy);
     } else {
-        pot = p.value() * inv_unit;
-        ex = x.value() * inv_unit * inv_unit;
-        ey = y.value() * inv_unit * inv_unit;
+        float inv_r = rsqrtf(r2);
+        float qr3 = q * inv_r * inv_r * inv_r;
+        p.add(q * inv_r);
+        x.add(qr3 * dx);
+        y.add(qr3 * dy);
     }
 }
 
@@ -256,7 +286,8 @@ __device__ __forceinline__ void near_mixed(const Sources& S, const i64* __restri
 // zero charges and source exclude[i] are skipped and any coincidence is an error.
 // Otherwise targets are the sources themselves: a particle skips itself and a
 // coincident pair is an error only if both charges are nonzero.  MIXED: FP32 pair
-// arithmetic with compensated sums (near_mixed), else FP64.
+// arithmetic with compensated sums (pair_mixed), else FP64.  The sources come through
+// shared memory (for_source_windows).
 template <int KERNEL, bool POT, bool OTHER, int LOCAL, bool MIXED>
 __global__ void __launch_bounds__(32 * NF_WARPS)
 k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
@@ -265,7 +296,9 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
        const double* __restrict__ local_b, int order, int width, double eps2,
        double* __restrict__ partial, double* __restrict__ phi, double* __restrict__ field,
        i64* status) {
+    __shared__ NearWindow windows[NF_WARPS];
     int lane = threadIdx.x & 31;
+    NearWindow& win = windows[threadIdx.x >> 5];
     i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     i64 leaf = seg_leaf[seg];
@@ -276,6 +309,14 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
     int tsz = pow2_at_least(count < 32 ? count : 32);
     int slices = 32 / tsz;
     int ti = lane % tsz, slice = lane / tsz;
+    const double inv_unit = 1.0 / S.unit;
+    const float eps2f = (float)(eps2 * inv_unit * inv_unit);
+    auto stage = [&](int p, i64 j) {
+        win.x[p] = S.pos[j];
+        win.y[p] = S.pos[S.n + j];
+        win.q[p] = S.charge[j];
+        win.tag[p] = OTHER ? (int)S.index[j] : (int)j;
+    };
     for (int base = 0; base < count; base += tsz) {
         int it = base + ti;
         bool valid = it < count;
@@ -285,39 +326,56 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
         i64 skip = OTHER ? (T.exclude ? T.exclude[k] : -1) : k;
         double pot = 0.0, ex = 0.0, ey = 0.0;
         bool bad = false;
-        if (valid && MIXED) {
-            near_mixed<KERNEL, POT, OTHER>(S, partners, er.x + slice, er.y, slices, xi, yi, qi, k,
-                                           skip, eps2, pot, ex, ey, bad);
-        } else if (valid) {
-            for (i64 e = er.x + slice; e < er.y; e += slices) {
-                i64 b = partners[e];
-                i64 b1 = S.end[b];
-                for (i64 j = S.start[b]; j < b1; ++j) {
-                    double qj = S.charge[j];
-                    if (OTHER) {
-                        if (qj == 0.0 || S.index[j] == skip) continue;
-                    } else if (j == skip) {
-                        continue;
-                    }
-                    double dx = xi - S.pos[j], dy = yi - S.pos[S.n + j];
-                    double r2 = dx * dx + dy * dy + eps2;
-                    if (r2 == 0.0) {
+        KahanF kp, kx, ky;
+        double qsum = 0.0;
+        for_source_windows<NF_CAP>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
+            if (!valid) return;
+            for (int p = slice; p < wn; p += slices) {
+                double qj = win.q[p];
+                i64 tag = win.tag[p];
+                if (OTHER) {
+                    if (qj == 0.0 || tag == skip) continue;
+                } else if (tag == skip) {
+                    continue;
+                }
+                double dx = xi - win.x[p], dy = yi - win.y[p];
+                if (MIXED) {
+                    if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) {
                         bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
                         continue;
                     }
-                    if (KERNEL == TD3_KERNEL_LOG) {
-                        if (POT) pot -= qj * log(r2);
-                        double f = 2.0 * qj / r2;
-                        ex += f * dx;
-                        ey += f * dy;
-                    } else {
-                        double inv_r = rsqrt(r2);
-                        double inv_r3 = inv_r * inv_r * inv_r;
-                        pot += qj * inv_r;
-                        ex += qj * inv_r3 * dx;
-                        ey += qj * inv_r3 * dy;
-                    }
+                    pair_mixed<KERNEL, POT>(dx, dy, qj, inv_unit, eps2f, kp, kx, ky, qsum);
+                    continue;
                 }
+                double r2 = dx * dx + dy * dy + eps2;
+                if (r2 == 0.0) {
+                    bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
+                    continue;
+                }
+                if (KERNEL == TD3_KERNEL_LOG) {
+                    if (POT) pot -= qj * log(r2);
+                    double f = 2.0 * qj / r2;
+                    ex += f * dx;
+                    ey += f * dy;
+                } else {
+                    double inv_r = rsqrt(r2);
+                    double inv_r3 = inv_r * inv_r * inv_r;
+                    pot += qj * inv_r;
+                    ex += qj * inv_r3 * dx;
+                    ey += qj * inv_r3 * dy;
+                }
+            }
+        });
+        if (MIXED) {
+            // back from units of L: Coulomb 1/L, 1/L^2; log -ln L^2 sum q, 1/L
+            if (KERNEL == TD3_KERNEL_LOG) {
+                pot = kp.value() - 2.0 * log(S.unit) * qsum;
+                ex = kx.value() * inv_unit;
+                ey = ky.value() * inv_unit;
+            } else {
+                pot = kp.value() * inv_unit;
+                ex = kx.value() * inv_unit * inv_unit;
+                ey = ky.value() * inv_unit * inv_unit;
             }
         }
         for (int off = tsz; off < 32; off <<= 1) {
@@ -506,6 +564,14 @@ __device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, 
     A.xbar[n + i] = -w * A.efield[n + i] + q * gy - (mxy * ex + myy * ey);
 }
 
+constexpr int NF_CAP_ADJ = 128;  // staged sources per warp window (adjoint)
+
+struct AdjointWindow {
+    double x[NF_CAP_ADJ], y[NF_CAP_ADJ], q[NF_CAP_ADJ], w[NF_CAP_ADJ], ex[NF_CAP_ADJ],
+        ey[NF_CAP_ADJ];
+    int tag[NF_CAP_ADJ];  // slot j (self-exclusion)
+};
+
 template <int KERNEL, int LOCAL, bool MIXED>
 __global__ void __launch_bounds__(32 * NF_WARPS)
 k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
@@ -514,7 +580,9 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
                const double* __restrict__ fb, const double* __restrict__ ba,
                const double* __restrict__ bb, int order, int width, double eps2,
                double* __restrict__ partial) {
+    __shared__ AdjointWindow windows[NF_WARPS];
     int lane = threadIdx.x & 31;
+    AdjointWindow& win = windows[threadIdx.x >> 5];
     i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     i64 leaf = seg_leaf[seg];
@@ -526,51 +594,54 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
     int slices = 32 / tsz;
     int ti = lane % tsz, slice = lane / tsz;
     i64 n = S.n;
+    // mixed: in units of L = S.unit (d' = d / L, e' = e / L) the log kernel's sums scale
+    // as (1, 1/L, 1/L^2) plus -ln L^2 sum w for Psi, the Coulomb kernel's as
+    // (1/L, 1/L^2, 1/L^3)
+    const double inv_unit = 1.0 / S.unit;
+    const float eps2f = (float)(eps2 * inv_unit * inv_unit);
+    auto stage = [&](int p, i64 j) {
+        win.x[p] = S.pos[j];
+        win.y[p] = S.pos[n + j];
+        win.q[p] = S.charge[j];
+        win.w[p] = A.weight[j];
+        win.ex[p] = A.dipole[j];
+        win.ey[p] = A.dipole[n + j];
+        win.tag[p] = (int)j;
+    };
     for (int base = 0; base < count; base += tsz) {
         int it = base + ti;
         bool valid = it < count;
         i64 k = s0 + (valid ? it : 0);
         double xi = S.pos[k], yi = S.pos[n + k];
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        if (valid && MIXED) {
-            // in units of L = S.unit (d' = d / L, e' = e / L): the log kernel's sums scale
-            // as (1, 1/L, 1/L^2) plus -ln L^2 sum w for Psi, the Coulomb kernel's as
-            // (1/L, 1/L^2, 1/L^3)
-            KahanF kacc[6];
-            double inv_unit = 1.0 / S.unit, wsum = 0.0;
-            float eps2f = (float)(eps2 * inv_unit * inv_unit);
-            for (i64 e = er.x + slice; e < er.y; e += slices) {
-                i64 b = partners[e];
-                i64 b1 = S.end[b];
-                for (i64 j = S.start[b]; j < b1; ++j) {
-                    if (j == k) continue;
-                    double dx = xi - S.pos[j], dy = yi - S.pos[n + j];
+        KahanF kacc[6];
+        double wsum = 0.0;
+        for_source_windows<NF_CAP_ADJ>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
+            if (!valid) return;
+            for (int p = slice; p < wn; p += slices) {
+                if (win.tag[p] == k) continue;
+                double dx = xi - win.x[p], dy = yi - win.y[p];
+                if (MIXED) {
                     if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) continue;
-                    double wj = A.weight[j];
+                    double wj = win.w[p];
                     if (KERNEL == TD3_KERNEL_LOG) wsum += wj;
-                    adjoint_pair_mixed<KERNEL>(
-                        (float)(dx * inv_unit), (float)(dy * inv_unit), eps2f, (float)S.charge[j],
-                        (float)wj, (float)(A.dipole[j] * inv_unit),
-                        (float)(A.dipole[n + j] * inv_unit), kacc);
-                }
-            }
-            double s0 = KERNEL == TD3_KERNEL_LOG ? 1.0 : inv_unit;
-            acc[0] = kacc[0].value() * s0;
-            if (KERNEL == TD3_KERNEL_LOG) acc[0] -= 2.0 * log(S.unit) * wsum;
-            for (int c = 1; c < 3; ++c) acc[c] = kacc[c].value() * (s0 * inv_unit);
-            for (int c = 3; c < 6; ++c) acc[c] = kacc[c].value() * (s0 * inv_unit * inv_unit);
-        } else if (valid) {
-            for (i64 e = er.x + slice; e < er.y; e += slices) {
-                i64 b = partners[e];
-                i64 b1 = S.end[b];
-                for (i64 j = S.start[b]; j < b1; ++j) {
-                    if (j == k) continue;
-                    double dx = xi - S.pos[j], dy = yi - S.pos[n + j];
+                    adjoint_pair_mixed<KERNEL>((float)(dx * inv_unit), (float)(dy * inv_unit),
+                                               eps2f, (float)win.q[p], (float)wj,
+                                               (float)(win.ex[p] * inv_unit),
+                                               (float)(win.ey[p] * inv_unit), kacc);
+                } else {
                     if (dx * dx + dy * dy + eps2 == 0.0) continue;
-                    adjoint_pair<KERNEL>(dx, dy, eps2, S.charge[j], A.weight[j], A.dipole[j],
-                                         A.dipole[n + j], acc);
+                    adjoint_pair<KERNEL>(dx, dy, eps2, win.q[p], win.w[p], win.ex[p], win.ey[p],
+                                         acc);
                 }
             }
+        });
+        if (MIXED) {
+            double sc = KERNEL == TD3_KERNEL_LOG ? 1.0 : inv_unit;
+            acc[0] = kacc[0].value() * sc;
+            if (KERNEL == TD3_KERNEL_LOG) acc[0] -= 2.0 * log(S.unit) * wsum;
+            for (int c = 1; c < 3; ++c) acc[c] = kacc[c].value() * (sc * inv_unit);
+            for (int c = 3; c < 6; ++c) acc[c] = kacc[c].value() * (sc * inv_unit * inv_unit);
         }
 #pragma unroll
         for (int c = 0; c < 6; ++c)
