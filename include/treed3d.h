@@ -102,10 +102,12 @@ int td3_pair_energy(const double* pos, const double* charge, int64_t n, double s
  * node_center (capacity, 2), node_half, node_start, node_end, node_child (-1 for
  * leaves), node_depth), perm (n; the particles in tree order) and sorted_pos (2, n;
  * pos[:, perm]).  levels (HOST, capacity + 1) receives the first node of each depth;
- * sizes (HOST, 3) receives node count, number of levels and 1 if capacity was too
+ * sizes (HOST, 4) receives node count, number of levels and 1 if capacity was too
  * small (then TD3_ENEEDMORE is returned, the tree is unfinished and sizes[0] is the
  * node count needed, or a lower bound of it: retry with a larger capacity, as the
- * reference doubles it).  Synchronises `stream` once (twice for trees deeper than 16
+ * reference doubles it); sizes[3] is 1 if a position is not finite, 2 if one lies
+ * outside the root cell (the inputs FlatQuadtree rejects, src/tree_d_3d/flat_tree.py:
+ * 788-794), and TD3_EINVAL is returned.  Synchronises `stream` once (twice for trees deeper than 16
  * levels; once per level for trees deeper than 32 levels).
  * Replaces quadtree_build (src/tree_d_3d/kernels/quadtree_build/quadtree_build_pyccel.py:
  * 12-137) and the GPU level kernels quadtree_quadrants / quadtree_scatter

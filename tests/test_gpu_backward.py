@@ -147,3 +147,23 @@ def test_backward_matches_central_finite_differences(kernel):
     assert np.max(np.abs(fd_x - bw_x)) < 1e-5 * np.max(np.abs(bw_x))
     fd_q, bw_q = np.array(fd_q), np.array(bw_q)
     assert np.max(np.abs(fd_q - bw_q)) < 1e-5 * np.max(np.abs(bw_q))
+
+
+def test_coincident_charges_are_reported_at_forward_or_after_backward():
+    """Without gradients fmm_field raises at the forward like FlatQuadtree.fmm; with
+    gradients the same ValueError comes at the end of the backward (the forward does
+    not wait for the GPU)."""
+    from tree_d_3d_b200 import Quad
+    from tree_d_3d_b200.autograd import fmm_field
+
+    rng = np.random.default_rng(5)
+    pos = rng.uniform(-0.9, 0.9, (2, 3000))
+    pos[:, 1] = pos[:, 0]  # two charged particles on one point, unsoftened
+    q = np.ones(3000)
+    P, Q = torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda")
+    with pytest.raises(ValueError, match="Coincident"):
+        fmm_field(P, Q, Quad(0, 0, 1), kernel="log", order=8)
+    Qg = Q.clone().requires_grad_(True)
+    phi, _ = fmm_field(P, Qg, Quad(0, 0, 1), kernel="log", order=8)
+    with pytest.raises(ValueError, match="Coincident"):
+        phi.sum().backward()

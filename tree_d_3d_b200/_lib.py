@@ -93,6 +93,15 @@ def call(name: str, *args) -> int:
     return rc
 
 
+def call_code(name: str, *args) -> int:
+    """Call entry point ``name`` and return its code; raise LibraryError only for a CUDA
+    failure (the caller interprets the other codes)."""
+    rc = getattr(lib(), name)(*args)
+    if rc == ECUDA:
+        raise LibraryError(f"{name} failed with code {rc} {lib().td3_last_error().decode()}")
+    return rc
+
+
 def query(name: str, *args) -> int:
     """A size query (``*_workspace_size``)."""
     return int(getattr(lib(), name)(*args))

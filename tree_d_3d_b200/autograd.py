@@ -11,12 +11,18 @@ Psi the potential of monopoles w and dipoles e at the sources: one transposed FM
 the Hessian of the forward expansions and kernel Hessian-vector products in P2P
 (``FlatQuadtree._fmm_adjoint``).  The tree and its interaction lists are built in the
 forward and kept for the backward; the tree topology is not differentiated.
+
+When the positions or charges require gradients, the check for coincident charges of
+the forward (the ValueError of ``FlatQuadtree.fmm``) is read at the end of the backward,
+so that the host queues the loss and the backward without waiting for the GPU; call
+without gradients for the check at the forward.
 """
 
 from __future__ import annotations
 
 import torch
 
+from tree_d_3d_b200._utils import _check, status_word
 from tree_d_3d_b200.flat_tree import FlatQuadtree
 from tree_d_3d_b200.quad import Quad
 
@@ -29,8 +35,14 @@ class _FMMField(torch.autograd.Function):
                             leaf_capacity=options["leaf_capacity"],
                             max_depth=options["max_depth"], symmetric=options["symmetric"],
                             precision=options["precision"])
-        phi, field = tree.fmm(theta=options["theta"], softening=options["softening"])
+        # with gradients on, the forward's coincident-charge report is read after the
+        # backward has been queued, so the host does not wait for the GPU here
+        deferred = any(ctx.needs_input_grad[:2])
+        status = status_word(tree.device) if deferred else None
+        phi, field = tree.fmm(theta=options["theta"], softening=options["softening"],
+                              _status=status)
         ctx.tree = tree
+        ctx.status = status
         ctx.options = options
         ctx.save_for_backward(field)
         return phi, field
@@ -47,6 +59,9 @@ class _FMMField(torch.autograd.Function):
             grad_field = torch.zeros_like(field)
         qbar, xbar = tree._fmm_adjoint(ctx.options["theta"], ctx.options["softening"],
                                        grad_phi.contiguous(), grad_field.contiguous(), field)
+        if ctx.status is not None:
+            _check(ctx.status)
+            tree._check_tensor_cores()
         return xbar, qbar, None, None
 
 

@@ -211,10 +211,14 @@ struct KeyLevels {
 };
 
 struct KeySummary {
+    int invalid;      // 1: a position is not finite, 2: a position lies outside the root
+    int deeper;       // a node at the last key digit still splits
     i64 split_total;  // splitting nodes
     int count[KEY_DIGITS];
-    int deeper;       // a node at the last key digit still splits
 };
+
+constexpr int INVALID_NONFINITE = 1;
+constexpr int INVALID_OUTSIDE = 2;
 
 __device__ __forceinline__ int key_cpl(unsigned long long a, unsigned long long b, int digits) {
     unsigned long long x = a ^ b;
@@ -231,10 +235,15 @@ __device__ __forceinline__ int key_digit(unsigned long long key, int i, int digi
 __global__ void k_path_keys(const double* __restrict__ pos, i64 n, double xmid, double ymid,
                             double half, int digits, int prefix_shift,
                             unsigned long long* __restrict__ key, unsigned* __restrict__ prefix,
-                            unsigned* __restrict__ index) {
+                            unsigned* __restrict__ index, KeySummary* summary) {
     i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     double x = pos[k], y = pos[n + k];
+    // the inputs the reference rejects (ft:788-794): not finite, or outside the root
+    if (!(isfinite(x) && isfinite(y)))
+        atomicOr(&summary->invalid, INVALID_NONFINITE);
+    else if (x < xmid - half || x > xmid + half || y < ymid - half || y > ymid + half)
+        atomicOr(&summary->invalid, INVALID_OUTSIDE);
     double cx = xmid, cy = ymid, h = half;
     unsigned long long v = 0;
     for (int d = 0; d < digits; ++d) {
@@ -497,7 +506,9 @@ int key_pass(const KeyBuffers& b, i64 n, int total, int digits, i64 leaf_capacit
     k_gather_keys<<<nb, BUILD_THREADS, 0, s>>>(n, b.key, vo, 2 * (total - digits), b.skey);
     if (vo != b.v0)
         TD3_TRY(cudaMemcpyAsync(b.v0, vo, sizeof(unsigned) * n, cudaMemcpyDeviceToDevice, s));
-    TD3_TRY(cudaMemsetAsync(b.summary, 0, sizeof(KeySummary), s));
+    // clear all but `invalid`, which the path-key pass wrote
+    TD3_TRY(cudaMemsetAsync(&b.summary->deeper, 0, sizeof(KeySummary) - offsetof(KeySummary, deeper),
+                            s));
     k_split_depths<<<nb, BUILD_THREADS, 0, s>>>(b.skey, n, digits, leaf_capacity, max_depth,
                                                 b.first, b.len, b.summary);
     TD3_CHECK_LAUNCH();
@@ -520,11 +531,16 @@ int build_by_keys(const double* pos, i64 n, double xmid, double ymid, double hal
     int total = max_depth < KEY_DIGITS ? (int)max_depth : KEY_DIGITS;
     int digits = total < PREFIX_DIGITS ? total : PREFIX_DIGITS;
     unsigned nb = td3_blocks(n, BUILD_THREADS);
+    TD3_TRY(cudaMemsetAsync(&b.summary->invalid, 0, sizeof(int), s));
     k_path_keys<<<nb, BUILD_THREADS, 0, s>>>(pos, n, xmid, ymid, half, total, 2 * (total - digits),
-                                             b.key, b.u0, b.v0);
+                                             b.key, b.u0, b.v0, b.summary);
     TD3_CHECK_LAUNCH();
     KeySummary host;
     TD3_TRY_RC(key_pass(b, n, total, digits, leaf_capacity, max_depth, host, s));
+    if (host.invalid) {
+        sizes[3] = (host.invalid & INVALID_NONFINITE) ? 1 : 2;
+        return TD3_EINVAL;
+    }
     if (host.deeper && digits < total) {
         digits = total;
         TD3_TRY_RC(key_pass(b, n, total, digits, leaf_capacity, max_depth, host, s));
@@ -605,6 +621,7 @@ extern "C" int td3_quadtree_build(const double* pos, int64_t n, double xmid, dou
     if (n < 1 || n > 0x7fffffffLL || leaf_capacity < 1 || max_depth < 0 || capacity < 1)
         return TD3_EINVAL;
     cudaStream_t s = td3_stream(stream);
+    sizes[3] = 0;
     {
         Workspace wk(workspace, workspace_bytes);
         bool levelwise = false;

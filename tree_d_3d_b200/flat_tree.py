@@ -257,14 +257,7 @@ class FlatQuadtree:
         n = self.pos.shape[1]
         if self.charge.shape[0] != n:
             raise ValueError("positions and charges must have the same length")
-        if not bool(torch.isfinite(self.pos).all()):
-            raise ValueError("Particle position must be finite")
-        lo = torch.tensor([[root_quad.xmid - root_quad.half], [root_quad.ymid - root_quad.half]],
-                          dtype=torch.float64, device=self.device)
-        hi = torch.tensor([[root_quad.xmid + root_quad.half], [root_quad.ymid + root_quad.half]],
-                          dtype=torch.float64, device=self.device)
-        if bool((self.pos < lo).any()) or bool((self.pos > hi).any()):
-            raise ValueError("Particle lies outside tree bounds")
+        # finite positions inside the root (ft:788-794) are checked by the build itself
         self.leaf_capacity = int(leaf_capacity)
         self.max_depth = int(max_depth)
         self.root_quad = Quad(float(root_quad.xmid), float(root_quad.ymid), float(root_quad.half))
@@ -313,7 +306,7 @@ class FlatQuadtree:
         f64, i64 = torch.float64, torch.int64
         self.perm = torch.empty(n, dtype=i64, device=dev)
         self._sorted_pos = torch.empty((2, n), dtype=f64, device=dev)
-        sizes = np.zeros(3, dtype=np.int64)
+        sizes = np.zeros(4, dtype=np.int64)
         while True:
             self.node_center = torch.empty((capacity, 2), dtype=f64, device=dev)
             self.node_half = torch.empty(capacity, dtype=f64, device=dev)
@@ -324,7 +317,7 @@ class FlatQuadtree:
             levels = np.zeros(capacity + 1, dtype=np.int64)
             ws = _lib.workspace(_lib.query("td3_quadtree_build_workspace_size", n, capacity), dev)
             q = self.root_quad
-            rc = _lib.call(
+            rc = _lib.call_code(
                 "td3_quadtree_build", self.pos.data_ptr(), n, q.xmid, q.ymid, q.half,
                 self.leaf_capacity, self.max_depth, capacity, self.node_center.data_ptr(),
                 self.node_half.data_ptr(), self.node_start.data_ptr(), self.node_end.data_ptr(),
@@ -335,6 +328,13 @@ class FlatQuadtree:
             self.build_restarts = getattr(self, "build_restarts", 0)
             if rc == _lib.OK:
                 break
+            # the build checks the positions as ft:788-794 (one read for the whole build)
+            if rc == _lib.EINVAL and sizes[3] == 1:
+                raise ValueError("Particle position must be finite")
+            if rc == _lib.EINVAL and sizes[3] == 2:
+                raise ValueError("Particle lies outside tree bounds")
+            if rc != _lib.ENEEDMORE:
+                raise _lib.LibraryError(f"td3_quadtree_build failed with code {rc}")
             self.build_restarts += 1
             capacity = max(2 * capacity, int(sizes[0]))
         self.levels = levels[: sizes[1] + 1].copy()
@@ -577,11 +577,17 @@ class FlatQuadtree:
                              self.device)
 
     # ------------------------------------------------------------------ FMM
-    def fmm(self, *, theta: float = 0.5, softening: float = 0.0, potential: bool = True):
+    def fmm(self, *, theta: float = 0.5, softening: float = 0.0, potential: bool = True,
+            _status: torch.Tensor | None = None):
         """Potential (N,) and field (2, N) at every source by the FMM, without ``k_e``
         (ft:1460-1634): complex expansions for ``kernel="log"``, Cartesian expansions of
         the softened kernel for ``kernel="coulomb"``; each particle's own charge
-        excluded; ``potential=False`` returns zeros for the potential."""
+        excluded; ``potential=False`` returns zeros for the potential.
+
+        ``_status`` (internal): a zeroed device status word that receives the
+        coincident-charge report instead of a check here, for callers that read it later
+        (the autograd function reads it after the backward) so the host does not wait
+        for the GPU at the end of the call."""
         theta = _finite("theta", theta, minimum=0)
         if not 0 < theta < 1:
             raise ValueError("FMM theta must lie in (0, 1)")
@@ -592,16 +598,17 @@ class FlatQuadtree:
         if not n:
             return out((phi, field), self._numpy)
         if self.kernel != "log":
-            self._coulomb_fmm(theta, softening, phi, field)
+            self._coulomb_fmm(theta, softening, phi, field, _status)
             return out((phi, field), self._numpy)
         lists = self._lists(theta)
         local_re, local_im = self._log_locals(lists)
         self._fwd_locals = ((theta, softening), local_re, local_im)
-        status = status_word(dev)
+        status = status_word(dev) if _status is None else _status
         self._evaluate_near(lists, _lib.KERNEL_LOG, local_re, local_im, softening, potential,
                             phi, field, status)
-        _check(status)
-        self._check_tensor_cores()
+        if _status is None:
+            _check(status)
+            self._check_tensor_cores()
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
         return out((phi, field), self._numpy)
 
@@ -689,7 +696,8 @@ class FlatQuadtree:
                       dst.node_center.data_ptr(), dst.node_half.data_ptr(),
                       self.node_center.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(),
                       self.order, coeff.ctypes.data, self._unit, tensor, local_re.data_ptr(),
-                      local_im.data_ptr(), self._tensor_status().data_ptr(), stream)
+                      local_im.data_ptr(), self._tensor_status().data_ptr() if tensor else 0,
+                      stream)
             return
         _lib.call("td3_fmm_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                   dst.node_center.data_ptr(), self.node_center.data_ptr(), mre.data_ptr(),
@@ -924,15 +932,17 @@ class FlatQuadtree:
                   local.data_ptr(), stream)
         return local
 
-    def _coulomb_fmm(self, theta, softening, phi, field):
+    def _coulomb_fmm(self, theta, softening, phi, field, status=None):
         """ft:1360-1428: the Coulomb FMM with Cartesian expansions (the potential is
-        always computed, as in the reference)."""
+        always computed, as in the reference); ``status`` as fmm's ``_status``."""
         lists = self._lists(theta)
         local = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"],
                                   lists["m2l"].shape[0], self, softening)
         self._fwd_locals = ((theta, softening), local, local)
-        status = status_word(self.device)
+        deferred = status is not None
+        status = status_word(self.device) if status is None else status
         self._evaluate_near(lists, _lib.KERNEL_COULOMB, local, local, softening, True, phi,
                             field, status)
-        _check(status)
+        if not deferred:
+            _check(status)
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
