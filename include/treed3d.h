@@ -187,7 +187,7 @@ int td3_target_order(const double* targets, int64_t m, int64_t* order, void* wor
  * above 190 the call returns TD3_EDEPTH.  with_potential = 0 writes phi = 0 and skips
  * the log kernel's logarithms.  mixed = 1 keeps the FP64 opening decisions and evaluates
  * leaf pairs and far-field terms in FP32 with compensated sums; the log kernel then
- * reads moment_hat (nodes, order_p + 1, 2) FP32, hat_k = a_k / h^k (td3_scale_moments)
+ * reads moment_hat (td3_scale_moments' layout), hat_k = a_k / h^k
  * instead of moment_re / moment_im.  mixed = 0 ignores moment_hat (may be NULL).
  * Replaces evaluate_quadtree (src/tree_d_3d/kernels/evaluate_quadtree/
  * evaluate_quadtree_cuda.cu:9-107), evaluate_log_quadtree (kernels/evaluate_log_quadtree/
@@ -270,16 +270,17 @@ int td3_fmm_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst
                 const double* moment_im, int order, const double* coeff, double* local_re,
                 double* local_im, void* stream);
 
-/* Mixed-precision M2L of the log kernel: moments scaled by the cell size, hat (nodes,
- * order + 1) complex float pairs with hat_k = a_k / h^k (td3_scale_moments), translated
+/* Mixed-precision M2L of the log kernel: moments scaled by the cell size, hat_k =
+ * a_k / h^k (td3_scale_moments: rows of order + 1 complex float pairs rounded up to an
+ * even count, so each row is 16-byte aligned, the pad pair zero), translated
  * in FP32 with ws = h_src / t and wd = h_dst / t (|ws|, |wd| < 1 for separated cells):
  * s_l = sum_k coeff[k, l] hat_k ws^k, bhat_0 = a_0 ln|t| - s_0, bhat_l = -(-1)^l s_l wd^l,
  * and local_re / local_im (FP64) += bhat_l / h_dst^l.  ln|t| is formed as ln|t / unit|
  * in FP32 plus ln(unit) sum a_0 in FP64 (unit > 0: a length of the problem, e.g. the
  * root half-width).  coeff is a HOST (order + 1)^2 array (the reference's M2L matrix);
  * order <= 20.  entry_row: the row of every entry of partners (td3_pair_csr); a warp
- * takes 32 consecutive entries at a time across row boundaries.  tensor_cores != 0 (orders <= 15) takes the matrix products s_l on the
- * tensor cores (tcgen05.mma, 3xTF32 with FP32 accumulation) and needs status, a device
+ * takes 32 consecutive entries at a time across row boundaries.  tensor_cores != 0
+ * (orders <= 15) takes the matrix products s_l on the tensor cores (tcgen05.mma, 3xTF32 with FP32 accumulation) and needs status, a device
  * int64 the caller zeroed: it becomes nonzero if a wait for the tensor cores ran out (the
  * locals are then incomplete); otherwise FP32 CUDA-core arithmetic, status unused.  The
  * rows of one destination are summed in row order either way (deterministic).  The
@@ -294,12 +295,20 @@ int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
                       double unit, int tensor_cores, double* local_re, double* local_im,
                       int64_t* status, void* stream);
 
+/* The parent of every node (node_parent (count), int32; -1 for the root), from
+ * node_child.  No reference counterpart (its walks keep explicit stacks). */
+int td3_node_parents(int64_t count, const int64_t* node_child, int32_t* node_parent,
+                     void* stream);
+
 /* L2L from the root down, level by level (levels HOST, n_levels + 1): every local
- * expansion shifted into its children, b_m(child) += sum_{l>=m} C(l, m) b_l s^(l-m).
+ * expansion shifted into its children, b_m(child) += sum_{l>=m} C(l, m) b_l s^(l-m),
+ * over the children of each level (node_parent from td3_node_parents); empty cells
+ * (node_start == node_end) are left as they are, nothing reads their locals.
  * Replaces fmm_downward (src/tree_d_3d/kernels/fmm_downward/fmm_downward_pyccel.py:15-64,
  * fmm_downward_cuda.cu:10-51) and its per-level loop (src/tree_d_3d/flat_tree.py:1540-1552). */
 int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node_center,
-                     const int64_t* node_child, int order, const double* binomial,
+                     const int32_t* node_parent, const int64_t* node_start,
+                     const int64_t* node_end, int order, const double* binomial,
                      int binomial_size, double* local_re, double* local_im, void* stream);
 
 /* ------------------------------------------------------------------ Coulomb FMM */

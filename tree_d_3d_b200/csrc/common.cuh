@@ -88,6 +88,15 @@ struct KahanF {
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
+// Pairs per node row of the size-scaled FP32 moments (td3_scale_moments): order + 1
+// rounded up to even, so every row starts on a 16-byte boundary.
+__host__ __device__ __forceinline__ int td3_hat_width(int order) { return (order + 2) & ~1; }
+
+// Pairs 2c and 2c + 1 of a scaled-moment row, zero beyond the order (w = order + 1).
+__device__ __forceinline__ float4 td3_hat_pair(const float2* row, int c, int w) {
+    return 2 * c < w ? reinterpret_cast<const float4*>(row)[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 // ln(x) for x > 0 of any FP64 magnitude in FP32 arithmetic: x = f 2^e with f in [0.5, 1)
 // (frexp, exact), ln x = ln f + e ln 2.
 __device__ __forceinline__ float log_split(double x) {

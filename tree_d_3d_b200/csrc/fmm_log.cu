@@ -118,18 +118,20 @@ k_m2l_log(const i64* __restrict__ row_start, const i64* __restrict__ partners, i
     }
 }
 
-// L2L of one level: thread per (node, child, m).
-__global__ void k_l2l_log(i64 lo, i64 hi, int order, const double* __restrict__ center,
-                          const i64* __restrict__ child, const double* __restrict__ binomial,
-                          int bsize, double* __restrict__ local_re, double* __restrict__ local_im) {
+// L2L into one level, b_m(child) += sum_{l>=m} C(l, m) b_l(parent) s^(l-m), s = c_child -
+// c_parent: thread per (child, m) over the level's non-empty nodes (an empty cell needs
+// no local expansion), the parent from node_parent.
+__global__ void k_l2l_log_level(i64 lo, i64 hi, int order, const double* __restrict__ center,
+                                const int* __restrict__ parent, const i64* __restrict__ start,
+                                const i64* __restrict__ end, const double* __restrict__ binomial,
+                                int bsize, double* __restrict__ local_re,
+                                double* __restrict__ local_im) {
     int w = order + 1;
     i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    i64 node = lo + t / (4 * w);
-    if (node >= hi) return;
-    i64 first = child[node];
-    if (first < 0) return;
-    int c = (int)((t / w) % 4), m = (int)(t % w);
-    i64 ch = first + c;
+    i64 ch = lo + t / w;
+    if (ch >= hi || end[ch] == start[ch]) return;
+    int m = (int)(t % w);
+    i64 node = parent[ch];
     double s_re = center[2 * ch] - center[2 * node];
     double s_im = center[2 * ch + 1] - center[2 * node + 1];
     double acc_re = 0.0, acc_im = 0.0, p_re = 1.0, p_im = 0.0;
@@ -147,19 +149,34 @@ __global__ void k_l2l_log(i64 lo, i64 hi, int order, const double* __restrict__ 
     local_im[ch * w + m] += acc_im;
 }
 
+__global__ void k_node_parents(i64 count, const i64* __restrict__ node_child,
+                               int* __restrict__ parent) {
+    i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= count) return;
+    if (p == 0) parent[0] = -1;
+    i64 c = node_child[p];
+    if (c >= 0)
+        for (int k = 0; k < 4; ++k) parent[c + k] = (int)p;
+}
+
 // ------------------------------------------------------------------ mixed precision
-// Moments scaled by the cell size, hat_k = a_k / h^k (|hat_k| <= sum |q|), in FP32.
+// Moments scaled by the cell size, hat_k = a_k / h^k (|hat_k| <= sum |q|), in FP32, in
+// rows of td3_hat_width(order) pairs (16-byte aligned rows; the pad pair is zero).
 __global__ void k_scale_moments(i64 count, int order, const double* __restrict__ mre,
                                 const double* __restrict__ mim, const double* __restrict__ half,
                                 float2* __restrict__ hat) {
-    int w = order + 1;
+    int w = order + 1, hw = td3_hat_width(order);
     i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= count * w) return;
-    i64 node = t / w;
-    int k = (int)(t % w);
+    if (t >= count * hw) return;
+    i64 node = t / hw;
+    int k = (int)(t % hw);
+    if (k >= w) {
+        hat[t] = make_float2(0.0f, 0.0f);
+        return;
+    }
     double inv = 1.0 / half[node], s = 1.0;
     for (int j = 0; j < k; ++j) s *= inv;
-    hat[t] = make_float2((float)(mre[t] * s), (float)(mim[t] * s));
+    hat[t] = make_float2((float)(mre[node * w + k] * s), (float)(mim[node * w + k] * s));
 }
 
 template <int P>
@@ -207,12 +224,21 @@ k_m2l_mixed(const i64* __restrict__ row_start, const int* __restrict__ entry_row
             float wsr = (float)(hs * tr * inv), wsi = (float)(-hs * ti * inv);
             float wdr = (float)(hd * tr * inv), wdi = (float)(-hd * ti * inv);
             float lnt = 0.5f * log_split(t2 * inv_unit2);
-            const float2* a = hat + src * w;
+            const float2* a = hat + src * td3_hat_width(order);
+            float hr[W + 1], hi[W + 1];
+#pragma unroll
+            for (int c = 0; c < (W + 1) / 2; ++c) {
+                float4 m = td3_hat_pair(a, c, w);
+                hr[2 * c] = m.x;
+                hi[2 * c] = m.y;
+                hr[2 * c + 1] = m.z;
+                hi[2 * c + 1] = m.w;
+            }
             float ar[W], ai[W];
             float pr = 1.0f, pi = 0.0f;
 #pragma unroll
             for (int k = 0; k < W; ++k) {
-                float2 m = k < w ? a[k] : make_float2(0.0f, 0.0f);
+                float2 m = make_float2(hr[k], hi[k]);
                 ar[k] = m.x * pr - m.y * pi;
                 ai[k] = m.x * pi + m.y * pr;
                 float nr = pr * wsr - pi * wsi;
@@ -307,7 +333,7 @@ extern "C" int td3_scale_moments(int64_t count, int order, const double* moment_
                                  void* stream) {
     if (count < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
     if (count == 0) return TD3_OK;
-    i64 threads = count * (order + 1);
+    i64 threads = count * td3_hat_width(order);
     k_scale_moments<<<td3_blocks(threads, 256), 256, 0, td3_stream(stream)>>>(
         count, order, moment_re, moment_im, node_half, reinterpret_cast<float2*>(hat));
     TD3_CHECK_LAUNCH();
@@ -346,21 +372,31 @@ extern "C" int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_
                                 src_half, h, order, coeff, unit, local_re, local_im, s);
 }
 
+extern "C" int td3_node_parents(int64_t count, const int64_t* node_child, int32_t* node_parent,
+                                void* stream) {
+    if (count < 1 || count > 0x7fffffffLL) return TD3_EINVAL;
+    k_node_parents<<<td3_blocks(count, 256), 256, 0, td3_stream(stream)>>>(count, node_child,
+                                                                          node_parent);
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
 extern "C" int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node_center,
-                                const int64_t* node_child, int order, const double* binomial,
+                                const int32_t* node_parent, const int64_t* node_start,
+                                const int64_t* node_end, int order, const double* binomial,
                                 int binomial_size, double* local_re, double* local_im,
                                 void* stream) {
     if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER || binomial_size < order + 1)
         return TD3_EINVAL;
     cudaStream_t s = td3_stream(stream);
     int w = order + 1;
-    for (i64 level = 0; level + 1 < n_levels; ++level) {
+    for (i64 level = 1; level < n_levels; ++level) {
         i64 lo = levels[level], hi = levels[level + 1];
         if (hi <= lo) continue;
-        i64 threads = (hi - lo) * 4 * w;
-        k_l2l_log<<<td3_blocks(threads, 256), 256, 0, s>>>(lo, hi, order, node_center, node_child,
-                                                            binomial, binomial_size, local_re,
-                                                            local_im);
+        i64 threads = (hi - lo) * w;
+        k_l2l_log_level<<<td3_blocks(threads, 256), 256, 0, s>>>(
+            lo, hi, order, node_center, node_parent, node_start, node_end, binomial, binomial_size,
+            local_re, local_im);
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;

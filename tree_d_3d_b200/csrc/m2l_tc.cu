@@ -110,11 +110,20 @@ k_m2l_tc(const i64* __restrict__ row_start, const int* __restrict__ entry_row,
             wdr = (float)(hd * tr * inv);
             wdi = (float)(-hd * ti * inv);
             lnt = 0.5f * log_split(t2 * inv_unit2);
-            const float2* a = hat + src * w;
+            const float2* a = hat + src * td3_hat_width(order);
+            float hr[W + 1], hi[W + 1];
+#pragma unroll
+            for (int c = 0; c < (W + 1) / 2; ++c) {
+                float4 m = td3_hat_pair(a, c, w);
+                hr[2 * c] = m.x;
+                hi[2 * c] = m.y;
+                hr[2 * c + 1] = m.z;
+                hi[2 * c + 1] = m.w;
+            }
             float pr = 1.0f, pi = 0.0f;
 #pragma unroll
             for (int k = 0; k < W; ++k) {
-                float2 m = k < w ? a[k] : make_float2(0.0f, 0.0f);
+                float2 m = make_float2(hr[k], hi[k]);
                 ar[k] = m.x * pr - m.y * pi;
                 ai[k] = m.x * pi + m.y * pr;
                 float nr = pr * wsr - pi * wsi;

@@ -158,7 +158,7 @@ int exclusive_scan(const T* in, T* out, i64 n, T* total, void* ws, size_t ws_byt
 // runs of equal digits (coalesced stores).
 constexpr int SORT_THREADS = 256;
 constexpr int SORT_WARPS = SORT_THREADS / 32;
-constexpr int SORT_ITEMS = 16;
+constexpr int SORT_ITEMS = 8;
 constexpr int WARP_ITEMS = 32 * SORT_ITEMS;
 constexpr int SORT_TILE = SORT_THREADS * SORT_ITEMS;
 constexpr int RADIX_BITS = 8;

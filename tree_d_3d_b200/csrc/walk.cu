@@ -340,7 +340,7 @@ k_walk_log(const double* __restrict__ targets, i64 m, const i64* __restrict__ ex
                     float wr = (float)(wr64 * g.z), wi = (float)(wi64 * g.z);
                     wr64 *= unit;  // w in units of 1 / L
                     wi64 *= unit;
-                    const float2* a = hat + (i64)node * w;
+                    const float2* a = hat + (i64)node * td3_hat_width(order_p);
                     float2 top = a[order_p];
                     float gr = top.x, gi = top.y;
                     float sr = top.x * inv_nf[order_p], si = top.y * inv_nf[order_p];

@@ -269,8 +269,8 @@ class FlatQuadtree:
             return
         count = self._build()
         self.node_count = int(count)
-        for name in _NODE_ARRAYS:
-            setattr(self, name, getattr(self, name)[:count].clone())
+        for name in _NODE_ARRAYS:  # views of the first `count` rows of the build's buffers
+            setattr(self, name, getattr(self, name)[:count])
         self._moments()
 
     # ------------------------------------------------------------------ build
@@ -622,13 +622,26 @@ class FlatQuadtree:
         stream = _lib.stream(dev)
         if lists["m2l"].shape[0]:
             self._m2l_log(lists, self, (mre, mim), local_re, local_im)
-        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
-        binom = self._binomial()
-        _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
-                  self.node_center.data_ptr(), self.node_child.data_ptr(), self.order,
-                  binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
-                  stream)
+        self._downward(local_re, local_im, self.order, self._binomial())
         return local_re, local_im
+
+    def _parents(self) -> torch.Tensor:
+        """The parent of every node (int32, -1 for the root), kept with the tree."""
+        if getattr(self, "_node_parent", None) is None:
+            self._node_parent = torch.empty(self.node_count, dtype=torch.int32, device=self.device)
+            _lib.call("td3_node_parents", self.node_count, self.node_child.data_ptr(),
+                      self._node_parent.data_ptr(), _lib.stream(self.device))
+        return self._node_parent
+
+    def _downward(self, local_re, local_im, order, binom) -> None:
+        """L2L of complex locals of ``order`` from the root down this tree
+        (td3_fmm_downward; ``binom`` the binomial table)."""
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
+                  self.node_center.data_ptr(), self._parents().data_ptr(),
+                  self.node_start.data_ptr(), self.node_end.data_ptr(), order,
+                  binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
+                  _lib.stream(self.device))
 
     def _evaluate_near(self, lists, kernel, local_a, local_b, softening, potential, phi, field,
                        status):
@@ -655,10 +668,11 @@ class FlatQuadtree:
         return self.root_quad.half
 
     def _scaled_moments(self, moments):
-        """FP32 moments scaled by the cell size, hat_k = a_k / h^k (nodes, order + 1, 2)."""
+        """FP32 moments scaled by the cell size, hat_k = a_k / h^k (nodes, order + 1
+        rounded up to even, 2; the pad pair is zero)."""
         mre, mim = moments
-        hat = torch.empty((self.node_count, self.order + 1, 2), dtype=torch.float32,
-                          device=self.device)
+        width = (self.order + 2) & ~1
+        hat = torch.empty((self.node_count, width, 2), dtype=torch.float32, device=self.device)
         _lib.call("td3_scale_moments", self.node_count, self.order, mre.data_ptr(),
                   mim.data_ptr(), self.node_half.data_ptr(), hat.data_ptr(),
                   _lib.stream(self.device))
@@ -876,12 +890,7 @@ class FlatQuadtree:
             local_b = torch.zeros_like(local_a)
             if n_m2l:
                 self._m2l_log(lists, tree, (self.moment_re, self.moment_im), local_a, local_b)
-            levels = np.ascontiguousarray(tree.levels, dtype=np.int64)
-            binom = self._binomial()
-            _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
-                      tree.node_center.data_ptr(), tree.node_child.data_ptr(), self.order,
-                      binom.data_ptr(), binom.shape[0], local_a.data_ptr(), local_b.data_ptr(),
-                      stream)
+            tree._downward(local_a, local_b, self.order, self._binomial())
             kernel, with_pot = _lib.KERNEL_LOG, potential
         else:
             local_a = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"], n_m2l, tree,
