@@ -61,6 +61,9 @@ def _args():
     p.add_argument("--impl", choices=("ours", "reference"), default="ours")
     p.add_argument("--n", type=int, default=N_PARTICLES)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--suite", action="store_true",
+                   help="every workload configuration (one JSON line per case) instead of "
+                        "the headline line")
     p.add_argument("--trace-only", action="store_true",
                    help="timed mixed steps only (no e2e, FP64 arm, counts or errors): for ncu")
     return p.parse_args()
@@ -399,7 +402,10 @@ def run_ours(args):
         "frac": achieved / FP32_PEAK,
         "peak_source": ("nominal FP32 FMA rate at the max SM clock (148 SM x 128 lanes x 2 x "
                         "1965 MHz); MEASURED_PEAKS.json has no FP32 CUDA-core figure"),
-        "traffic": None,
+        # dram read + write of one ncu capture of this kernel at 300k particles (86.4 MB
+        # for 3.745M translations), scaled by the translations of this launch
+        "traffic": 86.4e6 * (2 * n_m2l) / 3.745e6,
+        "traffic_unit": "bytes per launch (scaled from a 300k-particle ncu capture)",
         "ms_per_launch": m2l_ms,
         "flop_per_launch": flops,
     }
@@ -443,10 +449,183 @@ def run_ours(args):
     return 0
 
 
+# ----------------------------------------------------------------------------- suite
+def _event_ms(fn, torch, reps=5, warm=2):
+    """Median CUDA-event time of fn() in ms (inputs resident; no L2 flush: repeated work
+    on the same data, as an application that steps the same particles)."""
+    for _ in range(warm):
+        fn()
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    return float(np.median(times))
+
+
+def _sample_error(torch, pos, q, field, kernel, eps, n_sample=4096, targets=None, tfield=None):
+    """Normwise relative field error against the FP64 direct sum on sampled points."""
+    from tree_d_3d_b200 import direct_field
+
+    if targets is None:
+        idx = torch.tensor(np.random.default_rng(0).choice(pos.shape[1], n_sample, replace=False),
+                           device=pos.device)
+        _, ref = direct_field(pos[:, idx], pos, q, softening=eps, exclude=idx, kernel=kernel)
+        got = field[:, idx]
+    else:
+        idx = torch.tensor(np.random.default_rng(0).choice(targets.shape[1], n_sample,
+                                                           replace=False), device=pos.device)
+        _, ref = direct_field(targets[:, idx], pos, q, softening=eps, kernel=kernel)
+        got = tfield[:, idx]
+    return float((got - ref).abs().max() / ref.abs().max())
+
+
+def run_suite(args):
+    """Every workload configuration of the solver on one GPU, one JSON line per case:
+    config 1 (5000 uniform charges: walk and direct sum), config 2 (200k Gaussian line
+    charges: FMM p = 12), config 3 (1M 8-Gaussian mixture: walk at theta 0.3 / 0.5 / 0.7,
+    FMM at p = 8 / 12 / 16 for both kernels, fmm_at at 1M uniform targets), config 4
+    (100k uniform, N(0, 1) charges: energy and its backward), config 5 (1M protons: 100
+    simulation steps, gradient of the final kinetic energy through 20 checkpointed
+    steps).  Tree builds are inside the timed FMM cases (a fresh tree per call)."""
+    import torch
+
+    from tree_d_3d_b200 import FlatQuadtree, Quad, direct_field, synthetic
+    from tree_d_3d_b200.autograd import fmm_energy
+    from tree_d_3d_b200.simulation import ElectrostaticSimulation, rollout_kinetic_energy
+
+    dev = torch.device("cuda", 0)
+    root = Quad(0.0, 0.0, 1.0)
+
+    def emit(config, case, ms, n, unit="particles/s", **extra):
+        print(json.dumps({"suite": config, "case": case, "ms": round(ms, 4),
+                          "value": n / (ms / 1e3), "unit": unit, **extra}), flush=True)
+
+    # config 1
+    rng = np.random.default_rng(SEED)
+    p1 = torch.tensor(rng.uniform(-1, 1, (2, 5000)), device=dev)
+    q1 = torch.tensor(rng.choice([-1.0, 1.0], 5000), device=dev)
+    idx1 = torch.arange(5000, device=dev)
+    for prec in ("fp64", "mixed"):
+        tree = FlatQuadtree(p1, q1, root, precision=prec)
+        ms = _event_ms(lambda: tree.evaluate(p1, exclude=idx1, theta=0.5, softening=1e-3), torch)
+        _, f = tree.evaluate(p1, exclude=idx1, theta=0.5, softening=1e-3)
+        _, ref = direct_field(p1, p1, q1, softening=1e-3, exclude=idx1)
+        err = float((f - ref).abs().max() / ref.abs().max())
+        emit("1", f"walk coulomb theta=0.5 {prec}", ms, 5000, "targets/s", rel_err_vs_direct=err)
+    ms = _event_ms(lambda: direct_field(p1, p1, q1, softening=1e-3, exclude=idx1), torch)
+    emit("1", "direct coulomb", ms, 5000 * 5000, "pairs/s")
+
+    # config 2
+    p2, q2 = (torch.tensor(a, device=dev) for a in synthetic.gaussian(200_000, 0.3, seed=2))
+    for prec in ("fp64", "mixed"):
+        def run2():
+            return FlatQuadtree(p2, q2, root, kernel="log", order=12, precision=prec).fmm(theta=0.5)
+        ms = _event_ms(run2, torch)
+        err = _sample_error(torch, p2, q2, run2()[1], "log", 0.0)
+        emit("2", f"fmm log p=12 {prec}", ms, 200_000, rel_err_vs_direct=err)
+
+    # config 3
+    p3, q3 = (torch.tensor(a, device=dev) for a in synthetic.mixture8(1_000_000, seed=SEED))
+    idx3 = torch.arange(1_000_000, device=dev)
+    for prec in ("fp64", "mixed"):
+        tree = FlatQuadtree(p3, q3, root, kernel="coulomb", precision=prec)
+        for theta in (0.3, 0.5, 0.7):
+            ms = _event_ms(lambda: tree.evaluate(p3, exclude=idx3, theta=theta, softening=1e-3),
+                           torch, reps=3)
+            f = tree.evaluate(p3, exclude=idx3, theta=theta, softening=1e-3)[1]
+            err = _sample_error(torch, p3, q3, f, "coulomb", 1e-3)
+            emit("3", f"walk coulomb theta={theta} {prec}", ms, 1_000_000, "targets/s",
+                 rel_err_vs_direct=err)
+    for kernel, eps in (("coulomb", 1e-3), ("log", 0.0)):
+        for order in (8, 12, 16):
+            for prec in ("fp64", "mixed"):
+                def run3():
+                    return FlatQuadtree(p3, q3, root, kernel=kernel, order=order,
+                                        precision=prec).fmm(theta=0.5, softening=eps)
+                ms = _event_ms(run3, torch, reps=3)
+                err = _sample_error(torch, p3, q3, run3()[1], kernel, eps)
+                emit("3", f"fmm {kernel} p={order} {prec}", ms, 1_000_000,
+                     rel_err_vs_direct=err)
+    targets = torch.tensor(np.random.default_rng(SEED + 2).uniform(-1, 1, (2, 1_000_000)),
+                           device=dev)
+    for kernel, eps in (("coulomb", 1e-3), ("log", 0.0)):
+        for prec in ("fp64", "mixed"):
+            tree = FlatQuadtree(p3, q3, root, kernel=kernel, order=12, precision=prec)
+            tree.fmm_at(targets, theta=0.5, softening=eps)  # target tree and lists, kept
+            ms = _event_ms(lambda: tree.fmm_at(targets, theta=0.5, softening=eps), torch, reps=3)
+            err = _sample_error(torch, p3, q3, None, kernel, eps, targets=targets,
+                                tfield=tree.fmm_at(targets, theta=0.5, softening=eps)[1])
+            emit("3", f"fmm_at {kernel} p=12 1M targets {prec} (plan kept)", ms, 1_000_000,
+                 "targets/s", rel_err_vs_direct=err)
+
+    # config 4
+    rng = np.random.default_rng(SEED + 4)
+    p4 = torch.tensor(rng.uniform(-1, 1, (2, 100_000)), device=dev)
+    q4 = torch.tensor(rng.normal(size=100_000), device=dev)
+    for kernel, eps in (("log", 0.0), ("coulomb", 1e-3)):
+        for prec in ("fp64", "mixed"):
+            def run4():
+                P = p4.detach().requires_grad_(True)
+                Q = q4.detach().requires_grad_(True)
+                fmm_energy(P, Q, root, kernel=kernel, order=12, softening=eps,
+                           precision=prec).backward()
+                return P.grad, Q.grad
+            ms = _event_ms(run4, torch)
+            emit("4", f"energy + backward {kernel} p=12 {prec}", ms, 100_000)
+
+    # config 5
+    p5, q5 = synthetic.protons(1_000_000, seed=SEED)
+    walls = {"x_min": -1.0, "x_max": 1.0, "y_min": -1.0, "y_max": 1.0}
+    def new_sim():
+        return ElectrostaticSimulation(positions=p5, charges=q5, bounds=root, k_e=1.0, B_z=1.0,
+                                       dt=1e-4, absorbing_walls=walls)
+    # one step of the full 1M cloud (fields at the start and at the end of the step)
+    ms = _event_ms(lambda: new_sim().step(), torch, reps=3, warm=1)
+    emit("5", f"first step of 1M protons (method {new_sim()._resolve_method()})", ms,
+         1_000_000, "particle-steps/s")
+    # 100 steps: the like charges fly apart and the walls absorb most of them, so the
+    # later steps hold few particles (the method follows the particle count)
+    sim = new_sim()
+    sim.step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(100):
+        sim.step()
+    b.record()
+    b.synchronize()
+    ms = a.elapsed_time(b)
+    emit("5", "100 simulation steps after the first", ms, 100, "steps/s",
+         particles_left=int(sim.num_particles), method_at_end=sim._resolve_method(),
+         wall_s=time.perf_counter() - t0)
+    P = torch.tensor(p5, device=dev)
+    Q = torch.tensor(q5, device=dev)
+
+    def run5():
+        Qg = Q.detach().requires_grad_(True)
+        ke = rollout_kinetic_energy(P, torch.zeros_like(P), Qg, torch.ones_like(Q), 20,
+                                    bounds=root, dt=1e-4, B_z=1.0, k_e=1.0,
+                                    absorbing_walls=walls)
+        ke.backward()
+        return Qg.grad
+    ms = _event_ms(run5, torch, reps=2, warm=1)
+    emit("5", "gradient of the final kinetic energy through 20 checkpointed steps", ms,
+         20 * 1_000_000, "particle-steps/s")
+    return 0
+
+
 def main():
     args = _args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.suite:
+        return run_suite(args)
     return run_ours(args)
 
 
