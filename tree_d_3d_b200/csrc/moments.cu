@@ -147,17 +147,19 @@ __global__ void k_log_moments_node(i64 lo, i64 hi, int order, const double* __re
                                    const i64* __restrict__ node_child,
                                    const double* __restrict__ binomial, int bsize,
                                    double* node_qabs, double* moment_re, double* moment_im,
-                                   const double* __restrict__ sdip) {
+                                   const double* __restrict__ sdip, int part) {
     constexpr int W = P + 1;
     i64 node = lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= hi) return;
+    i64 first = node_child[node];
+    // part 1: leaves only (all levels in one launch), part 2: parents only (one level)
+    if ((part == 1 && first >= 0) || (part == 2 && first < 0)) return;
     int w = order + 1;
     double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
     double ar[W], ai[W];
 #pragma unroll
     for (int n = 0; n < W; ++n) ar[n] = ai[n] = 0.0;
     double qabs = 0.0;
-    i64 first = node_child[node];
     if (first < 0) {
         for (i64 k = node_start[node]; k < node_end[node]; ++k) {
             double q = scharge[k];
@@ -229,33 +231,44 @@ __global__ void k_log_moments_node(i64 lo, i64 hi, int order, const double* __re
     node_qabs[node] = qabs;
 }
 
-// Moments of every level, deepest first, with the per-node kernel for orders up to 16.
+// Moments of every node.  Orders up to 16: every leaf in one launch (leaves depend on
+// nothing), then the parents level by level, deepest first; higher orders: thread per
+// (node, coefficient), level by level.
 int launch_log_moments(const int64_t* levels, int64_t n_levels, int order, const double* spos,
                        const double* scharge, int64_t n, const double* center, const i64* start,
                        const i64* end, const i64* child, const double* binomial, int bsize,
                        double* qabs, double* mre, double* mim, const double* sdip,
                        cudaStream_t s) {
-    for (i64 level = n_levels - 1; level >= 0; --level) {
-        i64 lo = levels[level], hi = levels[level + 1];
-        if (hi <= lo) continue;
+    auto node_kernel = [&](i64 lo, i64 hi, int part) {
         unsigned nb = td3_blocks(hi - lo, MOM_THREADS);
 #define TD3_NODE_MOMENTS(P)                                                                  \
     k_log_moments_node<P><<<nb, MOM_THREADS, 0, s>>>(lo, hi, order, spos, scharge, n, center, \
                                                      start, end, child, binomial, bsize, qabs,\
-                                                     mre, mim, sdip)
+                                                     mre, mim, sdip, part)
         if (order <= 4)
             TD3_NODE_MOMENTS(4);
         else if (order <= 8)
             TD3_NODE_MOMENTS(8);
         else if (order <= 12)
             TD3_NODE_MOMENTS(12);
-        else if (order <= 16)
-            TD3_NODE_MOMENTS(16);
         else
-            k_log_moments<<<td3_blocks((hi - lo) * (order + 1), MOM_THREADS), MOM_THREADS, 0, s>>>(
-                lo, hi, order, spos, scharge, n, center, start, end, child, binomial, bsize, qabs,
-                mre, mim, sdip);
+            TD3_NODE_MOMENTS(16);
 #undef TD3_NODE_MOMENTS
+    };
+    if (order <= 16) {
+        node_kernel(0, levels[n_levels], 1);
+        for (i64 level = n_levels - 2; level >= 0; --level) {
+            i64 lo = levels[level], hi = levels[level + 1];
+            if (hi > lo) node_kernel(lo, hi, 2);
+        }
+    } else {
+        for (i64 level = n_levels - 1; level >= 0; --level) {
+            i64 lo = levels[level], hi = levels[level + 1];
+            if (hi <= lo) continue;
+            k_log_moments<<<td3_blocks((hi - lo) * (order + 1), MOM_THREADS), MOM_THREADS, 0,
+                            s>>>(lo, hi, order, spos, scharge, n, center, start, end, child,
+                                 binomial, bsize, qabs, mre, mim, sdip);
+        }
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;

@@ -323,19 +323,16 @@ int run_generations(const TreeView& t, const TreeView& s, double theta, Pair* m2
 
 // ------------------------------------------------------------------ pair CSR
 __global__ void k_csr_keys(const Pair* __restrict__ pairs, i64 count, int mutual, unsigned invalid,
-                           unsigned* __restrict__ keys, unsigned* __restrict__ vals,
-                           i64* __restrict__ row_count) {
+                           unsigned* __restrict__ keys, unsigned* __restrict__ vals) {
     i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= count) return;
     Pair pr = pairs[p];
     if (mutual) {
         keys[2 * p] = (unsigned)pr.a;
         vals[2 * p] = (unsigned)pr.b;
-        atomicAdd(reinterpret_cast<unsigned long long*>(row_count + pr.a), 1ULL);
         if (pr.a != pr.b) {
             keys[2 * p + 1] = (unsigned)pr.b;
             vals[2 * p + 1] = (unsigned)pr.a;
-            atomicAdd(reinterpret_cast<unsigned long long*>(row_count + pr.b), 1ULL);
         } else {
             keys[2 * p + 1] = invalid;
             vals[2 * p + 1] = 0;
@@ -343,8 +340,19 @@ __global__ void k_csr_keys(const Pair* __restrict__ pairs, i64 count, int mutual
     } else {
         keys[p] = (unsigned)pr.a;
         vals[p] = (unsigned)pr.b;
-        atomicAdd(reinterpret_cast<unsigned long long*>(row_count + pr.a), 1ULL);
     }
+}
+
+// row_start[d] = the first sorted position with key >= d (keys sorted, the invalid key
+// n_nodes last): position j sets the rows between its predecessor's key and its own.
+__global__ void k_row_starts(const unsigned* __restrict__ keys, i64 e, i64 n_nodes,
+                             i64* __restrict__ row_start) {
+    i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > e) return;
+    i64 prev = j == 0 ? -1 : (i64)keys[j - 1];
+    i64 cur = j == e ? n_nodes : (i64)keys[j];
+    if (cur > n_nodes) cur = n_nodes;
+    for (i64 d = prev + 1; d <= cur; ++d) row_start[d] = j;
 }
 
 // partners (int64) and, when asked, the row of every entry (int32)
@@ -414,8 +422,10 @@ extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int
                             void* workspace, size_t workspace_bytes, void* stream) {
     if (count < 0 || n_nodes < 1 || n_nodes >= 0x7fffffffLL) return TD3_EINVAL;
     cudaStream_t s = td3_stream(stream);
-    TD3_TRY(cudaMemsetAsync(row_start, 0, sizeof(i64) * (n_nodes + 1), s));
-    if (count == 0) return TD3_OK;
+    if (count == 0) {
+        TD3_TRY(cudaMemsetAsync(row_start, 0, sizeof(i64) * (n_nodes + 1), s));
+        return TD3_OK;
+    }
     i64 e = mutual ? 2 * count : count;
     Workspace w(workspace, workspace_bytes);
     unsigned* k0 = w.take<unsigned>(e);
@@ -423,15 +433,14 @@ extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int
     unsigned* v0 = w.take<unsigned>(e);
     unsigned* v1 = w.take<unsigned>(e);
     if (!v1) return TD3_EWORKSPACE;
-    // row counts go to row_start[1..], then an exclusive scan in place makes offsets
     k_csr_keys<<<td3_blocks(count, 256), 256, 0, s>>>(reinterpret_cast<const Pair*>(pairs), count,
-                                                      mutual, (unsigned)n_nodes, k0, v0, row_start);
+                                                      mutual, (unsigned)n_nodes, k0, v0);
     TD3_CHECK_LAUNCH();
     unsigned *ko, *vo;
     TD3_TRY_RC(td3_radix_sort_u32(k0, k1, v0, v1, e, bits_for(n_nodes), &ko, &vo, w.base + w.used,
                                   w.size - w.used, s));
-    TD3_TRY_RC(td3_exclusive_scan_i64(row_start, row_start, n_nodes + 1, nullptr, w.base + w.used,
-                                      w.size - w.used, s));
+    // the row offsets from the boundaries between equal keys of the sorted entries
+    k_row_starts<<<td3_blocks(e + 1, 256), 256, 0, s>>>(ko, e, n_nodes, row_start);
     // valid entries sort before the invalid key n_nodes (row_start[n_nodes] of them); the
     // entries after them are widened too (partners holds e slots), so no host read
     k_csr_out<<<td3_blocks(e, 256), 256, 0, s>>>(vo, ko, e, partners, entry_row);
