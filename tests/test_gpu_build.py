@@ -100,6 +100,47 @@ def test_moments_are_identical():
         np.testing.assert_array_equal(_np(tree._cartesian_moments()), data[f"cart{order}/moments"])
 
 
+@pytest.mark.parametrize("order,capacity", [(1, 40), (7, 70), (12, 8), (12, 100), (15, 33)])
+@pytest.mark.parametrize("adjoint", [False, True])
+def test_log_moments_of_low_orders_equal_the_coefficient_per_thread_form(order, capacity,
+                                                                         adjoint):
+    """Orders below 16 (leaf moments a thread per leaf, M2M 16 lanes per node) against
+    the first coefficients of order 20 (a thread per node and coefficient): a_n does not
+    depend on the order, so the bits agree.  Leaves of several dozen particles; plain
+    and dipole (adjoint) terms."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, _lib
+
+    rng = np.random.default_rng(order + capacity)
+    pos = np.concatenate([rng.uniform(-1, 1, (2, 6000)), rng.normal(0.3, 0.01, (2, 3000))], 1)
+    charge = rng.normal(size=pos.shape[1])
+    dipole = None
+    results = []
+    for p in (order, 20):
+        tree = FlatQuadtree(pos, charge, Quad(0, 0, 1), kernel="log", order=p,
+                            leaf_capacity=capacity)
+        if not adjoint:
+            results.append((tree.node_qabs, tree.moment_re[:, : order + 1],
+                            tree.moment_im[:, : order + 1]))
+            continue
+        dev, count = tree.device, tree.node_count
+        if dipole is None:
+            dipole = torch.tensor(rng.normal(size=(2, pos.shape[1])), device=dev)
+        levels = np.ascontiguousarray(tree.levels, dtype=np.int64)
+        binom = tree._binomial()
+        wabs = torch.empty(count, dtype=torch.float64, device=dev)
+        mre = torch.empty((count, p + 1), dtype=torch.float64, device=dev)
+        mim = torch.empty_like(mre)
+        _lib.call("td3_log_moments_adjoint", levels.ctypes.data, len(levels) - 1, p,
+                  tree._sorted_pos.data_ptr(), tree._sorted_charge.data_ptr(),
+                  dipole.data_ptr(), pos.shape[1], tree.node_center.data_ptr(),
+                  tree.node_start.data_ptr(), tree.node_end.data_ptr(),
+                  tree.node_child.data_ptr(), binom.data_ptr(), binom.shape[0],
+                  wabs.data_ptr(), mre.data_ptr(), mim.data_ptr(), _lib.stream(dev))
+        results.append((wabs, mre[:, : order + 1], mim[:, : order + 1]))
+    for low, high in zip(*results):
+        assert torch.equal(low, high)
+
+
 @pytest.mark.parametrize("kernel", ["log", "coulomb"])
 def test_set_charges_equals_a_new_tree(kernel):
     from tree_d_3d_b200 import FlatQuadtree, Quad

@@ -135,89 +135,52 @@ __global__ void k_log_moments(i64 lo, i64 hi, int order, const double* __restric
     if (n == 0) node_qabs[node] = qabs;
 }
 
-// The same moments with one thread per node and every coefficient in registers (orders
-// up to P, compile-time loop bounds); the operations and their order per coefficient are
-// those of k_log_moments, so the results are the same bits.
+
+// The leaf moments with one thread per leaf and every coefficient in registers (orders
+// up to P, compile-time loop bounds), every leaf of the tree in one launch; the
+// operations and their order per coefficient are those of k_log_moments, so the
+// results are the same bits.
 template <int P>
-__global__ void k_log_moments_node(i64 lo, i64 hi, int order, const double* __restrict__ spos,
+__global__ void k_log_leaf_moments(i64 count, int order, const double* __restrict__ spos,
                                    const double* __restrict__ scharge, i64 n_particles,
                                    const double* __restrict__ node_center,
                                    const i64* __restrict__ node_start,
                                    const i64* __restrict__ node_end,
-                                   const i64* __restrict__ node_child,
-                                   const double* __restrict__ binomial, int bsize,
-                                   double* node_qabs, double* moment_re, double* moment_im,
-                                   const double* __restrict__ sdip, int part) {
+                                   const i64* __restrict__ node_child, double* node_qabs,
+                                   double* moment_re, double* moment_im,
+                                   const double* __restrict__ sdip) {
     constexpr int W = P + 1;
-    i64 node = lo + (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (node >= hi) return;
-    i64 first = node_child[node];
-    // part 1: leaves only (all levels in one launch), part 2: parents only (one level)
-    if ((part == 1 && first >= 0) || (part == 2 && first < 0)) return;
+    i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= count || node_child[node] >= 0) return;
     int w = order + 1;
     double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
     double ar[W], ai[W];
 #pragma unroll
     for (int n = 0; n < W; ++n) ar[n] = ai[n] = 0.0;
     double qabs = 0.0;
-    if (first < 0) {
-        for (i64 k = node_start[node]; k < node_end[node]; ++k) {
-            double q = scharge[k];
-            qabs += fabs(q);
-            double dx = spos[k] - xmid, dy = spos[n_particles + k] - ymid;
-            double pr = q, pi = 0.0;
+    for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+        double q = scharge[k];
+        qabs += fabs(q);
+        double dx = spos[k] - xmid, dy = spos[n_particles + k] - ymid;
+        double pr = q, pi = 0.0;
 #pragma unroll
-            for (int n = 0; n < W; ++n) {
-                ar[n] += pr;
-                ai[n] += pi;
-                double next_re = pr * dx - pi * dy;
-                pi = pr * dy + pi * dx;
-                pr = next_re;
-            }
-            if (sdip) {
-                double er = sdip[k], ei = sdip[n_particles + k];
-                double zr = 1.0, zi = 0.0;
-#pragma unroll
-                for (int n = 1; n < W; ++n) {
-                    ar[n] -= n * (er * zr - ei * zi);
-                    ai[n] -= n * (er * zi + ei * zr);
-                    double nr = zr * dx - zi * dy;
-                    zi = zr * dy + zi * dx;
-                    zr = nr;
-                }
-            }
+        for (int n = 0; n < W; ++n) {
+            ar[n] += pr;
+            ai[n] += pi;
+            double next_re = pr * dx - pi * dy;
+            pi = pr * dy + pi * dx;
+            pr = next_re;
         }
-    } else {
-        for (i64 child = first; child < first + 4; ++child) {
-            qabs += node_qabs[child];
-            if (node_end[child] == node_start[child]) continue;
-            double s_re = node_center[2 * child] - xmid;
-            double s_im = node_center[2 * child + 1] - ymid;
-            double sh_re[W], sh_im[W], cr[W], ci[W];
-            sh_re[0] = 1.0;
-            sh_im[0] = 0.0;
+        if (sdip) {
+            double er = sdip[k], ei = sdip[n_particles + k];
+            double zr = 1.0, zi = 0.0;
 #pragma unroll
             for (int n = 1; n < W; ++n) {
-                sh_re[n] = sh_re[n - 1] * s_re - sh_im[n - 1] * s_im;
-                sh_im[n] = sh_re[n - 1] * s_im + sh_im[n - 1] * s_re;
-            }
-#pragma unroll
-            for (int m = 0; m < W; ++m) {
-                cr[m] = m < w ? moment_re[child * w + m] : 0.0;
-                ci[m] = m < w ? moment_im[child * w + m] : 0.0;
-            }
-#pragma unroll
-            for (int n = 0; n < W; ++n) {
-                double acc_re = 0.0, acc_im = 0.0;
-#pragma unroll
-                for (int m = 0; m <= n; ++m) {
-                    double c = binomial[n * bsize + m];
-                    double a_re = cr[m] * c, a_im = ci[m] * c;
-                    acc_re += a_re * sh_re[n - m] - a_im * sh_im[n - m];
-                    acc_im += a_re * sh_im[n - m] + a_im * sh_re[n - m];
-                }
-                ar[n] += acc_re;
-                ai[n] += acc_im;
+                ar[n] -= n * (er * zr - ei * zi);
+                ai[n] -= n * (er * zi + ei * zr);
+                double nr = zr * dx - zi * dy;
+                zi = zr * dy + zi * dx;
+                zr = nr;
             }
         }
     }
@@ -231,36 +194,132 @@ __global__ void k_log_moments_node(i64 lo, i64 hi, int order, const double* __re
     node_qabs[node] = qabs;
 }
 
-// Moments of every node.  Orders up to 16: every leaf in one launch (leaves depend on
-// nothing), then the parents level by level, deepest first; higher orders: thread per
-// (node, coefficient), level by level.
+// M2M of the internal nodes of one level, a thread per (node, child) with the child's
+// coefficients and the powers of its shift in registers (orders up to P): each thread
+// forms its child's shifted coefficients c_n = sum_m C(n, m) a_m s^(n-m) in the order of
+// k_log_moments into shared memory, then a thread per (node, n) adds the four children
+// in order.  The operations are those of k_log_moments, so the results are the same bits.
+constexpr int M2M_NODES = 32;  // nodes per block (4 threads each)
+
+template <int P>
+__global__ void __launch_bounds__(M2M_NODES * 4)
+k_log_m2m_level(i64 lo, i64 hi, int order, const double* __restrict__ node_center,
+                const i64* __restrict__ node_start, const i64* __restrict__ node_end,
+                const i64* __restrict__ node_child, const double* __restrict__ binomial,
+                int bsize, double* node_qabs, double* moment_re, double* moment_im) {
+    constexpr int W = P + 1;
+    __shared__ double2 shifted[M2M_NODES][4][W];
+    __shared__ int present[M2M_NODES][4];
+    int w = order + 1;
+    int local = threadIdx.x >> 2, c = threadIdx.x & 3;
+    i64 node = lo + (i64)blockIdx.x * M2M_NODES + local;
+    int has = 0;
+    if (node < hi) {
+        i64 first = node_child[node];
+        if (first >= 0) {
+            i64 child = first + c;
+            has = node_end[child] != node_start[child];
+            if (has) {
+                double s_re = node_center[2 * child] - node_center[2 * node];
+                double s_im = node_center[2 * child + 1] - node_center[2 * node + 1];
+                double sh_re[W], sh_im[W], cr[W], ci[W];
+                sh_re[0] = 1.0;
+                sh_im[0] = 0.0;
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    sh_re[n] = sh_re[n - 1] * s_re - sh_im[n - 1] * s_im;
+                    sh_im[n] = sh_re[n - 1] * s_im + sh_im[n - 1] * s_re;
+                }
+#pragma unroll
+                for (int m = 0; m < W; ++m) {
+                    cr[m] = m < w ? moment_re[child * w + m] : 0.0;
+                    ci[m] = m < w ? moment_im[child * w + m] : 0.0;
+                }
+#pragma unroll
+                for (int n = 0; n < W; ++n) {
+                    double c_re = 0.0, c_im = 0.0;
+#pragma unroll
+                    for (int m = 0; m <= n; ++m) {
+                        double b = binomial[n * bsize + m];
+                        double a_re = cr[m] * b, a_im = ci[m] * b;
+                        c_re += a_re * sh_re[n - m] - a_im * sh_im[n - m];
+                        c_im += a_re * sh_im[n - m] + a_im * sh_re[n - m];
+                    }
+                    shifted[local][c][n] = make_double2(c_re, c_im);
+                }
+            }
+        } else {
+            has = -1;  // a leaf: its moments come from its particles
+        }
+    } else {
+        has = -1;
+    }
+    present[local][c] = has;
+    __syncthreads();
+    for (int item = threadIdx.x; item < M2M_NODES * w; item += blockDim.x) {
+        int k = item / w, n = item - k * w;
+        i64 out = lo + (i64)blockIdx.x * M2M_NODES + k;
+        if (present[k][0] < 0) continue;
+        double acc_re = 0.0, acc_im = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            if (!present[k][j]) continue;
+            double2 v = shifted[k][j][n];
+            acc_re += v.x;
+            acc_im += v.y;
+        }
+        moment_re[out * w + n] = acc_re;
+        moment_im[out * w + n] = acc_im;
+        if (n == 0) {
+            i64 first = node_child[out];
+            double qabs = 0.0;
+            for (i64 child = first; child < first + 4; ++child) qabs += node_qabs[child];
+            node_qabs[out] = qabs;
+        }
+    }
+}
+
+// Moments of every node.  Orders up to 15: every leaf in one launch (leaves depend on
+// nothing), then the internal nodes level by level, deepest first, a thread per (node,
+// child); higher orders: thread per (node, coefficient), level by level.
 int launch_log_moments(const int64_t* levels, int64_t n_levels, int order, const double* spos,
                        const double* scharge, int64_t n, const double* center, const i64* start,
                        const i64* end, const i64* child, const double* binomial, int bsize,
                        double* qabs, double* mre, double* mim, const double* sdip,
                        cudaStream_t s) {
-    auto node_kernel = [&](i64 lo, i64 hi, int part) {
-        unsigned nb = td3_blocks(hi - lo, MOM_THREADS);
-#define TD3_NODE_MOMENTS(P)                                                                  \
-    k_log_moments_node<P><<<nb, MOM_THREADS, 0, s>>>(lo, hi, order, spos, scharge, n, center, \
-                                                     start, end, child, binomial, bsize, qabs,\
-                                                     mre, mim, sdip, part)
+    i64 count = levels[n_levels];
+    if (count <= 0) return TD3_OK;
+    if (order <= 15) {
+        unsigned nb = td3_blocks(count, MOM_THREADS);
+#define TD3_LEAF_MOMENTS(P)                                                                  \
+    k_log_leaf_moments<P><<<nb, MOM_THREADS, 0, s>>>(count, order, spos, scharge, n, center, \
+                                                     start, end, child, qabs, mre, mim, sdip)
+#define TD3_M2M(P)                                                                           \
+    k_log_m2m_level<P><<<nb, M2M_NODES * 4, 0, s>>>(lo, hi, order, center, start, end, child, \
+                                                    binomial, bsize, qabs, mre, mim)
         if (order <= 4)
-            TD3_NODE_MOMENTS(4);
+            TD3_LEAF_MOMENTS(4);
         else if (order <= 8)
-            TD3_NODE_MOMENTS(8);
+            TD3_LEAF_MOMENTS(8);
         else if (order <= 12)
-            TD3_NODE_MOMENTS(12);
+            TD3_LEAF_MOMENTS(12);
         else
-            TD3_NODE_MOMENTS(16);
-#undef TD3_NODE_MOMENTS
-    };
-    if (order <= 16) {
-        node_kernel(0, levels[n_levels], 1);
+            TD3_LEAF_MOMENTS(15);
         for (i64 level = n_levels - 2; level >= 0; --level) {
             i64 lo = levels[level], hi = levels[level + 1];
-            if (hi > lo) node_kernel(lo, hi, 2);
+            if (hi <= lo) continue;
+            nb = (unsigned)((hi - lo + M2M_NODES - 1) / M2M_NODES);
+            if (order <= 4)
+                TD3_M2M(4);
+            else if (order <= 8)
+                TD3_M2M(8);
+            else if (order <= 12)
+                TD3_M2M(12);
+            else
+                TD3_M2M(15);
         }
+#undef TD3_LEAF_MOMENTS
+#undef TD3_M2M
     } else {
         for (i64 level = n_levels - 1; level >= 0; --level) {
             i64 lo = levels[level], hi = levels[level + 1];
