@@ -101,7 +101,8 @@ int td3_pair_energy(const double* pos, const double* charge, int64_t n, double s
  * particles of a cell keep their input order.  Writes the node arrays (capacity rows:
  * node_center (capacity, 2), node_half, node_start, node_end, node_child (-1 for
  * leaves), node_depth), perm (n; the particles in tree order) and sorted_pos (2, n;
- * pos[:, perm]).  levels (HOST, capacity + 1) receives the first node of each depth;
+ * pos[:, perm]).  levels (HOST, min(capacity, max_depth + 1) + 1) receives the first
+ * node of each depth;
  * sizes (HOST, 4) receives node count, number of levels and 1 if capacity was too
  * small (then TD3_ENEEDMORE is returned, the tree is unfinished and sizes[0] is the
  * node count needed, or a lower bound of it: retry with a larger capacity, as the

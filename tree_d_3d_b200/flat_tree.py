@@ -314,7 +314,8 @@ class FlatQuadtree:
             self.node_end = torch.empty(capacity, dtype=i64, device=dev)
             self.node_child = torch.empty(capacity, dtype=i64, device=dev)
             self.node_depth = torch.empty(capacity, dtype=i64, device=dev)
-            levels = np.zeros(capacity + 1, dtype=np.int64)
+            # the first node of each depth: at most max_depth + 2 entries
+            levels = np.zeros(min(capacity, self.max_depth + 1) + 1, dtype=np.int64)
             ws = _lib.workspace(_lib.query("td3_quadtree_build_workspace_size", n, capacity), dev)
             q = self.root_quad
             rc = _lib.call_code(
