@@ -255,6 +255,15 @@ struct NearWindow {
     int tag[NF_CAP];  // slot j (self-exclusion) or the source's input index (OTHER)
 };
 
+// The length unit u of the mixed-precision pair arithmetic: the power of two with
+// unit <= u < 2 unit.  Positions scale by 1/u exactly, so the FP64 difference of two
+// scaled positions is the scaled FP64 difference of the positions.
+__device__ __forceinline__ double pair_unit(double unit) {
+    int e;
+    frexp(unit, &e);
+    return ldexp(1.0, e);
+}
+
 // One mixed-precision pair: the difference in FP64 (exact enough for close pairs far
 // from the origin), in units of L = S.unit and rounded to FP32, then FP32 arithmetic with
 // compensated accumulation.  Coulomb sums q / r' and q d' / r'^3; log sums -q ln r'^2
@@ -547,14 +556,11 @@ __device__ __forceinline__ void adjoint_pair_mixed(float dx, float dy, float eps
     }
 }
 
-template <int LOCAL>
-__device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, i64 n,
-                                               double ux, double uy, i64 leaf, int order,
-                                               int width, const double* fa, const double* fb,
-                                               const double* ba, const double* bb,
-                                               const Sources& S, const Adjoint& A) {
-    LocalJet f = local_jet<LOCAL>(fa, fb, leaf, order, width, ux, uy);  // forward: Hessian
-    LocalJet b = local_jet<LOCAL>(ba, bb, leaf, order, width, ux, uy);  // adjoint: Psi
+// qbar and xbar of slot k (input index i) from the near sums acc and the far parts: f
+// the forward local expansion's jet (its Hessian), b the adjoint one's (Psi, grad Psi).
+__device__ __forceinline__ void adjoint_combine(const double* acc, const LocalJet& f,
+                                                const LocalJet& b, i64 k, i64 i, i64 n,
+                                                const Sources& S, const Adjoint& A) {
     double psi = acc[0] + b.v;
     double gx = acc[1] + b.gx, gy = acc[2] + b.gy;
     double mxx = acc[3] + f.hxx, mxy = acc[4] + f.hxy, myy = acc[5] + f.hyy;
@@ -564,25 +570,46 @@ __device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, 
     A.xbar[n + i] = -w * A.efield[n + i] + q * gy - (mxy * ex + myy * ey);
 }
 
+template <int LOCAL>
+__device__ __forceinline__ void adjoint_finish(const double* acc, i64 k, i64 i, i64 n,
+                                               double ux, double uy, i64 leaf, int order,
+                                               int width, const double* fa, const double* fb,
+                                               const double* ba, const double* bb,
+                                               const Sources& S, const Adjoint& A) {
+    LocalJet f = local_jet<LOCAL>(fa, fb, leaf, order, width, ux, uy);  // forward: Hessian
+    LocalJet b = local_jet<LOCAL>(ba, bb, leaf, order, width, ux, uy);  // adjoint: Psi
+    adjoint_combine(acc, f, b, k, i, n, S, A);
+}
+
 constexpr int NF_CAP_ADJ = 128;  // staged sources per warp window (adjoint)
 
+// FP64: positions, charges, monopoles and dipoles.  Mixed: positions (scaled by 1/u)
+// and monopoles in FP64 (the pair difference and the monopole sum), the rest in FP32
+// (dipoles scaled by 1/u), converted once per staged source instead of once per pair.
+template <bool MIXED>
 struct AdjointWindow {
     double x[NF_CAP_ADJ], y[NF_CAP_ADJ], q[NF_CAP_ADJ], w[NF_CAP_ADJ], ex[NF_CAP_ADJ],
         ey[NF_CAP_ADJ];
     int tag[NF_CAP_ADJ];  // slot j (self-exclusion)
 };
+template <>
+struct AdjointWindow<true> {
+    double x[NF_CAP_ADJ], y[NF_CAP_ADJ], w[NF_CAP_ADJ];
+    float qf[NF_CAP_ADJ], wf[NF_CAP_ADJ], exf[NF_CAP_ADJ], eyf[NF_CAP_ADJ];
+    int tag[NF_CAP_ADJ];
+};
 
 template <int KERNEL, int LOCAL, bool MIXED>
-__global__ void __launch_bounds__(32 * NF_WARPS)
+__global__ void __launch_bounds__(32 * NF_WARPS, 6)
 k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
                const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
                const i64* __restrict__ partners, const double* __restrict__ fa,
                const double* __restrict__ fb, const double* __restrict__ ba,
                const double* __restrict__ bb, int order, int width, double eps2,
                double* __restrict__ partial) {
-    __shared__ AdjointWindow windows[NF_WARPS];
+    __shared__ AdjointWindow<MIXED> windows[NF_WARPS];
     int lane = threadIdx.x & 31;
-    AdjointWindow& win = windows[threadIdx.x >> 5];
+    AdjointWindow<MIXED>& win = windows[threadIdx.x >> 5];
     i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     i64 leaf = seg_leaf[seg];
@@ -597,38 +624,47 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
     // mixed: in units of L = S.unit (d' = d / L, e' = e / L) the log kernel's sums scale
     // as (1, 1/L, 1/L^2) plus -ln L^2 sum w for Psi, the Coulomb kernel's as
     // (1/L, 1/L^2, 1/L^3)
-    const double inv_unit = 1.0 / S.unit;
+    // mixed: positions in units of u (pair_unit), scaled exactly
+    const double unit = MIXED ? pair_unit(S.unit) : 1.0, inv_unit = 1.0 / unit;
     const float eps2f = (float)(eps2 * inv_unit * inv_unit);
     auto stage = [&](int p, i64 j) {
-        win.x[p] = S.pos[j];
-        win.y[p] = S.pos[n + j];
-        win.q[p] = S.charge[j];
+        win.x[p] = S.pos[j] * inv_unit;
+        win.y[p] = S.pos[n + j] * inv_unit;
         win.w[p] = A.weight[j];
-        win.ex[p] = A.dipole[j];
-        win.ey[p] = A.dipole[n + j];
         win.tag[p] = (int)j;
+        if constexpr (MIXED) {
+            win.qf[p] = (float)S.charge[j];
+            win.wf[p] = (float)A.weight[j];
+            win.exf[p] = (float)(A.dipole[j] * inv_unit);
+            win.eyf[p] = (float)(A.dipole[n + j] * inv_unit);
+        } else {
+            win.q[p] = S.charge[j];
+            win.ex[p] = A.dipole[j];
+            win.ey[p] = A.dipole[n + j];
+        }
     };
     for (int base = 0; base < count; base += tsz) {
         int it = base + ti;
         bool valid = it < count;
         i64 k = s0 + (valid ? it : 0);
         double xi = S.pos[k], yi = S.pos[n + k];
+        double xs = xi * inv_unit, ys = yi * inv_unit;
+        int self = (int)k;
         double acc[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         KahanF kacc[6];
         double wsum = 0.0;
         for_source_windows<NF_CAP_ADJ>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
             if (!valid) return;
             for (int p = slice; p < wn; p += slices) {
-                if (win.tag[p] == k) continue;
-                double dx = xi - win.x[p], dy = yi - win.y[p];
-                if (MIXED) {
-                    if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) continue;
-                    double wj = win.w[p];
-                    if (KERNEL == TD3_KERNEL_LOG) wsum += wj;
-                    adjoint_pair_mixed<KERNEL>((float)(dx * inv_unit), (float)(dy * inv_unit),
-                                               eps2f, (float)win.q[p], (float)wj,
-                                               (float)(win.ex[p] * inv_unit),
-                                               (float)(win.ey[p] * inv_unit), kacc);
+                if (win.tag[p] == self) continue;
+                double dx = xs - win.x[p], dy = ys - win.y[p];
+                if constexpr (MIXED) {
+                    float dxf = (float)dx, dyf = (float)dy;
+                    if (dxf == 0.0f && dyf == 0.0f && eps2 == 0.0 && dx == 0.0 && dy == 0.0)
+                        continue;
+                    if (KERNEL == TD3_KERNEL_LOG) wsum += win.w[p];
+                    adjoint_pair_mixed<KERNEL>(dxf, dyf, eps2f, win.qf[p], win.wf[p], win.exf[p],
+                                               win.eyf[p], kacc);
                 } else {
                     if (dx * dx + dy * dy + eps2 == 0.0) continue;
                     adjoint_pair<KERNEL>(dx, dy, eps2, win.q[p], win.w[p], win.ex[p], win.ey[p],
@@ -639,7 +675,7 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
         if (MIXED) {
             double sc = KERNEL == TD3_KERNEL_LOG ? 1.0 : inv_unit;
             acc[0] = kacc[0].value() * sc;
-            if (KERNEL == TD3_KERNEL_LOG) acc[0] -= 2.0 * log(S.unit) * wsum;
+            if (KERNEL == TD3_KERNEL_LOG) acc[0] -= 2.0 * log(unit) * wsum;
             for (int c = 1; c < 3; ++c) acc[c] = kacc[c].value() * (sc * inv_unit);
             for (int c = 3; c < 6; ++c) acc[c] = kacc[c].value() * (sc * inv_unit * inv_unit);
         }
@@ -647,15 +683,26 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
         for (int c = 0; c < 6; ++c)
             for (int off = tsz; off < 32; off <<= 1)
                 acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
-        if (valid && slice == 0) {
-            if (outp < 0) {
-                adjoint_finish<LOCAL>(acc, k, T.perm[k], n, xi - T.center[2 * leaf],
-                                      yi - T.center[2 * leaf + 1], leaf, order, width, fa, fb, ba,
-                                      bb, S, A);
-            } else {
-                i64 p = outp + it;
-                for (int c = 0; c < 6; ++c) partial[6 * p + c] = acc[c];
+        if (outp < 0) {
+            // the two far-field jets in one instruction stream: slice 0 evaluates the
+            // forward expansion, slice 1 the adjoint one (with a single slice, slice 0
+            // evaluates both)
+            double ux = xi - T.center[2 * leaf], uy = yi - T.center[2 * leaf + 1];
+            bool adj = slices > 1 && slice == 1;
+            LocalJet f{}, b{};
+            if (valid && slice <= 1)
+                f = local_jet<LOCAL>(adj ? ba : fa, adj ? bb : fb, leaf, order, width, ux, uy);
+            if (slices > 1) {
+                b.v = __shfl_down_sync(0xffffffffu, f.v, tsz);
+                b.gx = __shfl_down_sync(0xffffffffu, f.gx, tsz);
+                b.gy = __shfl_down_sync(0xffffffffu, f.gy, tsz);
+            } else if (valid) {
+                b = local_jet<LOCAL>(ba, bb, leaf, order, width, ux, uy);
             }
+            if (valid && slice == 0) adjoint_combine(acc, f, b, k, T.perm[k], n, S, A);
+        } else if (valid && slice == 0) {
+            i64 p = outp + it;
+            for (int c = 0; c < 6; ++c) partial[6 * p + c] = acc[c];
         }
     }
 }
