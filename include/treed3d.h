@@ -222,27 +222,30 @@ int td3_evaluate_quadtree(int kernel, const double* targets, int64_t m, const in
  * Synchronises `stream` once per 8 generations.  Replaces fmm_traverse
  * (src/tree_d_3d/kernels/fmm_traverse/fmm_traverse_pyccel.py:15-106,
  * fmm_traverse_cuda.cu:14-97) driven by FlatQuadtree._traverse
- * (src/tree_d_3d/flat_tree.py:1318-1358); identical lists. */
-size_t td3_fmm_traverse_workspace_size(int64_t frontier_capacity);
+ * (src/tree_d_3d/flat_tree.py:1318-1358); identical lists.  n_nodes: the node count
+ * (the traversal first packs each node into one 32-byte record in the workspace). */
+size_t td3_fmm_traverse_workspace_size(int64_t frontier_capacity, int64_t n_nodes);
 int td3_fmm_traverse(const double* node_center, const double* node_half,
                      const int64_t* node_start, const int64_t* node_end,
-                     const int64_t* node_child, double theta, int64_t* m2l, int64_t m2l_capacity,
-                     int64_t* p2p, int64_t p2p_capacity, int64_t frontier_capacity,
-                     int64_t* sizes, void* workspace, size_t workspace_bytes, void* stream);
+                     const int64_t* node_child, int64_t n_nodes, double theta, int64_t* m2l,
+                     int64_t m2l_capacity, int64_t* p2p, int64_t p2p_capacity,
+                     int64_t frontier_capacity, int64_t* sizes, void* workspace,
+                     size_t workspace_bytes, void* stream);
 
 /* The one-way traversal of a target tree (t_*) against a source tree (s_*) from
  * (root, root), with the predicates of td3_fmm_traverse; pairs are (target cell,
  * source cell), breadth first (the reference walks depth first: the same set of
  * pairs in another order).  Replaces dual_traverse (src/tree_d_3d/kernels/
  * dual_traverse/dual_traverse_pyccel.py:14-86) of FlatQuadtree._dual_lists
- * (src/tree_d_3d/flat_tree.py:1086-1122).  Uses the workspace size of
- * td3_fmm_traverse_workspace_size. */
+ * (src/tree_d_3d/flat_tree.py:1086-1122).  t_nodes, s_nodes: the node counts; the
+ * workspace size is td3_fmm_traverse_workspace_size(frontier_capacity, t_nodes + s_nodes). */
 int td3_dual_traverse(const double* t_center, const double* t_half, const int64_t* t_start,
-                      const int64_t* t_end, const int64_t* t_child, const double* s_center,
-                      const double* s_half, const int64_t* s_start, const int64_t* s_end,
-                      const int64_t* s_child, double theta, int64_t* m2l, int64_t m2l_capacity,
-                      int64_t* p2p, int64_t p2p_capacity, int64_t frontier_capacity,
-                      int64_t* sizes, void* workspace, size_t workspace_bytes, void* stream);
+                      const int64_t* t_end, const int64_t* t_child, int64_t t_nodes,
+                      const double* s_center, const double* s_half, const int64_t* s_start,
+                      const int64_t* s_end, const int64_t* s_child, int64_t s_nodes,
+                      double theta, int64_t* m2l, int64_t m2l_capacity, int64_t* p2p,
+                      int64_t p2p_capacity, int64_t frontier_capacity, int64_t* sizes,
+                      void* workspace, size_t workspace_bytes, void* stream);
 
 /* Rows by node of the pairs (count, 2): row_start (n_nodes + 1) and partners, in pair
  * order; mutual != 0 lists b under a and a under b (once if a == b).  partners holds

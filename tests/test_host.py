@@ -29,7 +29,7 @@ def test_library_exports_every_declared_entry_point():
     assert _lib.query("td3_direct_sum_workspace_size", 100, 10_000) > 0
     assert _lib.query("td3_quadtree_build_workspace_size", 1000, 4000) > 0
     assert _lib.query("td3_walk_workspace_size", 1000, 0) > 0
-    assert _lib.query("td3_fmm_traverse_workspace_size", 1000) > 0
+    assert _lib.query("td3_fmm_traverse_workspace_size", 1000, 500) > 0
     assert _lib.query("td3_pair_csr_workspace_size", 1000, 1, 500) > 0
     assert _lib.query("td3_nearfield_plan_workspace_size", 500) > 0
 

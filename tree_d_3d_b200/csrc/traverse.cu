@@ -21,24 +21,44 @@ struct Pair {
     i64 a, b;
 };
 
+// A frontier pair: node indices fit 32 bits (the entry points check the node counts).
+struct __align__(8) FPair {
+    int a, b;
+};
+
 enum : int { ACT_NONE = 0, ACT_M2L = 1, ACT_P2P = 2, ACT_SELF = 3, ACT_SPLIT_A = 4, ACT_SPLIT_B = 5 };
 
+// A node as the traversal reads it: one 32-byte record (one memory sector) instead of
+// five arrays.  child is the first child (-1 for a leaf), filled is 0 for an empty cell.
+struct __align__(32) NodeRec {
+    double cx, cy, half;
+    int child, filled;
+};
+
+__global__ void k_node_records(i64 count, const double* __restrict__ center,
+                               const double* __restrict__ half, const i64* __restrict__ start,
+                               const i64* __restrict__ end, const i64* __restrict__ child,
+                               NodeRec* __restrict__ rec) {
+    i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    rec[i] = NodeRec{center[2 * i], center[2 * i + 1], half[i], (int)child[i],
+                     end[i] != start[i] ? 1 : 0};
+}
+
 // The decision of the mutual traversal for pair (a, b) (fmm_traverse_pyccel.py:48-106).
-__device__ __forceinline__ int classify_mutual(i64 a, i64 b, const double* __restrict__ center,
-                                               const double* __restrict__ half,
-                                               const i64* __restrict__ start,
-                                               const i64* __restrict__ end,
-                                               const i64* __restrict__ child, double theta) {
-    if (end[a] == start[a] || end[b] == start[b]) return ACT_NONE;
-    bool leaf_a = child[a] < 0, leaf_b = child[b] < 0;
+__device__ __forceinline__ int classify_mutual(i64 a, i64 b, const NodeRec* __restrict__ rec,
+                                               double theta) {
+    NodeRec ra = rec[a], rb = rec[b];
+    if (!ra.filled || !rb.filled) return ACT_NONE;
+    bool leaf_a = ra.child < 0, leaf_b = rb.child < 0;
     if (a == b) return leaf_a ? ACT_P2P : ACT_SELF;
-    double dx = xsub(center[2 * a], center[2 * b]);
-    double dy = xsub(center[2 * a + 1], center[2 * b + 1]);
+    double dx = xsub(ra.cx, rb.cx);
+    double dy = xsub(ra.cy, rb.cy);
     double distance = xsqrt(xnorm2(dx, dy));
-    double radii = xmul(TD3_ROOT2, xadd(half[a], half[b]));
+    double radii = xmul(TD3_ROOT2, xadd(ra.half, rb.half));
     if (radii < xmul(theta, distance)) return ACT_M2L;
     if (leaf_a && leaf_b) return ACT_P2P;
-    if (leaf_b || (!leaf_a && half[a] >= half[b])) return ACT_SPLIT_A;
+    if (leaf_b || (!leaf_a && ra.half >= rb.half)) return ACT_SPLIT_A;
     return ACT_SPLIT_B;
 }
 
@@ -55,24 +75,17 @@ __device__ __forceinline__ td3_i64x2 action_counts(int act) {
 }
 
 // The one-way decision for (target cell a, source cell b) (dual_traverse_pyccel.py:46-86).
-__device__ __forceinline__ int classify_dual(i64 a, i64 b, const double* __restrict__ t_center,
-                                             const double* __restrict__ t_half,
-                                             const i64* __restrict__ t_start,
-                                             const i64* __restrict__ t_end,
-                                             const i64* __restrict__ t_child,
-                                             const double* __restrict__ s_center,
-                                             const double* __restrict__ s_half,
-                                             const i64* __restrict__ s_start,
-                                             const i64* __restrict__ s_end,
-                                             const i64* __restrict__ s_child, double theta) {
-    if (t_end[a] == t_start[a] || s_end[b] == s_start[b]) return ACT_NONE;
-    double dx = xsub(t_center[2 * a], s_center[2 * b]);
-    double dy = xsub(t_center[2 * a + 1], s_center[2 * b + 1]);
-    if (xmul(TD3_ROOT2, xadd(t_half[a], s_half[b])) < xmul(theta, xsqrt(xnorm2(dx, dy))))
+__device__ __forceinline__ int classify_dual(i64 a, i64 b, const NodeRec* __restrict__ t_rec,
+                                             const NodeRec* __restrict__ s_rec, double theta) {
+    NodeRec ra = t_rec[a], rb = s_rec[b];
+    if (!ra.filled || !rb.filled) return ACT_NONE;
+    double dx = xsub(ra.cx, rb.cx);
+    double dy = xsub(ra.cy, rb.cy);
+    if (xmul(TD3_ROOT2, xadd(ra.half, rb.half)) < xmul(theta, xsqrt(xnorm2(dx, dy))))
         return ACT_M2L;
-    bool leaf_a = t_child[a] < 0, leaf_b = s_child[b] < 0;
+    bool leaf_a = ra.child < 0, leaf_b = rb.child < 0;
     if (leaf_a && leaf_b) return ACT_P2P;
-    if (leaf_b || (!leaf_a && t_half[a] >= s_half[b])) return ACT_SPLIT_A;
+    if (leaf_b || (!leaf_a && ra.half >= rb.half)) return ACT_SPLIT_A;
     return ACT_SPLIT_B;
 }
 
@@ -96,21 +109,11 @@ struct TravState {
     i64 need_m2l, need_p2p, need_frontier;
 };
 
-struct TreeView {
-    const double* center;
-    const double* half;
-    const i64* start;
-    const i64* end;
-    const i64* child;
-};
-
 template <bool DUAL>
-__device__ __forceinline__ int classify_pair(const TreeView& t, const TreeView& s, double theta,
-                                             Pair pr) {
-    if (DUAL)
-        return classify_dual(pr.a, pr.b, t.center, t.half, t.start, t.end, t.child, s.center,
-                             s.half, s.start, s.end, s.child, theta);
-    return classify_mutual(pr.a, pr.b, t.center, t.half, t.start, t.end, t.child, theta);
+__device__ __forceinline__ int classify_pair(const NodeRec* t, const NodeRec* s, double theta,
+                                             FPair pr) {
+    if (DUAL) return classify_dual(pr.a, pr.b, t, s, theta);
+    return classify_mutual(pr.a, pr.b, t, theta);
 }
 
 __device__ __forceinline__ td3_i64x2 warp_inclusive_x2(td3_i64x2 v, int lane) {
@@ -145,19 +148,20 @@ __device__ __forceinline__ td3_i64x2 block_exclusive_x2(td3_i64x2 v, td3_i64x2* 
     return off + inc - v;
 }
 
-__global__ void k_gen_init(TravState* st, Pair* frontier) {
+__global__ void k_gen_init(TravState* st, FPair* frontier) {
     st->nf[0] = 1;
     st->nf[1] = 0;
     st->emit_nf = 0;
     st->n_m2l = st->n_p2p = st->base_m2l = st->base_p2p = 0;
     st->overflow = st->need_m2l = st->need_p2p = st->need_frontier = 0;
-    frontier[0] = Pair{0, 0};
+    frontier[0] = FPair{0, 0};
 }
 
 template <bool DUAL>
 __global__ void __launch_bounds__(TRAV_THREADS)
-k_gen_classify(const Pair* __restrict__ frontier, const TravState* st, int parity, TreeView t,
-               TreeView s, double theta, signed char* __restrict__ action,
+k_gen_classify(const FPair* __restrict__ frontier, const TravState* st, int parity,
+               const NodeRec* __restrict__ t, const NodeRec* __restrict__ s, double theta,
+               signed char* __restrict__ action,
                td3_i64x2* __restrict__ tile_sum) {
     i64 nf = st->nf[parity];
     i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
@@ -213,42 +217,64 @@ k_gen_scan(TravState* st, int parity, td3_i64x2* __restrict__ tile_sum, i64 m2l_
     }
 }
 
+// Emit: a warp takes 32 * GEN_ITEMS consecutive pairs of the tile (round r, lane l:
+// pair warp_base + 32 r + l); the warps' totals are scanned once per tile, then each
+// round's slots come from a warp scan, in frontier order.
 template <bool DUAL>
 __global__ void __launch_bounds__(TRAV_THREADS)
-k_gen_emit(const Pair* __restrict__ frontier, const TravState* st,
+k_gen_emit(const FPair* __restrict__ frontier, const TravState* st,
            const signed char* __restrict__ action, const td3_i64x2* __restrict__ tile_off,
-           const i64* __restrict__ t_child, const i64* __restrict__ s_child,
-           Pair* __restrict__ m2l, Pair* __restrict__ p2p, Pair* __restrict__ next) {
+           const NodeRec* __restrict__ t_rec, const NodeRec* __restrict__ s_rec,
+           Pair* __restrict__ m2l, Pair* __restrict__ p2p, FPair* __restrict__ next) {
+    __shared__ td3_i64x2 warp_total[TRAV_THREADS / 32];
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     i64 nf = st->emit_nf;
     i64 base_m2l = st->base_m2l, base_p2p = st->base_p2p;
     i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
     for (i64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        i64 first = tile * GEN_TILE + (i64)wib * 32 * GEN_ITEMS;
+        int act[GEN_ITEMS];
+        td3_i64x2 mine(0);
+#pragma unroll
+        for (int r = 0; r < GEN_ITEMS; ++r) {
+            i64 k = first + r * 32 + lane;
+            act[r] = k < nf ? action[k] : ACT_NONE;
+            mine += action_counts(act[r]);
+        }
+        td3_i64x2 wsum = warp_inclusive_x2(mine, lane);
+        __syncthreads();  // the previous tile's readers are done with warp_total
+        if (lane == 31) warp_total[wib] = wsum;
+        __syncthreads();
         td3_i64x2 carry = tile_off[tile];
-        for (int i = 0; i < GEN_ITEMS; ++i) {
-            i64 k = tile * GEN_TILE + i * TRAV_THREADS + threadIdx.x;
-            int act = k < nf ? action[k] : ACT_NONE;
-            td3_i64x2 total;
-            td3_i64x2 off = carry + block_exclusive_x2(action_counts(act), &total);
-            carry += total;
-            if (act == ACT_NONE) continue;
-            Pair pr = frontier[k];
-            switch (act) {
-                case ACT_M2L: m2l[base_m2l + (off.a & 0xffffffffLL)] = pr; break;
-                case ACT_P2P: p2p[base_p2p + (off.a >> 32)] = pr; break;
+        for (int w = 0; w < wib; ++w) carry += warp_total[w];
+#pragma unroll
+        for (int r = 0; r < GEN_ITEMS; ++r) {
+            td3_i64x2 c = action_counts(act[r]);
+            td3_i64x2 inc = warp_inclusive_x2(c, lane);
+            td3_i64x2 off = carry + inc - c;
+            long long ta = __shfl_sync(0xffffffffu, (long long)inc.a, 31);
+            long long tb = __shfl_sync(0xffffffffu, (long long)inc.b, 31);
+            carry += td3_i64x2(ta, tb);
+            if (act[r] == ACT_NONE) continue;
+            FPair pr = frontier[first + r * 32 + lane];
+            switch (act[r]) {
+                case ACT_M2L: m2l[base_m2l + (off.a & 0xffffffffLL)] = Pair{pr.a, pr.b}; break;
+                case ACT_P2P: p2p[base_p2p + (off.a >> 32)] = Pair{pr.a, pr.b}; break;
                 case ACT_SELF: {
-                    i64 first = t_child[pr.a], j = off.b;
-                    for (int c = 0; c < 4; ++c)
-                        for (int d = c; d < 4; ++d) next[j++] = Pair{first + c, first + d};
+                    int f = t_rec[pr.a].child;
+                    i64 j = off.b;
+                    for (int c1 = 0; c1 < 4; ++c1)
+                        for (int d = c1; d < 4; ++d) next[j++] = FPair{f + c1, f + d};
                     break;
                 }
                 case ACT_SPLIT_A: {
-                    i64 first = t_child[pr.a];
-                    for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{first + c, pr.b};
+                    int f = t_rec[pr.a].child;
+                    for (int c1 = 0; c1 < 4; ++c1) next[off.b + c1] = FPair{f + c1, pr.b};
                     break;
                 }
                 default: {
-                    i64 first = (DUAL ? s_child : t_child)[pr.b];
-                    for (int c = 0; c < 4; ++c) next[off.b + c] = Pair{pr.a, first + c};
+                    int f = (DUAL ? s_rec : t_rec)[pr.b].child;
+                    for (int c1 = 0; c1 < 4; ++c1) next[off.b + c1] = FPair{pr.a, f + c1};
                     break;
                 }
             }
@@ -257,32 +283,42 @@ k_gen_emit(const Pair* __restrict__ frontier, const TravState* st,
 }
 
 struct TraverseBuffers {
-    Pair* frontier[2];
+    FPair* frontier[2];
     signed char* action;
     td3_i64x2* tile_sum;
     TravState* state;
+    NodeRec* rec[2];  // target (and source) tree records
 };
 
 i64 gen_tiles(i64 frontier_cap) { return (frontier_cap + GEN_TILE - 1) / GEN_TILE; }
 
-size_t traverse_workspace(i64 frontier_cap) {
-    return 2 * td3_ws_bytes<Pair>(frontier_cap) + td3_ws_bytes<signed char>(frontier_cap) +
-           td3_ws_bytes<td3_i64x2>(gen_tiles(frontier_cap)) + td3_ws_bytes<TravState>(1) + 256;
+size_t traverse_workspace(i64 frontier_cap, i64 n_records) {
+    return 2 * td3_ws_bytes<FPair>(frontier_cap) + td3_ws_bytes<signed char>(frontier_cap) +
+           td3_ws_bytes<td3_i64x2>(gen_tiles(frontier_cap)) + td3_ws_bytes<TravState>(1) +
+           td3_ws_bytes<NodeRec>(n_records) + 512;
 }
 
-bool take_traverse(Workspace& w, i64 frontier_cap, TraverseBuffers& b) {
-    b.frontier[0] = w.take<Pair>(frontier_cap);
-    b.frontier[1] = w.take<Pair>(frontier_cap);
+bool take_traverse(Workspace& w, i64 frontier_cap, i64 n_t, i64 n_s, TraverseBuffers& b) {
+    b.frontier[0] = w.take<FPair>(frontier_cap);
+    b.frontier[1] = w.take<FPair>(frontier_cap);
     b.action = w.take<signed char>(frontier_cap);
     b.tile_sum = w.take<td3_i64x2>(gen_tiles(frontier_cap));
     b.state = w.take<TravState>(1);
-    return b.state != nullptr;
+    b.rec[0] = w.take<NodeRec>(n_t);
+    b.rec[1] = n_s ? w.take<NodeRec>(n_s) : b.rec[0];
+    return b.rec[1] != nullptr;
+}
+
+void launch_records(i64 count, const double* center, const double* half, const i64* start,
+                    const i64* end, const i64* child, NodeRec* rec, cudaStream_t stream) {
+    k_node_records<<<td3_blocks(count, 256), 256, 0, stream>>>(count, center, half, start, end,
+                                                               child, rec);
 }
 
 // The generations from (root, root) until the frontier is empty; sizes as the entry
 // points document them.
 template <bool DUAL>
-int run_generations(const TreeView& t, const TreeView& s, double theta, Pair* m2l,
+int run_generations(const NodeRec* t, const NodeRec* s, double theta, Pair* m2l,
                     i64 m2l_capacity, Pair* p2p, i64 p2p_capacity, i64 frontier_capacity,
                     int64_t* sizes, const TraverseBuffers& b, cudaStream_t stream) {
     i64 tiles = gen_tiles(frontier_capacity);
@@ -299,7 +335,7 @@ int run_generations(const TreeView& t, const TreeView& s, double theta, Pair* m2
                                                             m2l_capacity, p2p_capacity,
                                                             frontier_capacity);
             k_gen_emit<DUAL><<<grid, TRAV_THREADS, 0, stream>>>(
-                b.frontier[parity], b.state, b.action, b.tile_sum, t.child, s.child, m2l, p2p,
+                b.frontier[parity], b.state, b.action, b.tile_sum, t, s, m2l, p2p,
                 b.frontier[parity ^ 1]);
             TD3_CHECK_LAUNCH();
         }
@@ -372,43 +408,48 @@ int bits_for(i64 v) {
 
 }  // namespace
 
-extern "C" size_t td3_fmm_traverse_workspace_size(int64_t frontier_capacity) {
-    return traverse_workspace(frontier_capacity);
+extern "C" size_t td3_fmm_traverse_workspace_size(int64_t frontier_capacity, int64_t n_nodes) {
+    return traverse_workspace(frontier_capacity, n_nodes);
 }
 
 extern "C" int td3_fmm_traverse(const double* node_center, const double* node_half,
                                 const int64_t* node_start, const int64_t* node_end,
-                                const int64_t* node_child, double theta, int64_t* m2l,
-                                int64_t m2l_capacity, int64_t* p2p, int64_t p2p_capacity,
-                                int64_t frontier_capacity, int64_t* sizes, void* workspace,
-                                size_t workspace_bytes, void* stream) {
+                                const int64_t* node_child, int64_t n_nodes, double theta,
+                                int64_t* m2l, int64_t m2l_capacity, int64_t* p2p,
+                                int64_t p2p_capacity, int64_t frontier_capacity, int64_t* sizes,
+                                void* workspace, size_t workspace_bytes, void* stream) {
     if (frontier_capacity < 1 || m2l_capacity < 0 || p2p_capacity < 0) return TD3_EINVAL;
+    if (n_nodes < 1 || n_nodes > 0x7fffffffLL) return TD3_EINVAL;
     Workspace w(workspace, workspace_bytes);
     TraverseBuffers b;
-    if (!take_traverse(w, frontier_capacity, b)) return TD3_EWORKSPACE;
-    TreeView t{node_center, node_half, node_start, node_end, node_child};
-    return run_generations<false>(t, t, theta, reinterpret_cast<Pair*>(m2l), m2l_capacity,
-                                  reinterpret_cast<Pair*>(p2p), p2p_capacity, frontier_capacity,
-                                  sizes, b, td3_stream(stream));
+    if (!take_traverse(w, frontier_capacity, n_nodes, 0, b)) return TD3_EWORKSPACE;
+    cudaStream_t s = td3_stream(stream);
+    launch_records(n_nodes, node_center, node_half, node_start, node_end, node_child, b.rec[0], s);
+    return run_generations<false>(b.rec[0], b.rec[0], theta, reinterpret_cast<Pair*>(m2l),
+                                  m2l_capacity, reinterpret_cast<Pair*>(p2p), p2p_capacity,
+                                  frontier_capacity, sizes, b, s);
 }
 
 extern "C" int td3_dual_traverse(const double* t_center, const double* t_half,
                                  const int64_t* t_start, const int64_t* t_end,
-                                 const int64_t* t_child, const double* s_center,
+                                 const int64_t* t_child, int64_t t_nodes, const double* s_center,
                                  const double* s_half, const int64_t* s_start,
-                                 const int64_t* s_end, const int64_t* s_child, double theta,
-                                 int64_t* m2l, int64_t m2l_capacity, int64_t* p2p,
+                                 const int64_t* s_end, const int64_t* s_child, int64_t s_nodes,
+                                 double theta, int64_t* m2l, int64_t m2l_capacity, int64_t* p2p,
                                  int64_t p2p_capacity, int64_t frontier_capacity, int64_t* sizes,
                                  void* workspace, size_t workspace_bytes, void* stream) {
     if (frontier_capacity < 1 || m2l_capacity < 0 || p2p_capacity < 0) return TD3_EINVAL;
+    if (t_nodes < 1 || s_nodes < 1 || t_nodes > 0x7fffffffLL || s_nodes > 0x7fffffffLL)
+        return TD3_EINVAL;
     Workspace w(workspace, workspace_bytes);
     TraverseBuffers b;
-    if (!take_traverse(w, frontier_capacity, b)) return TD3_EWORKSPACE;
-    TreeView t{t_center, t_half, t_start, t_end, t_child};
-    TreeView s{s_center, s_half, s_start, s_end, s_child};
-    return run_generations<true>(t, s, theta, reinterpret_cast<Pair*>(m2l), m2l_capacity,
-                                 reinterpret_cast<Pair*>(p2p), p2p_capacity, frontier_capacity,
-                                 sizes, b, td3_stream(stream));
+    if (!take_traverse(w, frontier_capacity, t_nodes, s_nodes, b)) return TD3_EWORKSPACE;
+    cudaStream_t s = td3_stream(stream);
+    launch_records(t_nodes, t_center, t_half, t_start, t_end, t_child, b.rec[0], s);
+    launch_records(s_nodes, s_center, s_half, s_start, s_end, s_child, b.rec[1], s);
+    return run_generations<true>(b.rec[0], b.rec[1], theta, reinterpret_cast<Pair*>(m2l),
+                                 m2l_capacity, reinterpret_cast<Pair*>(p2p), p2p_capacity,
+                                 frontier_capacity, sizes, b, s);
 }
 
 extern "C" size_t td3_pair_csr_workspace_size(int64_t count, int mutual, int64_t n_nodes) {

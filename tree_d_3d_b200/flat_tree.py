@@ -529,11 +529,13 @@ class FlatQuadtree:
         while True:
             m2l = torch.empty((int(capacity[0]), 2), dtype=torch.int64, device=dev)
             p2p = torch.empty((int(capacity[1]), 2), dtype=torch.int64, device=dev)
-            ws = _lib.workspace(_lib.query("td3_fmm_traverse_workspace_size", int(capacity[2])), dev)
+            ws = _lib.workspace(_lib.query("td3_fmm_traverse_workspace_size", int(capacity[2]),
+                                           self.node_count), dev)
             rc = _lib.call(
                 "td3_fmm_traverse", self.node_center.data_ptr(), self.node_half.data_ptr(),
                 self.node_start.data_ptr(), self.node_end.data_ptr(), self.node_child.data_ptr(),
-                float(theta), m2l.data_ptr(), int(capacity[0]), p2p.data_ptr(), int(capacity[1]),
+                self.node_count, float(theta), m2l.data_ptr(), int(capacity[0]), p2p.data_ptr(),
+                int(capacity[1]),
                 int(capacity[2]), sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
             if rc == _lib.OK:
                 return m2l[: sizes[0]], p2p[: sizes[1]]
@@ -816,12 +818,14 @@ class FlatQuadtree:
         while True:
             m2l = torch.empty((int(capacity[0]), 2), dtype=torch.int64, device=dev)
             p2p = torch.empty((int(capacity[1]), 2), dtype=torch.int64, device=dev)
-            ws = _lib.workspace(_lib.query("td3_fmm_traverse_workspace_size", int(capacity[2])), dev)
+            ws = _lib.workspace(_lib.query("td3_fmm_traverse_workspace_size", int(capacity[2]),
+                                           tree.node_count + self.node_count), dev)
             rc = _lib.call(
                 "td3_dual_traverse", tree.node_center.data_ptr(), tree.node_half.data_ptr(),
                 tree.node_start.data_ptr(), tree.node_end.data_ptr(), tree.node_child.data_ptr(),
-                self.node_center.data_ptr(), self.node_half.data_ptr(), self.node_start.data_ptr(),
-                self.node_end.data_ptr(), self.node_child.data_ptr(), float(theta),
+                tree.node_count, self.node_center.data_ptr(), self.node_half.data_ptr(),
+                self.node_start.data_ptr(), self.node_end.data_ptr(), self.node_child.data_ptr(),
+                self.node_count, float(theta),
                 m2l.data_ptr(), int(capacity[0]), p2p.data_ptr(), int(capacity[1]),
                 int(capacity[2]), sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
             if rc == _lib.OK:
