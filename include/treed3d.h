@@ -444,6 +444,43 @@ int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_c
                     const double* efield, double softening, int mixed, double unit,
                     double* qbar, double* xbar, void* stream);
 
+/* ------------------------------------------------------------------ grounded strip */
+
+/* The conformal map zeta = exp(i pi (x + i y) / width) of the strip 0 < x < width
+ * (src/tree_d_3d/strip.py:147-163, GroundedStripField.to_plane / _sources).  pos
+ * (2, n).  With charge (n) given: sources (2, 2n) receive the n mapped charges then
+ * their images conj(zeta), source_charge (2n) receives q then -q; without: sources
+ * (2, n) receive the mapped points.  A point not strictly between the plates reports
+ * 1 + its index in status (the caller raises the reference's ValueError). */
+int td3_strip_map(const double* pos, int64_t n, double width, const double* charge,
+                  double* sources, double* source_charge, int64_t* status, void* stream);
+
+/* Field and potential in the strip from the mapped-plane sums (strip.py:228-246 and
+ * :289-293): zeta (2, m) with row stride zeta_stride, phi_raw (m) and field_raw (2, m)
+ * with row stride field_stride (raw E_x - i E_y = 2 W'(zeta)).  E_x - i E_y = raw (i pi /
+ * width) zeta; with charge (m) given (the charges themselves) plus the own regular term
+ * 2 q (i pi / 2 width) and phi = phi_raw - 2 q ln(pi |zeta| / width); without (probes)
+ * phi = phi_raw.  phi is 0 when with_potential is 0.  Not yet scaled by k_e. */
+int td3_strip_assemble(const double* zeta, int64_t zeta_stride, int64_t m, double width,
+                       const double* charge, const double* phi_raw, const double* field_raw,
+                       int64_t field_stride, int with_potential, double* phi, double* field,
+                       void* stream);
+
+/* Softening of close pairs in the physical plane, then scaling: for every target
+ * (targets (2, m)) the sources (sources (2, n), charge (n)) within `radius` get the
+ * softened log kernel instead of the bare one, phi += q ln(r^2 / (r^2 + eps^2)) and
+ * E += q (2 / (r^2 + eps^2) - 2 / r^2) d, and then phi, field (2, m) are multiplied by
+ * `scale` (phi set to 0 when with_potential is 0).  same != 0: targets are the sources
+ * (a target skips itself).  A zero separation reports 1 + the target's index in status.
+ * softening = 0 only scales.  Replaces soften_pairs (src/tree_d_3d/kernels/soften_pairs/
+ * soften_pairs_pyccel.py:16-52) over the k-d tree pairs of strip.py:172-201, and the
+ * probe correction of strip.py:296-326. */
+size_t td3_soften_workspace_size(int64_t n);
+int td3_soften(const double* targets, int64_t m, const double* sources, const double* charge,
+               int64_t n, int same, double radius, double softening, int with_potential,
+               double scale, double* phi, double* field, int64_t* status, void* workspace,
+               size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------ utilities */
 
 /* Stable radix sort of (key, value) uint32 pairs by the low `bits` bits of the key.

@@ -375,10 +375,34 @@ def make_energy(ft, Quad):
     return {"pos": pos, "charge": charge, "energy": energy, "status": status}
 
 
+def make_strip():
+    strip = importlib.import_module("tree_d_3d.strip")
+    rng = np.random.default_rng(21)
+    width = 2.0
+    n = 1200
+    pos = np.stack((rng.uniform(0.05, 0.95, n) * width, rng.normal(0, 0.6, n)))
+    charge = np.where(rng.random(n) < 0.5, -1.0, 1.0) * rng.uniform(0.5, 1.5, n)
+    points = np.stack((rng.uniform(0.02, 0.98, 400) * width, rng.normal(0, 0.8, 400)))
+    out = {"pos": pos, "charge": charge, "points": points, "width": np.asarray(width)}
+    for method in ("fmm", "direct"):
+        for eps in (0.0, 0.02):
+            field = strip.GroundedStripField(width, method=method, softening=eps)
+            key = f"{method}/eps{eps}"
+            out[f"{key}/phi"], out[f"{key}/field"] = field.field_at_charges(pos, charge)
+            _, out[f"{key}/field_nopot"] = field.field_at_charges(pos, charge, potential=False)
+            out[f"{key}/probe_phi"], out[f"{key}/probe_field"] = field.probe(pos, charge, points)
+    # a lone charge: the image force of the plates
+    lone = strip.GroundedStripField(2.5, k_e=1.0)
+    out["lone/phi"], out["lone/field"] = lone.field_at_charges(np.array([[0.7], [0.3]]),
+                                                               np.array([1.5]))
+    return out
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--reference", default="/root/reference/src")
     parser.add_argument("--python", action="store_true", help="plain Python kernels")
+    parser.add_argument("--only", nargs="*", help="the fixture groups to write (default all)")
     args = parser.parse_args()
     install_stubs(Path(args.reference), use_numba=not args.python)
     ft = importlib.import_module("tree_d_3d.flat_tree")
@@ -393,8 +417,11 @@ def main() -> None:
         "fmm_at": lambda: make_fmm_at(ft, Quad),
         "tables": make_tables,
         "energy": lambda: make_energy(ft, Quad),
+        "strip": make_strip,
     }
     for name, make in groups.items():
+        if args.only and name not in args.only:
+            continue
         data = make()
         np.savez_compressed(HERE / f"{name}.npz", **data)
         size = (HERE / f"{name}.npz").stat().st_size

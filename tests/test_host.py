@@ -121,3 +121,19 @@ def test_synthetic_distributions():
     a = synthetic.mixture8(1000, seed=9)[0]
     b = synthetic.mixture8(1000, seed=9)[0]
     np.testing.assert_array_equal(a, b)
+
+
+def test_strip_arguments_are_checked_like_the_reference():
+    from tree_d_3d_b200.strip import GroundedStripField
+
+    for width in (0.0, -1.0, float("inf")):
+        with pytest.raises(ValueError, match="width must be finite and positive"):
+            GroundedStripField(width)
+    with pytest.raises(ValueError, match="method must be"):
+        GroundedStripField(1.0, method="walk")
+    with pytest.raises(ValueError, match="softening must be finite and nonnegative"):
+        GroundedStripField(1.0, softening=-1.0)
+    with pytest.raises(ValueError, match="cutoff must exceed 1"):
+        GroundedStripField(1.0, cutoff=1.0)
+    strip = GroundedStripField(2.0)
+    assert (strip.order, strip.theta, strip.leaf_capacity, strip.cutoff) == (14, 0.5, 32, 6.0)

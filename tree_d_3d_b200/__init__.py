@@ -16,6 +16,7 @@ from tree_d_3d_b200.flat_tree import (
     direct_field,
 )
 from tree_d_3d_b200.quad import Quad
+from tree_d_3d_b200.strip import GroundedStripField
 
 __version__ = "0.1.0"
 
@@ -26,6 +27,7 @@ __all__ = [
     "MAX_ORDER",
     "FlatNode",
     "FlatQuadtree",
+    "GroundedStripField",
     "Quad",
     "direct_field",
 ]
