@@ -39,6 +39,34 @@ static inline unsigned td3_blocks(i64 n, int threads) {
     return (unsigned)(b < 1 ? 1 : b);
 }
 
+// Programmatic dependent launch for chains of short dependent kernels (a level or a
+// traversal generation at a time): the launch may start while the previous kernel on
+// the stream still runs; the kernel's first statement is td3_chain_wait(), which
+// returns once every earlier kernel of the stream has finished and its memory writes
+// are visible (hardware-tracked, griddepcontrol.wait), and td3_chain_release() lets the
+// next kernel of the chain start launching.
+__device__ __forceinline__ void td3_chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void td3_chain_release() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... Params, typename... Args>
+static inline cudaError_t td3_launch_chained(void (*kernel)(Params...), unsigned grid,
+                                             unsigned block, size_t smem, cudaStream_t s,
+                                             Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<Params>(args)...);
+}
+
 // Carves aligned sub-buffers out of a caller-provided workspace.
 struct Workspace {
     char* base;

@@ -126,6 +126,8 @@ __global__ void k_l2l_log_level(i64 lo, i64 hi, int order, const double* __restr
                                 const i64* __restrict__ end, const double* __restrict__ binomial,
                                 int bsize, double* __restrict__ local_re,
                                 double* __restrict__ local_im) {
+    td3_chain_wait();
+    td3_chain_release();
     int w = order + 1;
     i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     i64 ch = lo + t / w;
@@ -394,9 +396,9 @@ extern "C" int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const d
         i64 lo = levels[level], hi = levels[level + 1];
         if (hi <= lo) continue;
         i64 threads = (hi - lo) * w;
-        k_l2l_log_level<<<td3_blocks(threads, 256), 256, 0, s>>>(
-            lo, hi, order, node_center, node_parent, node_start, node_end, binomial, binomial_size,
-            local_re, local_im);
+        TD3_TRY(td3_launch_chained(k_l2l_log_level, td3_blocks(threads, 256), 256, 0, s, lo, hi,
+                                   order, node_center, node_parent, node_start, node_end,
+                                   binomial, binomial_size, local_re, local_im));
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;

@@ -210,6 +210,8 @@ k_log_m2m_level(i64 lo, i64 hi, int order, const double* __restrict__ node_cente
     constexpr int W = P + 1;
     __shared__ double2 shifted[M2M_NODES][4][W];
     __shared__ int present[M2M_NODES][4];
+    td3_chain_wait();
+    td3_chain_release();
     int w = order + 1;
     int local = threadIdx.x >> 2, c = threadIdx.x & 3;
     i64 node = lo + (i64)blockIdx.x * M2M_NODES + local;
@@ -295,8 +297,8 @@ int launch_log_moments(const int64_t* levels, int64_t n_levels, int order, const
     k_log_leaf_moments<P><<<nb, MOM_THREADS, 0, s>>>(count, order, spos, scharge, n, center, \
                                                      start, end, child, qabs, mre, mim, sdip)
 #define TD3_M2M(P)                                                                           \
-    k_log_m2m_level<P><<<nb, M2M_NODES * 4, 0, s>>>(lo, hi, order, center, start, end, child, \
-                                                    binomial, bsize, qabs, mre, mim)
+    TD3_TRY(td3_launch_chained(k_log_m2m_level<P>, nb, M2M_NODES * 4, 0, s, lo, hi, order,    \
+                               center, start, end, child, binomial, bsize, qabs, mre, mim))
         if (order <= 4)
             TD3_LEAF_MOMENTS(4);
         else if (order <= 8)

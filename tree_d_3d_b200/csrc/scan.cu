@@ -54,6 +54,8 @@ __device__ __forceinline__ T block_exclusive(T v, T* total) {
 
 template <typename T>
 __global__ void k_tile_reduce(const T* __restrict__ in, i64 n, T* __restrict__ partial) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 base = (i64)blockIdx.x * SCAN_TILE;
     T s = 0;
 #pragma unroll
@@ -69,6 +71,8 @@ __global__ void k_tile_reduce(const T* __restrict__ in, i64 n, T* __restrict__ p
 // One block scans the partials in place (exclusive), carrying across chunks.
 template <typename T>
 __global__ void k_partials_scan(T* partial, i64 m, T* total_out) {
+    td3_chain_wait();
+    td3_chain_release();
     T carry = 0;
     for (i64 base = 0; base < m; base += blockDim.x) {
         i64 k = base + threadIdx.x;
@@ -84,6 +88,8 @@ __global__ void k_partials_scan(T* partial, i64 m, T* total_out) {
 template <typename T>
 __global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, i64 n,
                             const T* __restrict__ partial) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 base = (i64)blockIdx.x * SCAN_TILE + (i64)threadIdx.x * SCAN_ITEMS;
     T v[SCAN_ITEMS];
     T s = 0;
@@ -107,6 +113,8 @@ __global__ void k_tile_scan(const T* __restrict__ in, T* __restrict__ out, i64 n
 template <typename T>
 __global__ void k_single_tile_scan(const T* __restrict__ in, T* __restrict__ out, i64 n,
                                    T* __restrict__ total_out) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 base = (i64)threadIdx.x * SCAN_ITEMS;
     T v[SCAN_ITEMS];
     T s = 0;
@@ -135,17 +143,18 @@ int exclusive_scan(const T* in, T* out, i64 n, T* total, void* ws, size_t ws_byt
         return TD3_OK;
     }
     if (n <= SCAN_TILE) {
-        k_single_tile_scan<T><<<1, SCAN_THREADS, 0, stream>>>(in, out, n, total);
-        TD3_CHECK_LAUNCH();
+        TD3_TRY(td3_launch_chained(k_single_tile_scan<T>, 1, SCAN_THREADS, 0, stream, in, out, n,
+                                   total));
         return TD3_OK;
     }
     i64 tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     if ((size_t)tiles * sizeof(T) > ws_bytes) return TD3_EWORKSPACE;
     T* partial = static_cast<T*>(ws);
-    k_tile_reduce<T><<<(unsigned)tiles, SCAN_THREADS, 0, stream>>>(in, n, partial);
-    k_partials_scan<T><<<1, 1024, 0, stream>>>(partial, tiles, total);
-    k_tile_scan<T><<<(unsigned)tiles, SCAN_THREADS, 0, stream>>>(in, out, n, partial);
-    TD3_CHECK_LAUNCH();
+    TD3_TRY(td3_launch_chained(k_tile_reduce<T>, (unsigned)tiles, SCAN_THREADS, 0, stream, in, n,
+                               partial));
+    TD3_TRY(td3_launch_chained(k_partials_scan<T>, 1, 1024, 0, stream, partial, tiles, total));
+    TD3_TRY(td3_launch_chained(k_tile_scan<T>, (unsigned)tiles, SCAN_THREADS, 0, stream, in, out,
+                               n, (const T*)partial));
     return TD3_OK;
 }
 
@@ -175,6 +184,8 @@ __global__ void __launch_bounds__(SORT_THREADS)
 k_sort_hist(const unsigned* __restrict__ keys, i64 n, int shift, unsigned mask, int n_tiles,
             int* __restrict__ hist) {
     __shared__ int counts[SORT_WARPS][RADIX];
+    td3_chain_wait();
+    td3_chain_release();
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&counts[0][0])[i] = 0;
     __syncthreads();
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -203,6 +214,8 @@ k_sort_scatter(const unsigned* __restrict__ keys, const unsigned* __restrict__ v
     __shared__ int wcount[SORT_WARPS][RADIX];
     __shared__ int tstart[RADIX];
     __shared__ int goff[RADIX];
+    td3_chain_wait();
+    td3_chain_release();
     for (int i = threadIdx.x; i < SORT_WARPS * RADIX; i += SORT_THREADS) (&wcount[0][0])[i] = 0;
     __syncthreads();
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -280,10 +293,12 @@ int radix_sort(unsigned* keys, unsigned* keys_alt, unsigned* vals, unsigned* val
     for (int shift = 0; shift < bits; shift += RADIX_BITS) {
         int digit_bits = bits - shift < RADIX_BITS ? bits - shift : RADIX_BITS;
         unsigned mask = (1u << digit_bits) - 1u;
-        k_sort_hist<<<n_tiles, SORT_THREADS, 0, stream>>>(src_k, n, shift, mask, n_tiles, hist);
+        TD3_TRY(td3_launch_chained(k_sort_hist, n_tiles, SORT_THREADS, 0, stream,
+                                   (const unsigned*)src_k, n, shift, mask, n_tiles, hist));
         TD3_TRY_RC(td3_exclusive_scan_i32(hist, hist, n_hist, nullptr, scan_ws, scan_bytes, stream));
-        k_sort_scatter<<<n_tiles, SORT_THREADS, 0, stream>>>(src_k, src_v, dst_k, dst_v, n, shift,
-                                                             mask, n_tiles, hist);
+        TD3_TRY(td3_launch_chained(k_sort_scatter, n_tiles, SORT_THREADS, 0, stream,
+                                   (const unsigned*)src_k, (const unsigned*)src_v, dst_k, dst_v,
+                                   n, shift, mask, n_tiles, (const int*)hist));
         TD3_CHECK_LAUNCH();
         unsigned* tk = src_k;
         src_k = dst_k;

@@ -163,6 +163,8 @@ k_gen_classify(const FPair* __restrict__ frontier, const TravState* st, int pari
                const NodeRec* __restrict__ t, const NodeRec* __restrict__ s, double theta,
                signed char* __restrict__ action,
                td3_i64x2* __restrict__ tile_sum) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 nf = st->nf[parity];
     i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
     for (i64 tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
@@ -185,6 +187,8 @@ k_gen_classify(const FPair* __restrict__ frontier, const TravState* st, int pari
 __global__ void __launch_bounds__(GEN_SCAN_THREADS)
 k_gen_scan(TravState* st, int parity, td3_i64x2* __restrict__ tile_sum, i64 m2l_capacity,
            i64 p2p_capacity, i64 frontier_capacity) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 nf = st->nf[parity];
     i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
     td3_i64x2 carry(0);
@@ -227,6 +231,8 @@ k_gen_emit(const FPair* __restrict__ frontier, const TravState* st,
            const NodeRec* __restrict__ t_rec, const NodeRec* __restrict__ s_rec,
            Pair* __restrict__ m2l, Pair* __restrict__ p2p, FPair* __restrict__ next) {
     __shared__ td3_i64x2 warp_total[TRAV_THREADS / 32];
+    td3_chain_wait();
+    td3_chain_release();
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     i64 nf = st->emit_nf;
     i64 base_m2l = st->base_m2l, base_p2p = st->base_p2p;
@@ -329,14 +335,17 @@ int run_generations(const NodeRec* t, const NodeRec* s, double theta, Pair* m2l,
     for (int gen = 0;;) {
         for (int k = 0; k < GEN_BATCH; ++k, ++gen) {
             int parity = gen & 1;
-            k_gen_classify<DUAL><<<grid, TRAV_THREADS, 0, stream>>>(
-                b.frontier[parity], b.state, parity, t, s, theta, b.action, b.tile_sum);
-            k_gen_scan<<<1, GEN_SCAN_THREADS, 0, stream>>>(b.state, parity, b.tile_sum,
-                                                            m2l_capacity, p2p_capacity,
-                                                            frontier_capacity);
-            k_gen_emit<DUAL><<<grid, TRAV_THREADS, 0, stream>>>(
-                b.frontier[parity], b.state, b.action, b.tile_sum, t, s, m2l, p2p,
-                b.frontier[parity ^ 1]);
+            TD3_TRY(td3_launch_chained(k_gen_classify<DUAL>, grid, TRAV_THREADS, 0, stream,
+                                       (const FPair*)b.frontier[parity], (const TravState*)b.state,
+                                       parity, t, s, theta, b.action, b.tile_sum));
+            TD3_TRY(td3_launch_chained(k_gen_scan, 1, GEN_SCAN_THREADS, 0, stream, b.state, parity,
+                                       b.tile_sum, m2l_capacity, p2p_capacity,
+                                       frontier_capacity));
+            TD3_TRY(td3_launch_chained(k_gen_emit<DUAL>, grid, TRAV_THREADS, 0, stream,
+                                       (const FPair*)b.frontier[parity], (const TravState*)b.state,
+                                       (const signed char*)b.action,
+                                       (const td3_i64x2*)b.tile_sum, t, s, m2l, p2p,
+                                       b.frontier[parity ^ 1]));
             TD3_CHECK_LAUNCH();
         }
         TravState h;
