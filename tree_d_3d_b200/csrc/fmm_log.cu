@@ -167,6 +167,8 @@ __global__ void k_node_parents(i64 count, const i64* __restrict__ node_child,
 __global__ void k_scale_moments(i64 count, int order, const double* __restrict__ mre,
                                 const double* __restrict__ mim, const double* __restrict__ half,
                                 float2* __restrict__ hat) {
+    td3_chain_wait();
+    td3_chain_release();
     int w = order + 1, hw = td3_hat_width(order);
     i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= count * hw) return;
@@ -202,6 +204,8 @@ k_m2l_mixed(const i64* __restrict__ row_start, const int* __restrict__ entry_row
             const double* __restrict__ src_half, const float2* __restrict__ hat, int order,
             const CoefTable<P> C, double unit, double* __restrict__ local_re,
             double* __restrict__ local_im) {
+    td3_chain_wait();
+    td3_chain_release();
     constexpr int W = P + 1, V = 2 * W + 2;
     __shared__ float carry[M2L_WARPS][V];
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -287,9 +291,9 @@ int launch_m2l_mixed(const i64* row_start, const int* entry_row, const i64* part
     for (int k = 0; k <= P; ++k)
         for (int l = 0; l <= P; ++l)
             C.c[k * (P + 1) + l] = (k < w && l < w) ? (float)coeff[k * w + l] : 0.0f;
-    k_m2l_mixed<P><<<148 * 16, 32 * M2L_WARPS, 0, s>>>(row_start, entry_row, partners, n_dst,
-                                                       dst_center, dst_half, src_center, src_half,
-                                                       hat, order, C, unit, lre, lim);
+    TD3_TRY(td3_launch_chained(k_m2l_mixed<P>, 148 * 16, 32 * M2L_WARPS, 0, s, row_start,
+                               entry_row, partners, n_dst, dst_center, dst_half, src_center,
+                               src_half, hat, order, C, unit, lre, lim));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
@@ -336,8 +340,9 @@ extern "C" int td3_scale_moments(int64_t count, int order, const double* moment_
     if (count < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
     if (count == 0) return TD3_OK;
     i64 threads = count * td3_hat_width(order);
-    k_scale_moments<<<td3_blocks(threads, 256), 256, 0, td3_stream(stream)>>>(
-        count, order, moment_re, moment_im, node_half, reinterpret_cast<float2*>(hat));
+    TD3_TRY(td3_launch_chained(k_scale_moments, td3_blocks(threads, 256), 256, 0,
+                               td3_stream(stream), count, order, moment_re, moment_im, node_half,
+                               reinterpret_cast<float2*>(hat)));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }

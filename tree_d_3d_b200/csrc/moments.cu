@@ -149,6 +149,8 @@ __global__ void k_log_leaf_moments(i64 count, int order, const double* __restric
                                    const i64* __restrict__ node_child, double* node_qabs,
                                    double* moment_re, double* moment_im,
                                    const double* __restrict__ sdip) {
+    td3_chain_wait();
+    td3_chain_release();
     constexpr int W = P + 1;
     i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (node >= count || node_child[node] >= 0) return;
@@ -294,8 +296,8 @@ int launch_log_moments(const int64_t* levels, int64_t n_levels, int order, const
     if (order <= 15) {
         unsigned nb = td3_blocks(count, MOM_THREADS);
 #define TD3_LEAF_MOMENTS(P)                                                                  \
-    k_log_leaf_moments<P><<<nb, MOM_THREADS, 0, s>>>(count, order, spos, scharge, n, center, \
-                                                     start, end, child, qabs, mre, mim, sdip)
+    TD3_TRY(td3_launch_chained(k_log_leaf_moments<P>, nb, MOM_THREADS, 0, s, count, order, spos, \
+                               scharge, n, center, start, end, child, qabs, mre, mim, sdip))
 #define TD3_M2M(P)                                                                           \
     TD3_TRY(td3_launch_chained(k_log_m2m_level<P>, nb, M2M_NODES * 4, 0, s, lo, hi, order,    \
                                center, start, end, child, binomial, bsize, qabs, mre, mim))

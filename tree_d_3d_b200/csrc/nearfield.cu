@@ -29,6 +29,8 @@ __device__ __forceinline__ int pow2_at_least(int v) {
 __global__ void k_plan_count(i64 n_nodes, const i64* __restrict__ rows, const i64* __restrict__ child,
                              const i64* __restrict__ start, const i64* __restrict__ end, int segment,
                              i64* __restrict__ nseg, i64* __restrict__ psize) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n_nodes) return;
     i64 count = end[n] - start[n];
@@ -46,6 +48,8 @@ __global__ void k_plan_fill(i64 n_nodes, const i64* __restrict__ rows, const i64
                             const i64* __restrict__ nseg_scan, const i64* __restrict__ psize_scan,
                             const i64* __restrict__ nseg, int* __restrict__ seg_leaf,
                             longlong2* __restrict__ seg_range, i64* __restrict__ seg_out) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 n = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= n_nodes) return;
     i64 s = nseg[n];
@@ -305,6 +309,8 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
        const double* __restrict__ local_b, int order, int width, double eps2,
        double* __restrict__ partial, double* __restrict__ phi, double* __restrict__ field,
        i64* status) {
+    td3_chain_wait();
+    td3_chain_release();
     __shared__ NearWindow windows[NF_WARPS];
     int lane = threadIdx.x & 31;
     NearWindow& win = windows[threadIdx.x >> 5];
@@ -437,6 +443,8 @@ __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_
                               const double* __restrict__ local_b, int order, int width,
                               const double* __restrict__ partial, double* __restrict__ phi,
                               double* __restrict__ field) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (seg >= n_seg) return;
@@ -607,6 +615,8 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
                const double* __restrict__ fb, const double* __restrict__ ba,
                const double* __restrict__ bb, int order, int width, double eps2,
                double* __restrict__ partial) {
+    td3_chain_wait();
+    td3_chain_release();
     __shared__ AdjointWindow<MIXED> windows[NF_WARPS];
     int lane = threadIdx.x & 31;
     AdjointWindow<MIXED>& win = windows[threadIdx.x >> 5];
@@ -714,6 +724,8 @@ __global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg
                                       const double* __restrict__ fb, const double* __restrict__ ba,
                                       const double* __restrict__ bb, int order, int width,
                                       const double* __restrict__ partial) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
     int lane = threadIdx.x & 31;
     if (seg >= n_seg) return;
@@ -763,12 +775,13 @@ template <int KERNEL, bool POT, bool OTHER, int LOCAL, bool MIXED>
 int launch_near(const NearArgs& a, cudaStream_t s) {
     if (a.n_seg == 0) return TD3_OK;
     unsigned blocks = td3_blocks(a.n_seg, NF_WARPS);
-    k_near<KERNEL, POT, OTHER, LOCAL, MIXED><<<blocks, 32 * NF_WARPS, 0, s>>>(
-        a.T, a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out, a.partners, a.la, a.lb, a.order,
-        a.width, a.eps2, a.partial, a.phi, a.field, a.status);
-    k_near_finish<POT, LOCAL><<<blocks, 32 * NF_WARPS, 0, s>>>(a.T, a.n_seg, a.seg_leaf, a.seg_out,
-                                                               a.la, a.lb, a.order, a.width,
-                                                               a.partial, a.phi, a.field);
+    TD3_TRY(td3_launch_chained(k_near<KERNEL, POT, OTHER, LOCAL, MIXED>, blocks, 32 * NF_WARPS, 0,
+                               s, a.T, a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out,
+                               a.partners, a.la, a.lb, a.order, a.width, a.eps2, a.partial, a.phi,
+                               a.field, a.status));
+    TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL>, blocks, 32 * NF_WARPS, 0, s, a.T,
+                               a.n_seg, a.seg_leaf, a.seg_out, a.la, a.lb, a.order, a.width,
+                               a.partial, a.phi, a.field));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
@@ -810,8 +823,8 @@ extern "C" int td3_nearfield_plan(const int64_t* rows, int64_t n_nodes, const in
     i64* psize_scan = w.take<i64>(n_nodes + 1);
     if (!psize_scan) return TD3_EWORKSPACE;
     unsigned nb = td3_blocks(n_nodes, 256);
-    k_plan_count<<<nb, 256, 0, s>>>(n_nodes, rows, node_child, node_start, node_end, segment, nseg,
-                                    psize);
+    TD3_TRY(td3_launch_chained(k_plan_count, nb, 256, 0, s, n_nodes, rows, node_child, node_start,
+                               node_end, segment, nseg, psize));
     TD3_CHECK_LAUNCH();
     TD3_TRY(cudaMemsetAsync(nseg + n_nodes, 0, sizeof(i64), s));
     TD3_TRY(cudaMemsetAsync(psize + n_nodes, 0, sizeof(i64), s));
@@ -826,9 +839,9 @@ extern "C" int td3_nearfield_plan(const int64_t* rows, int64_t n_nodes, const in
     sizes[0] = totals[0];
     sizes[1] = totals[1];
     if (totals[0] > seg_capacity) return TD3_ENEEDMORE;
-    k_plan_fill<<<nb, 256, 0, s>>>(n_nodes, rows, node_start, node_end, segment, nseg_scan,
-                                   psize_scan, nseg, seg_leaf, reinterpret_cast<longlong2*>(seg_range),
-                                   seg_out);
+    TD3_TRY(td3_launch_chained(k_plan_fill, nb, 256, 0, s, n_nodes, rows, node_start, node_end,
+                               segment, nseg_scan, psize_scan, nseg, seg_leaf,
+                               reinterpret_cast<longlong2*>(seg_range), seg_out));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
@@ -859,17 +872,19 @@ extern "C" int td3_fmm_evaluate(int kernel, const double* sorted_pos, const doub
 }
 
 template <int KERNEL, int LOCAL, bool MIXED>
-void launch_adjoint(const Targets& T, const Sources& S, const Adjoint& A, i64 n_seg,
-                    const int* seg_leaf, const longlong2* sr, const i64* seg_out,
-                    const i64* partners, const double* fa, const double* fb, const double* ba,
-                    const double* bb, int order, int width, double eps2, double* partial,
-                    cudaStream_t s) {
+int launch_adjoint(const Targets& T, const Sources& S, const Adjoint& A, i64 n_seg,
+                   const int* seg_leaf, const longlong2* sr, const i64* seg_out,
+                   const i64* partners, const double* fa, const double* fb, const double* ba,
+                   const double* bb, int order, int width, double eps2, double* partial,
+                   cudaStream_t s) {
     unsigned blocks = td3_blocks(n_seg, NF_WARPS);
-    k_near_adjoint<KERNEL, LOCAL, MIXED><<<blocks, 32 * NF_WARPS, 0, s>>>(
-        T, S, A, n_seg, seg_leaf, sr, seg_out, partners, fa, fb, ba, bb, order, width, eps2,
-        partial);
-    k_near_adjoint_finish<LOCAL><<<blocks, 32 * NF_WARPS, 0, s>>>(
-        T, S, A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb, order, width, partial);
+    TD3_TRY(td3_launch_chained(k_near_adjoint<KERNEL, LOCAL, MIXED>, blocks, 32 * NF_WARPS, 0, s,
+                               T, S, A, n_seg, seg_leaf, sr, seg_out, partners, fa, fb, ba, bb,
+                               order, width, eps2, partial));
+    TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL>, blocks, 32 * NF_WARPS, 0, s, T, S,
+                               A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb, order, width,
+                               partial));
+    return TD3_OK;
 }
 
 extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_charge,
@@ -895,29 +910,22 @@ extern "C" int td3_fmm_adjoint(int kernel, const double* sorted_pos, const doubl
     if (kernel == TD3_KERNEL_LOG) {
         int width = order + 1;
         if (mixed)
-            launch_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX, true>(T, S, A, n_seg, seg_leaf, sr, seg_out,
-                                                                p2p_partners, fwd_a, fwd_b, adj_a,
-                                                                adj_b, order, width, eps2, partial, s);
-        else
-            launch_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX, false>(T, S, A, n_seg, seg_leaf, sr,
-                                                                 seg_out, p2p_partners, fwd_a, fwd_b,
-                                                                 adj_a, adj_b, order, width, eps2,
-                                                                 partial, s);
+            return launch_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX, true>(
+                T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b,
+                order, width, eps2, partial, s);
+        return launch_adjoint<TD3_KERNEL_LOG, LOCAL_COMPLEX, false>(
+            T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b, order,
+            width, eps2, partial, s);
     } else {
         int width = (order + 1) * (order + 2) / 2;
         if (mixed)
-            launch_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART, true>(T, S, A, n_seg, seg_leaf, sr,
-                                                                 seg_out, p2p_partners, fwd_a, fwd_b,
-                                                                 adj_a, adj_b, order, width, eps2,
-                                                                 partial, s);
-        else
-            launch_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART, false>(T, S, A, n_seg, seg_leaf, sr,
-                                                                  seg_out, p2p_partners, fwd_a, fwd_b,
-                                                                  adj_a, adj_b, order, width, eps2,
-                                                                  partial, s);
+            return launch_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART, true>(
+                T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b,
+                order, width, eps2, partial, s);
+        return launch_adjoint<TD3_KERNEL_COULOMB, LOCAL_CART, false>(
+            T, S, A, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b, order,
+            width, eps2, partial, s);
     }
-    TD3_CHECK_LAUNCH();
-    return TD3_OK;
 }
 
 extern "C" int td3_fmm_targets(int kernel, const double* sorted_targets,

@@ -39,6 +39,8 @@ __global__ void k_node_records(i64 count, const double* __restrict__ center,
                                const double* __restrict__ half, const i64* __restrict__ start,
                                const i64* __restrict__ end, const i64* __restrict__ child,
                                NodeRec* __restrict__ rec) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 i = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     rec[i] = NodeRec{center[2 * i], center[2 * i + 1], half[i], (int)child[i],
@@ -149,6 +151,8 @@ __device__ __forceinline__ td3_i64x2 block_exclusive_x2(td3_i64x2 v, td3_i64x2* 
 }
 
 __global__ void k_gen_init(TravState* st, FPair* frontier) {
+    td3_chain_wait();
+    td3_chain_release();
     st->nf[0] = 1;
     st->nf[1] = 0;
     st->emit_nf = 0;
@@ -315,10 +319,11 @@ bool take_traverse(Workspace& w, i64 frontier_cap, i64 n_t, i64 n_s, TraverseBuf
     return b.rec[1] != nullptr;
 }
 
-void launch_records(i64 count, const double* center, const double* half, const i64* start,
+int launch_records(i64 count, const double* center, const double* half, const i64* start,
                     const i64* end, const i64* child, NodeRec* rec, cudaStream_t stream) {
-    k_node_records<<<td3_blocks(count, 256), 256, 0, stream>>>(count, center, half, start, end,
-                                                               child, rec);
+    TD3_TRY(td3_launch_chained(k_node_records, td3_blocks(count, 256), 256, 0, stream, count,
+                               center, half, start, end, child, rec));
+    return TD3_OK;
 }
 
 // The generations from (root, root) until the frontier is empty; sizes as the entry
@@ -329,7 +334,7 @@ int run_generations(const NodeRec* t, const NodeRec* s, double theta, Pair* m2l,
                     int64_t* sizes, const TraverseBuffers& b, cudaStream_t stream) {
     i64 tiles = gen_tiles(frontier_capacity);
     unsigned grid = (unsigned)(tiles < 148 * 4 ? tiles : 148 * 4);
-    k_gen_init<<<1, 1, 0, stream>>>(b.state, b.frontier[0]);
+    TD3_TRY(td3_launch_chained(k_gen_init, 1, 1, 0, stream, b.state, b.frontier[0]));
     TD3_CHECK_LAUNCH();
     sizes[0] = sizes[1] = sizes[2] = sizes[3] = 0;
     for (int gen = 0;;) {
@@ -369,6 +374,8 @@ int run_generations(const NodeRec* t, const NodeRec* s, double theta, Pair* m2l,
 // ------------------------------------------------------------------ pair CSR
 __global__ void k_csr_keys(const Pair* __restrict__ pairs, i64 count, int mutual, unsigned invalid,
                            unsigned* __restrict__ keys, unsigned* __restrict__ vals) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= count) return;
     Pair pr = pairs[p];
@@ -392,6 +399,8 @@ __global__ void k_csr_keys(const Pair* __restrict__ pairs, i64 count, int mutual
 // n_nodes last): position j sets the rows between its predecessor's key and its own.
 __global__ void k_row_starts(const unsigned* __restrict__ keys, i64 e, i64 n_nodes,
                              i64* __restrict__ row_start) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (j > e) return;
     i64 prev = j == 0 ? -1 : (i64)keys[j - 1];
@@ -403,6 +412,8 @@ __global__ void k_row_starts(const unsigned* __restrict__ keys, i64 e, i64 n_nod
 // partners (int64) and, when asked, the row of every entry (int32)
 __global__ void k_csr_out(const unsigned* __restrict__ vals, const unsigned* __restrict__ keys,
                           i64 count, i64* __restrict__ partners, int* __restrict__ entry_row) {
+    td3_chain_wait();
+    td3_chain_release();
     i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= count) return;
     partners[k] = vals[k];
@@ -433,7 +444,8 @@ extern "C" int td3_fmm_traverse(const double* node_center, const double* node_ha
     TraverseBuffers b;
     if (!take_traverse(w, frontier_capacity, n_nodes, 0, b)) return TD3_EWORKSPACE;
     cudaStream_t s = td3_stream(stream);
-    launch_records(n_nodes, node_center, node_half, node_start, node_end, node_child, b.rec[0], s);
+    TD3_TRY_RC(launch_records(n_nodes, node_center, node_half, node_start, node_end, node_child,
+                              b.rec[0], s));
     return run_generations<false>(b.rec[0], b.rec[0], theta, reinterpret_cast<Pair*>(m2l),
                                   m2l_capacity, reinterpret_cast<Pair*>(p2p), p2p_capacity,
                                   frontier_capacity, sizes, b, s);
@@ -454,8 +466,8 @@ extern "C" int td3_dual_traverse(const double* t_center, const double* t_half,
     TraverseBuffers b;
     if (!take_traverse(w, frontier_capacity, t_nodes, s_nodes, b)) return TD3_EWORKSPACE;
     cudaStream_t s = td3_stream(stream);
-    launch_records(t_nodes, t_center, t_half, t_start, t_end, t_child, b.rec[0], s);
-    launch_records(s_nodes, s_center, s_half, s_start, s_end, s_child, b.rec[1], s);
+    TD3_TRY_RC(launch_records(t_nodes, t_center, t_half, t_start, t_end, t_child, b.rec[0], s));
+    TD3_TRY_RC(launch_records(s_nodes, s_center, s_half, s_start, s_end, s_child, b.rec[1], s));
     return run_generations<true>(b.rec[0], b.rec[1], theta, reinterpret_cast<Pair*>(m2l),
                                  m2l_capacity, reinterpret_cast<Pair*>(p2p), p2p_capacity,
                                  frontier_capacity, sizes, b, s);
@@ -483,17 +495,20 @@ extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int
     unsigned* v0 = w.take<unsigned>(e);
     unsigned* v1 = w.take<unsigned>(e);
     if (!v1) return TD3_EWORKSPACE;
-    k_csr_keys<<<td3_blocks(count, 256), 256, 0, s>>>(reinterpret_cast<const Pair*>(pairs), count,
-                                                      mutual, (unsigned)n_nodes, k0, v0);
+    TD3_TRY(td3_launch_chained(k_csr_keys, td3_blocks(count, 256), 256, 0, s,
+                               reinterpret_cast<const Pair*>(pairs), count, mutual,
+                               (unsigned)n_nodes, k0, v0));
     TD3_CHECK_LAUNCH();
     unsigned *ko, *vo;
     TD3_TRY_RC(td3_radix_sort_u32(k0, k1, v0, v1, e, bits_for(n_nodes), &ko, &vo, w.base + w.used,
                                   w.size - w.used, s));
     // the row offsets from the boundaries between equal keys of the sorted entries
-    k_row_starts<<<td3_blocks(e + 1, 256), 256, 0, s>>>(ko, e, n_nodes, row_start);
+    TD3_TRY(td3_launch_chained(k_row_starts, td3_blocks(e + 1, 256), 256, 0, s, ko, e, n_nodes,
+                               row_start));
     // valid entries sort before the invalid key n_nodes (row_start[n_nodes] of them); the
     // entries after them are widened too (partners holds e slots), so no host read
-    k_csr_out<<<td3_blocks(e, 256), 256, 0, s>>>(vo, ko, e, partners, entry_row);
+    TD3_TRY(td3_launch_chained(k_csr_out, td3_blocks(e, 256), 256, 0, s, vo, ko, e, partners,
+                               entry_row));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }

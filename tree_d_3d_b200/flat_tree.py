@@ -352,26 +352,28 @@ class FlatQuadtree:
         self._fwd_locals = None
         count, dev, f64 = self.node_count, self.device, torch.float64
         n = self.pos.shape[1]
-        self.node_q = torch.empty(count, dtype=f64, device=dev)
-        self.node_qabs = torch.empty(count, dtype=f64, device=dev)
-        self.node_p = torch.empty((count, 2), dtype=f64, device=dev)
-        self.node_s = torch.zeros((count, 3), dtype=f64, device=dev)
         levels = np.ascontiguousarray(self.levels, dtype=np.int64)
         stream = _lib.stream(dev)
         common = (self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(), n,
                   self.node_center.data_ptr(), self.node_start.data_ptr(),
                   self.node_end.data_ptr(), self.node_child.data_ptr())
+        self.node_qabs = torch.empty(count, dtype=f64, device=dev)
         if self.kernel == "log":
+            # the moments launch first (the GPU waits for them after the build's host
+            # read); the derived node arrays follow
             self.moment_re = torch.empty((count, self.order + 1), dtype=f64, device=dev)
             self.moment_im = torch.empty((count, self.order + 1), dtype=f64, device=dev)
             binom = self._binomial()
             _lib.call("td3_log_moments", levels.ctypes.data, len(levels) - 1, self.order, *common,
                       binom.data_ptr(), binom.shape[0], self.node_qabs.data_ptr(),
                       self.moment_re.data_ptr(), self.moment_im.data_ptr(), stream)
-            self.node_q.copy_(self.moment_re[:, 0])
-            self.node_p[:, 0] = self.moment_re[:, 1]
-            self.node_p[:, 1] = self.moment_im[:, 1]
+            self.node_q = self.moment_re[:, 0].clone()
+            self.node_p = torch.stack((self.moment_re[:, 1], self.moment_im[:, 1]), dim=1)
+            self.node_s = torch.zeros((count, 3), dtype=f64, device=dev)
             return
+        self.node_q = torch.empty(count, dtype=f64, device=dev)
+        self.node_p = torch.empty((count, 2), dtype=f64, device=dev)
+        self.node_s = torch.zeros((count, 3), dtype=f64, device=dev)
         self.moment_re = torch.zeros((1, 1), dtype=f64, device=dev)
         self.moment_im = torch.zeros((1, 1), dtype=f64, device=dev)
         _lib.call("td3_quadtree_moments", levels.ctypes.data, len(levels) - 1, *common,
