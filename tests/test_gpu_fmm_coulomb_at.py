@@ -34,7 +34,7 @@ def test_coulomb_fmm_matches_golden(order):
     assert relative(field, data[f"coulomb/p{order}/field"]) < TOL
 
 
-@pytest.mark.parametrize("order,leaf", [(4, 8), (12, 32), (16, 16)])
+@pytest.mark.parametrize("order,leaf", [(4, 8), (12, 32), (16, 16), (18, 16)])
 def test_coulomb_fmm_matches_oracle(oracle, order, leaf):
     from tree_d_3d_b200 import FlatQuadtree, Quad, synthetic
 
