@@ -395,29 +395,26 @@ __global__ void k_csr_keys(const Pair* __restrict__ pairs, i64 count, int mutual
     }
 }
 
-// row_start[d] = the first sorted position with key >= d (keys sorted, the invalid key
-// n_nodes last): position j sets the rows between its predecessor's key and its own.
-__global__ void k_row_starts(const unsigned* __restrict__ keys, i64 e, i64 n_nodes,
-                             i64* __restrict__ row_start) {
+// The CSR from the sorted entries, one thread per position j in [0, e]: partners (int64)
+// and, when asked, the row of every entry (int32); and row_start[d] = the first sorted
+// position with key >= d (keys sorted, the invalid key n_nodes last), position j setting
+// the rows between its predecessor's key and its own.
+__global__ void k_csr_out(const unsigned* __restrict__ vals, const unsigned* __restrict__ keys,
+                          i64 e, i64 n_nodes, i64* __restrict__ row_start,
+                          i64* __restrict__ partners, int* __restrict__ entry_row) {
     td3_chain_wait();
     td3_chain_release();
     i64 j = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (j > e) return;
     i64 prev = j == 0 ? -1 : (i64)keys[j - 1];
-    i64 cur = j == e ? n_nodes : (i64)keys[j];
-    if (cur > n_nodes) cur = n_nodes;
+    i64 cur = n_nodes;
+    if (j < e) {
+        unsigned key = keys[j];
+        partners[j] = vals[j];
+        if (entry_row) entry_row[j] = (int)key;
+        cur = (i64)key < n_nodes ? (i64)key : n_nodes;
+    }
     for (i64 d = prev + 1; d <= cur; ++d) row_start[d] = j;
-}
-
-// partners (int64) and, when asked, the row of every entry (int32)
-__global__ void k_csr_out(const unsigned* __restrict__ vals, const unsigned* __restrict__ keys,
-                          i64 count, i64* __restrict__ partners, int* __restrict__ entry_row) {
-    td3_chain_wait();
-    td3_chain_release();
-    i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= count) return;
-    partners[k] = vals[k];
-    if (entry_row) entry_row[k] = (int)keys[k];
 }
 
 int bits_for(i64 v) {
@@ -502,13 +499,11 @@ extern "C" int td3_pair_csr(const int64_t* pairs, int64_t count, int mutual, int
     unsigned *ko, *vo;
     TD3_TRY_RC(td3_radix_sort_u32(k0, k1, v0, v1, e, bits_for(n_nodes), &ko, &vo, w.base + w.used,
                                   w.size - w.used, s));
-    // the row offsets from the boundaries between equal keys of the sorted entries
-    TD3_TRY(td3_launch_chained(k_row_starts, td3_blocks(e + 1, 256), 256, 0, s, ko, e, n_nodes,
-                               row_start));
-    // valid entries sort before the invalid key n_nodes (row_start[n_nodes] of them); the
-    // entries after them are widened too (partners holds e slots), so no host read
-    TD3_TRY(td3_launch_chained(k_csr_out, td3_blocks(e, 256), 256, 0, s, vo, ko, e, partners,
-                               entry_row));
+    // the row offsets from the boundaries between equal keys of the sorted entries; valid
+    // entries sort before the invalid key n_nodes (row_start[n_nodes] of them), the entries
+    // after them are widened too (partners holds e slots), so no host read
+    TD3_TRY(td3_launch_chained(k_csr_out, td3_blocks(e + 1, 256), 256, 0, s, vo, ko, e, n_nodes,
+                               row_start, partners, entry_row));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
