@@ -76,6 +76,112 @@ k_m2l_cart(const i64* __restrict__ row_start, const i64* __restrict__ partners, 
     }
 }
 
+// The same M2L for orders up to P (P = 4, 8, 12, 16) in scaled form and a lane per
+// partner.  With m~_a = (-1)^|a| m_a / (a_x! a_y!) and A~_g = g_x! g_y! A_g, the rows
+// (b, a, a + b) with coef = (-1)^|a| C(a_x + b_x, a_x) C(a_y + b_y, a_y) become
+//   T_b = T~_b / (b_x! b_y!),  T~_b = sum_a m~_a A~_(a+b).
+// A warp takes one destination and its partners CART_GROUP at a time: lane p < 8 builds
+// partner p's A~ by the reference's recurrence (scaled, the last two degrees in
+// registers) into a column of shared memory, lane 8 + p scales partner p's moments into
+// another; then lane (q, p) = (lane / 8, lane % 8) forms partner p's share of T~_b for
+// b = 4j + q, and three butterfly steps over p add the 8 shares (fixed order).
+constexpr int CART_GROUP = 8;
+constexpr int CART_LANE_MAX = 16;
+
+struct CartScale {
+    short bx[(CART_LANE_MAX + 1) * (CART_LANE_MAX + 2) / 2];
+    short by[(CART_LANE_MAX + 1) * (CART_LANE_MAX + 2) / 2];
+    double inv_fact2[(CART_LANE_MAX + 1) * (CART_LANE_MAX + 2) / 2];  // 1 / (a_x! a_y!)
+};
+
+template <int P>
+__global__ void __launch_bounds__(32 * CM2L_WARPS)
+k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ partners,
+                 i64 n_dst, const double* __restrict__ dst_center,
+                 const double* __restrict__ src_center, const double* __restrict__ moments,
+                 int order, double eps2, const CartScale C, double* __restrict__ local) {
+    constexpr int W = P + 1;
+    extern __shared__ double cart_smem[];
+    td3_chain_wait();
+    td3_chain_release();
+    int n_coef = (order + 1) * (order + 2) / 2;
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int p = lane & (CART_GROUP - 1), q = lane >> 3;
+    // per warp: A~ [g][partner], m~ [a][partner], T~ [b]
+    double* At = cart_smem + (size_t)wib * (2 * CART_GROUP + 1) * n_coef;
+    double* Mt = At + CART_GROUP * n_coef;
+    double* T = Mt + CART_GROUP * n_coef;
+    for (i64 dst = (i64)blockIdx.x * CM2L_WARPS + wib; dst < n_dst;
+         dst += (i64)gridDim.x * CM2L_WARPS) {
+        i64 e0 = row_start[dst], e1 = row_start[dst + 1];
+        if (e0 == e1) continue;
+        double cx = dst_center[2 * dst], cy = dst_center[2 * dst + 1];
+        for (int b = lane; b < n_coef; b += 32) T[b] = 0.0;
+        for (i64 base = e0; base < e1; base += CART_GROUP) {
+            __syncwarp();
+            bool live = base + p < e1;
+            i64 src = live ? partners[base + p] : 0;
+            if (lane < CART_GROUP) {
+                double tx = cx - src_center[2 * src], ty = cy - src_center[2 * src + 1];
+                // a lane past the row's end builds a zero column (finite scale)
+                double r2 = live ? tx * tx + ty * ty + eps2 : 1.0;
+                double prev2[W], prev1[W], cur[W];
+                prev1[0] = live ? 1.0 / sqrt(r2) : 0.0;
+                At[p] = prev1[0];
+                double inv_r2 = 1.0 / r2;
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    if (n > order) break;
+                    double scale = -inv_r2 / n;
+#pragma unroll
+                    for (int gy = 0; gy <= n; ++gy) {
+                        int gx = n - gy;
+                        double s = 0.0;
+                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy];
+                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[gy - 1];
+                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy];
+                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[gy - 2];
+                        cur[gy] = s * scale;
+                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = cur[gy];
+                    }
+#pragma unroll
+                    for (int k = 0; k < W; ++k) {
+                        prev2[k] = prev1[k];
+                        prev1[k] = cur[k];
+                    }
+                }
+            } else if (lane < 2 * CART_GROUP) {
+                const double* m = moments + src * n_coef;
+                for (int a = 0; a < n_coef; ++a) {
+                    double v = live ? m[a] * C.inv_fact2[a] : 0.0;
+                    Mt[a * CART_GROUP + p] = ((C.bx[a] + C.by[a]) & 1) ? -v : v;
+                }
+            }
+            __syncwarp();
+            for (int j0 = 0; j0 < n_coef; j0 += 4) {
+                int b = j0 + q;
+                double acc = 0.0;
+                if (b < n_coef) {
+                    int bx = C.bx[b], by = C.by[b], nb = bx + by;
+                    for (int na = 0; na + nb <= order; ++na) {
+                        int ng = na + nb;
+                        const double* mrow = Mt + (na * (na + 1) / 2) * CART_GROUP + p;
+                        const double* grow = At + (ng * (ng + 1) / 2 + by) * CART_GROUP + p;
+                        for (int ay = 0; ay <= na; ++ay)
+                            acc += mrow[ay * CART_GROUP] * grow[ay * CART_GROUP];
+                    }
+                }
+                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                if (p == 0 && b < n_coef) T[b] += acc;
+            }
+        }
+        __syncwarp();
+        for (int b = lane; b < n_coef; b += 32) local[dst * n_coef + b] += T[b] * C.inv_fact2[b];
+    }
+}
+
 // L2L of one level: thread per (node, child, b): T_b(child) += sum_g C(g, b) T_g s^(g-b)
 // over the rows of b (g, d = g - b, coef), the monomial s^d built as the reference's mono
 // recurrence builds it (d_y factors of s_y, then d_x of s_x).
@@ -114,6 +220,34 @@ extern "C" int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, i
     if (n_dst == 0) return TD3_OK;
     cudaStream_t s = td3_stream(stream);
     int n_coef = (order + 1) * (order + 2) / 2;
+    if (order <= CART_LANE_MAX) {
+        CartScale C{};
+        double f[CART_LANE_MAX + 1];
+        f[0] = 1.0;
+        for (int k = 1; k <= CART_LANE_MAX; ++k) f[k] = f[k - 1] * k;
+        for (int n = 0; n <= order; ++n)
+            for (int y = 0; y <= n; ++y) {
+                int i = n * (n + 1) / 2 + y;
+                C.bx[i] = (short)(n - y);
+                C.by[i] = (short)y;
+                C.inv_fact2[i] = 1.0 / (f[n - y] * f[y]);
+            }
+        size_t lane_smem = sizeof(double) * (2 * CART_GROUP + 1) * n_coef * CM2L_WARPS;
+        i64 nb = (n_dst + CM2L_WARPS - 1) / CM2L_WARPS;
+        unsigned grid = (unsigned)(nb < 148 * 64 ? nb : 148 * 64);
+        auto run = [&](auto kernel) -> int {
+            TD3_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)lane_smem));
+            TD3_TRY(td3_launch_chained(kernel, grid, 32 * CM2L_WARPS, lane_smem, s, row_start,
+                                       partners, n_dst, dst_center, src_center, moments, order,
+                                       softening * softening, C, local));
+            return TD3_OK;
+        };
+        if (order <= 4) return run(k_m2l_cart_lanes<4>);
+        if (order <= 8) return run(k_m2l_cart_lanes<8>);
+        if (order <= 12) return run(k_m2l_cart_lanes<12>);
+        return run(k_m2l_cart_lanes<16>);
+    }
     size_t smem = sizeof(double) * 2 * n_coef * CM2L_WARPS;
     if (smem > 48 * 1024)
         TD3_TRY(cudaFuncSetAttribute(k_m2l_cart, cudaFuncAttributeMaxDynamicSharedMemorySize,
