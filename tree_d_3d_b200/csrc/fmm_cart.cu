@@ -182,31 +182,35 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
     }
 }
 
-// L2L of one level: thread per (node, child, b): T_b(child) += sum_g C(g, b) T_g s^(g-b)
-// over the rows of b (g, d = g - b, coef), the monomial s^d built as the reference's mono
-// recurrence builds it (d_y factors of s_y, then d_x of s_x).
-__global__ void k_l2l_cart(i64 lo, i64 hi, int n_coef, const double* __restrict__ center,
-                           const i64* __restrict__ child, const i64* __restrict__ ex,
-                           const i64* __restrict__ ey, const int* __restrict__ l2l_start,
+// L2L of one level: a block per (node, child), thread b: T_b(child) += sum_g C(g, b) T_g
+// s^(g-b) over the rows of b (g, d = g - b, coef).  The monomials s^d are built once per
+// block into shared memory, column d_y by thread d_y as the reference's mono recurrence
+// builds them (d_y factors of s_y, then s_x one at a time).
+__global__ void k_l2l_cart(i64 lo, int order, int n_coef, const double* __restrict__ center,
+                           const i64* __restrict__ child, const int* __restrict__ l2l_start,
                            const int* __restrict__ l2l_g, const int* __restrict__ l2l_d,
                            const double* __restrict__ l2l_coef, double* __restrict__ local) {
-    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    i64 node = lo + t / (4 * n_coef);
-    if (node >= hi) return;
+    extern __shared__ double shift_mono[];
+    i64 node = lo + blockIdx.x / 4;
     i64 first = child[node];
-    if (first < 0) return;
-    int c = (int)((t / n_coef) % 4), b = (int)(t % n_coef);
-    i64 ch = first + c;
+    if (first < 0) return;  // the whole block: a leaf has no children
+    i64 ch = first + (blockIdx.x & 3);
     double sx = center[2 * ch] - center[2 * node], sy = center[2 * ch + 1] - center[2 * node + 1];
-    double acc = 0.0;
-    for (int r = l2l_start[b]; r < l2l_start[b + 1]; ++r) {
-        int d = l2l_d[r];
+    for (int dy = threadIdx.x; dy <= order; dy += blockDim.x) {
         double mono = 1.0;
-        for (int k = 0; k < (int)ey[d]; ++k) mono = mono * sy;
-        for (int k = 0; k < (int)ex[d]; ++k) mono = mono * sx;
-        acc += l2l_coef[r] * local[node * n_coef + l2l_g[r]] * mono;
+        for (int k = 0; k < dy; ++k) mono = mono * sy;
+        for (int dx = 0; dx + dy <= order; ++dx) {
+            shift_mono[(dx + dy) * (dx + dy + 1) / 2 + dy] = mono;
+            mono = mono * sx;
+        }
     }
-    local[ch * n_coef + b] += acc;
+    __syncthreads();
+    for (int b = threadIdx.x; b < n_coef; b += blockDim.x) {
+        double acc = 0.0;
+        for (int r = l2l_start[b]; r < l2l_start[b + 1]; ++r)
+            acc += l2l_coef[r] * local[node * n_coef + l2l_g[r]] * shift_mono[l2l_d[r]];
+        local[ch * n_coef + b] += acc;
+    }
 }
 
 }  // namespace
@@ -269,13 +273,19 @@ extern "C" int td3_cart_downward(const int64_t* levels, int64_t n_levels, const 
     if (n_levels < 1 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
     cudaStream_t s = td3_stream(stream);
     int n_coef = (order + 1) * (order + 2) / 2;
+    unsigned threads = (unsigned)((n_coef + 31) / 32 * 32);
+    if (threads > 256) threads = 256;
+    size_t smem = sizeof(double) * n_coef;
+    if (smem > 48 * 1024)
+        TD3_TRY(cudaFuncSetAttribute(k_l2l_cart, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+    (void)ex;
+    (void)ey;
     for (i64 level = 0; level + 1 < n_levels; ++level) {
         i64 lo = levels[level], hi = levels[level + 1];
         if (hi <= lo) continue;
-        i64 threads = (hi - lo) * 4 * n_coef;
-        k_l2l_cart<<<td3_blocks(threads, 256), 256, 0, s>>>(lo, hi, n_coef, node_center, node_child,
-                                                            ex, ey, l2l_start, l2l_g, l2l_d,
-                                                            l2l_coef, local);
+        k_l2l_cart<<<(unsigned)(4 * (hi - lo)), threads, smem, s>>>(
+            lo, order, n_coef, node_center, node_child, l2l_start, l2l_g, l2l_d, l2l_coef, local);
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;

@@ -337,55 +337,125 @@ int launch_log_moments(const int64_t* levels, int64_t n_levels, int order, const
     return TD3_OK;
 }
 
-// One thread per (node, coefficient g).  The monomial u^(a,b) is built as the
-// reference's mono recurrence builds it: b factors of u_y, then a factors of u_x.
-__device__ __forceinline__ double monomial(double start, double ux, double uy, int a, int b) {
-    double v = start;
-    for (int t = 0; t < b; ++t) v = v * uy;
-    for (int t = 0; t < a; ++t) v = v * ux;
-    return v;
-}
+// Cartesian moments with a block per node and thread g per coefficient.  The monomials
+// u^(a,b) a particle (or a child's shift) needs are built once into shared memory, column
+// b by thread b as the reference's mono recurrence builds them (b factors of u_y, then
+// u_x one at a time; for a particle the first factor is its charge), and each
+// coefficient sums them row by row in the reference's order.
+__device__ __forceinline__ int cart_index(int a, int b) { return (a + b) * (a + b + 1) / 2 + b; }
 
-__global__ void k_cart_moments(i64 lo, i64 hi, int n_coef, const double* __restrict__ spos,
-                               const double* __restrict__ scharge, i64 n_particles,
-                               const double* __restrict__ node_center,
-                               const i64* __restrict__ node_start, const i64* __restrict__ node_end,
-                               const i64* __restrict__ node_child, const i64* __restrict__ ex,
-                               const i64* __restrict__ ey, const i64* __restrict__ shift,
-                               const double* __restrict__ shift_coef,
-                               const i64* __restrict__ shift_start, double* moments,
-                               const double* __restrict__ sdip) {
-    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    i64 node = lo + t / n_coef;
-    int g = (int)(t % n_coef);
-    if (node >= hi) return;
+constexpr int CART_MOM_THREADS = 256;
+constexpr int CART_MOM_PER_THREAD = 9;  // 256 x 9 coefficients: orders up to 66
+
+__global__ void __launch_bounds__(CART_MOM_THREADS)
+k_cart_moments_block(i64 lo, int order, int n_coef, const double* __restrict__ spos,
+                     const double* __restrict__ scharge, i64 n_particles,
+                     const double* __restrict__ node_center, const i64* __restrict__ node_start,
+                     const i64* __restrict__ node_end, const i64* __restrict__ node_child,
+                     const i64* __restrict__ shift, const double* __restrict__ shift_coef,
+                     const i64* __restrict__ shift_start, double* moments,
+                     const double* __restrict__ sdip) {
+    extern __shared__ double mono_tab[];  // [n_coef] start q (or 1), [n_coef] start 1
+    i64 node = lo + blockIdx.x;
     double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
-    int ga = (int)ex[g], gb = (int)ey[g];
-    double acc = 0.0;
+    double acc[CART_MOM_PER_THREAD];
+#pragma unroll
+    for (int j = 0; j < CART_MOM_PER_THREAD; ++j) acc[j] = 0.0;
     i64 first = node_child[node];
     if (first < 0) {
         for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+            double q = scharge[k];
             double ux = spos[k] - xmid, uy = spos[n_particles + k] - ymid;
-            acc += monomial(scharge[k], ux, uy, ga, gb);
-            if (sdip) {
-                // a point dipole p = -e: m_g += p . grad (r - c)^g
-                if (ga > 0) acc -= sdip[k] * ga * monomial(1.0, ux, uy, ga - 1, gb);
-                if (gb > 0) acc -= sdip[n_particles + k] * gb * monomial(1.0, ux, uy, ga, gb - 1);
+            __syncthreads();
+            for (int dy = threadIdx.x; dy <= order; dy += blockDim.x) {
+                double v = q, w = 1.0;
+                for (int t = 0; t < dy; ++t) {
+                    v = v * uy;
+                    w = w * uy;
+                }
+                for (int dx = 0; dx + dy <= order; ++dx) {
+                    mono_tab[cart_index(dx, dy)] = v;
+                    if (sdip) mono_tab[n_coef + cart_index(dx, dy)] = w;
+                    v = v * ux;
+                    w = w * ux;
+                }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int j = 0; j < CART_MOM_PER_THREAD; ++j) {
+                int g = threadIdx.x + j * blockDim.x;
+                if (g >= n_coef) break;
+                acc[j] += mono_tab[g];
+                if (sdip) {
+                    int n = 0;
+                    while ((n + 1) * (n + 2) / 2 <= g) ++n;
+                    int gb = g - n * (n + 1) / 2, ga = n - gb;
+                    // a point dipole p = -e: m_g += p . grad (r - c)^g
+                    if (ga > 0) acc[j] -= sdip[k] * ga * mono_tab[n_coef + cart_index(ga - 1, gb)];
+                    if (gb > 0)
+                        acc[j] -= sdip[n_particles + k] * gb *
+                                  mono_tab[n_coef + cart_index(ga, gb - 1)];
+                }
             }
         }
     } else {
         for (i64 child = first; child < first + 4; ++child) {
             if (node_end[child] == node_start[child]) continue;
             double ux = node_center[2 * child] - xmid, uy = node_center[2 * child + 1] - ymid;
+            __syncthreads();
+            for (int dy = threadIdx.x; dy <= order; dy += blockDim.x) {
+                double v = 1.0;
+                for (int t = 0; t < dy; ++t) v = v * uy;
+                for (int dx = 0; dx + dy <= order; ++dx) {
+                    mono_tab[cart_index(dx, dy)] = v;
+                    v = v * ux;
+                }
+            }
+            __syncthreads();
             const double* cm = moments + child * n_coef;
-            for (i64 r = shift_start[g]; r < shift_start[g + 1]; ++r) {
-                int b = (int)shift[3 * r + 1];
-                int d = (int)shift[3 * r + 2];
-                acc += shift_coef[r] * cm[b] * monomial(1.0, ux, uy, (int)ex[d], (int)ey[d]);
+#pragma unroll
+            for (int j = 0; j < CART_MOM_PER_THREAD; ++j) {
+                int g = threadIdx.x + j * blockDim.x;
+                if (g >= n_coef) break;
+                for (i64 r = shift_start[g]; r < shift_start[g + 1]; ++r) {
+                    int b = (int)shift[3 * r + 1];
+                    int d = (int)shift[3 * r + 2];
+                    acc[j] += shift_coef[r] * cm[b] * mono_tab[d];
+                }
             }
         }
     }
-    moments[node * n_coef + g] = acc;
+#pragma unroll
+    for (int j = 0; j < CART_MOM_PER_THREAD; ++j) {
+        int g = threadIdx.x + j * blockDim.x;
+        if (g < n_coef) moments[node * n_coef + g] = acc[j];
+    }
+}
+
+int launch_cart_moments(const int64_t* levels, int64_t n_levels, const double* spos,
+                        const double* scharge, int64_t n, const double* center, const i64* start,
+                        const i64* end, const i64* child, const i64* shift,
+                        const double* shift_coef, const i64* shift_start, int n_coef,
+                        double* moments, const double* sdip, cudaStream_t s) {
+    int order = 0;
+    while ((order + 1) * (order + 2) / 2 < n_coef) ++order;
+    if ((order + 1) * (order + 2) / 2 != n_coef) return TD3_EINVAL;
+    unsigned threads = (unsigned)((n_coef + 31) / 32 * 32);
+    if (threads > CART_MOM_THREADS) threads = CART_MOM_THREADS;
+    if (n_coef > (int)threads * CART_MOM_PER_THREAD) return TD3_EINVAL;
+    size_t smem = sizeof(double) * 2 * n_coef;
+    if (smem > 48 * 1024)
+        TD3_TRY(cudaFuncSetAttribute(k_cart_moments_block,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    for (i64 level = n_levels - 1; level >= 0; --level) {
+        i64 lo = levels[level], hi = levels[level + 1];
+        if (hi <= lo) continue;
+        k_cart_moments_block<<<(unsigned)(hi - lo), threads, smem, s>>>(
+            lo, order, n_coef, spos, scharge, n, center, start, end, child, shift, shift_coef,
+            shift_start, moments, sdip);
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
 }
 
 }  // namespace
@@ -445,17 +515,11 @@ extern "C" int td3_cart_moments(const int64_t* levels, int64_t n_levels, const d
                                 const int64_t* shift_start, int n_coef, double* moments,
                                 void* stream) {
     if (n_levels < 1 || n_coef < 1) return TD3_EINVAL;
-    cudaStream_t s = td3_stream(stream);
-    for (i64 level = n_levels - 1; level >= 0; --level) {
-        i64 lo = levels[level], hi = levels[level + 1];
-        if (hi <= lo) continue;
-        i64 threads = (hi - lo) * n_coef;
-        k_cart_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
-            lo, hi, n_coef, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
-            node_child, ex, ey, shift, shift_coef, shift_start, moments, nullptr);
-    }
-    TD3_CHECK_LAUNCH();
-    return TD3_OK;
+    (void)ex;
+    (void)ey;
+    return launch_cart_moments(levels, n_levels, sorted_pos, sorted_charge, n, node_center,
+                               node_start, node_end, node_child, shift, shift_coef, shift_start,
+                               n_coef, moments, nullptr, td3_stream(stream));
 }
 
 extern "C" int td3_cart_moments_adjoint(const int64_t* levels, int64_t n_levels,
@@ -468,15 +532,9 @@ extern "C" int td3_cart_moments_adjoint(const int64_t* levels, int64_t n_levels,
                                         const int64_t* shift_start, int n_coef, double* moments,
                                         void* stream) {
     if (n_levels < 1 || n_coef < 1) return TD3_EINVAL;
-    cudaStream_t s = td3_stream(stream);
-    for (i64 level = n_levels - 1; level >= 0; --level) {
-        i64 lo = levels[level], hi = levels[level + 1];
-        if (hi <= lo) continue;
-        i64 threads = (hi - lo) * n_coef;
-        k_cart_moments<<<td3_blocks(threads, MOM_THREADS), MOM_THREADS, 0, s>>>(
-            lo, hi, n_coef, sorted_pos, sorted_weight, n, node_center, node_start, node_end,
-            node_child, ex, ey, shift, shift_coef, shift_start, moments, sorted_dipole);
-    }
-    TD3_CHECK_LAUNCH();
-    return TD3_OK;
+    (void)ex;
+    (void)ey;
+    return launch_cart_moments(levels, n_levels, sorted_pos, sorted_weight, n, node_center,
+                               node_start, node_end, node_child, shift, shift_coef, shift_start,
+                               n_coef, moments, sorted_dipole, td3_stream(stream));
 }
