@@ -156,7 +156,9 @@ int td3_log_moments(const int64_t* levels, int64_t n_levels, int order,
  * (moments (nodes, n_coef)), with the index tables of the reference's _cartesian.tables
  * (src/tree_d_3d/_cartesian.py:40-107): ex, ey (n_coef), shift (n_shift, 3) rows
  * (g, b, g - b) sorted by g with shift_coef, and shift_start (n_coef + 1) the first
- * row of each g.  Replaces cart_moments_upward (src/tree_d_3d/kernels/
+ * row of each g (ex, ey are accepted for the reference's argument list; the powers of a
+ * coefficient follow from its index).  Bit-identical to the reference; orders up to 66.
+ * Replaces cart_moments_upward (src/tree_d_3d/kernels/
  * cart_moments_upward/cart_moments_upward_pyccel.py:14-82), called by
  * FlatQuadtree._cartesian_moments (src/tree_d_3d/flat_tree.py:1063-1084). */
 int td3_cart_moments(const int64_t* levels, int64_t n_levels, const double* sorted_pos,
@@ -323,7 +325,9 @@ int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node
  * reference's recurrence, then local[n, b] += coef * m_a * A_{a+b} over the M2L rows
  * (b, a, a + b) of _cartesian.tables (src/tree_d_3d/_cartesian.py:40-107): row_a,
  * row_g (int32), row_coef, b_start (int32, n_coef + 1: first row of each b).  moments
- * (src cells, n_coef), local (n_dst, n_coef).  Replaces cart_m2l_host
+ * (src cells, n_coef), local (n_dst, n_coef).  Orders up to 16 use the scaled form
+ * T_b = (1 / b!) sum_a ((-1)^|a| m_a / a!) (g! A_g), g = a + b, with computed indices
+ * (the row tables are then not read); higher orders read the rows.  Replaces cart_m2l_host
  * (src/tree_d_3d/kernels/cart_m2l_host/cart_m2l_host_pyccel.py:16-80). */
 int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
                  const double* dst_center, const double* src_center, const double* moments,
@@ -332,8 +336,8 @@ int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_ds
 
 /* L2L of the Cartesian local expansions from the root down (levels HOST, n_levels + 1):
  * T_b(child) += C(g, b) T_g s^(g - b) over the shift rows regrouped by b (l2l_start
- * (n_coef + 1), l2l_g, l2l_d = g - b, l2l_coef; int32 indices), ex / ey the powers of
- * each coefficient.  Replaces cart_downward (src/tree_d_3d/kernels/cart_downward/
+ * (n_coef + 1), l2l_g, l2l_d = g - b, l2l_coef; int32 indices); ex / ey are accepted for
+ * the reference's argument list.  Replaces cart_downward (src/tree_d_3d/kernels/cart_downward/
  * cart_downward_pyccel.py:14-55). */
 int td3_cart_downward(const int64_t* levels, int64_t n_levels, const double* node_center,
                       const int64_t* node_child, int order, const int64_t* ex, const int64_t* ey,
