@@ -16,8 +16,9 @@ the FP64 direct sum on 4096 sampled particles is reported (``rel_err_field``).
 host-device copies of its inputs and results inside the timed region.
 
 ``--impl reference`` times the reference algorithm on the host cores: the C
-restatement of the reference's CPU kernels (``oracle/``) with OpenMP on every core
-(field only: the reference has no backward), on a bounded sample of the workload.
+restatement of the reference's CPU kernels (``oracle/``) with OpenMP on every core, on
+the same 1M particles (field only, FP64: the reference has no backward and no mixed
+form), with one single-threaded step beside it.
 Under torchrun with N > 1 every rank runs an independent replica; rank 0 prints.
 """
 
@@ -44,7 +45,6 @@ LEAF = 8
 #: against the direct sum is defined for the unsoftened kernel
 SOFTENING = 0.0
 SEED = 3
-CPU_SAMPLE = 250_000
 L2_FLUSH_BYTES = 256 << 20
 METRIC = "FMM particles/s at N=1M p=12: mixed-prec vs FP64 GPU at rel err<=1e-6, +backward"
 WORKLOAD = ("log-kernel FMM field + backward, 1M particles, 8-Gaussian mixture, p=12, "
@@ -85,6 +85,12 @@ def _config(n):
 
 
 # ----------------------------------------------------------------------------- CPU arm
+#: what the CPU arm runs, against the GPU arm's step
+CPU_DIFFERS = ("forward only: build + FP64 FMM field at every particle (the reference has no "
+               "backward and no mixed-precision form); same particles, kernel, order, theta, "
+               "leaf capacity and softening as the GPU arm")
+
+
 def _cpu_fmm(pos, q):
     from oracle import flat_tree_oracle as oracle
 
@@ -94,44 +100,68 @@ def _cpu_fmm(pos, q):
     return time.perf_counter() - t0
 
 
+def _cpu_config(n):
+    return {**_config(n), "backward": False, "precision": "fp64", "differs": CPU_DIFFERS,
+            "implementation": ("the oracle: C restatement of the reference's CPU kernels "
+                               "(K/*/<name>_pyccel.py) driven as the reference's flat_tree.py, "
+                               "OpenMP on the loops the reference parallelises")}
+
+
+def _single_thread(pos, q, cores):
+    """One step of the same workload on one thread (the reference's unmodified,
+    single-threaded kernels), then the thread count back to ``cores``."""
+    from oracle import flat_tree_oracle as oracle
+
+    oracle.set_threads(1)
+    try:
+        seconds = _cpu_fmm(pos, q)
+    finally:
+        oracle.set_threads(cores)
+    return {"value": pos.shape[1] / seconds, "unit": "particles/s", "cores": 1,
+            "ms_per_step": 1e3 * seconds}
+
+
 def cpu_baseline(repeats=2):
-    """The oracle (C restatement of the reference's CPU kernels, OpenMP on all cores)
-    on a bounded sample of the workload, field only; particles/s."""
+    """The oracle on the host cores, on the full 1M workload, field only: particles/s
+    on every core (best of ``repeats`` after one warm-up) and on one thread."""
     from oracle import flat_tree_oracle as oracle
     from tree_d_3d_b200 import synthetic
 
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    pos, q = synthetic.mixture8(CPU_SAMPLE, seed=SEED)
+    pos, q = synthetic.mixture8(N_PARTICLES, seed=SEED)
     _cpu_fmm(pos, q)
     best = min(_cpu_fmm(pos, q) for _ in range(repeats))
     return {
-        "value": CPU_SAMPLE / best,
+        "value": N_PARTICLES / best,
         "unit": "particles/s",
         "cores": cores,
         "kind": "port",
-        "sample": (f"{CPU_SAMPLE} particles of the workload's distribution, tree build + "
-                   f"FP64 FMM field (the reference has no backward), best of {repeats}"),
+        "sample": (f"the full workload ({N_PARTICLES} particles), {CPU_DIFFERS}; best of "
+                   f"{repeats}"),
+        "single_thread": _single_thread(pos, q, cores),
     }
 
 
 def run_reference(args):
+    """The reference's CPU algorithm (the oracle) on the host cores, on the same 1M
+    particles as the GPU arm; rank 0 alone runs it under torchrun."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     from oracle import flat_tree_oracle as oracle
     from tree_d_3d_b200 import synthetic
 
+    n = args.n
     cores = os.cpu_count() or 1
     oracle.set_threads(cores)
-    pos, q = synthetic.mixture8(CPU_SAMPLE, seed=SEED)
+    pos, q = synthetic.mixture8(n, seed=SEED)
     for _ in range(max(args.warmup, 1)):
         _cpu_fmm(pos, q)
     times = [_cpu_fmm(pos, q) for _ in range(args.steps)]
     total = sum(times)
-    value = CPU_SAMPLE * args.steps / total
-    sample = (f"{CPU_SAMPLE} particles of the workload's distribution per step, tree build + "
-              "FP64 FMM field (the reference has no backward)")
+    value = n * args.steps / total
+    sample = f"{n} particles per step (the full workload), {CPU_DIFFERS}"
     line = {
         "impl": "reference",
         "metric": METRIC,
@@ -146,9 +176,9 @@ def run_reference(args):
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic",
-        "config": _config(N_PARTICLES),
+        "config": _cpu_config(n),
         "cpu_baseline": {"value": value, "unit": "particles/s", "cores": cores, "kind": "port",
-                         "sample": sample},
+                         "sample": sample, "single_thread": _single_thread(pos, q, cores)},
         "e2e": {"value": value, "unit": "particles/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -431,7 +461,8 @@ def run_ours(args):
         "vs_baseline": None,
         "dtype": "f32+f64 mixed",
         "data": "synthetic",
-        "config": {**_config(n), "parallelism": f"replicas x{world}", "precision": "mixed"},
+        "config": {**_config(n), "parallelism": f"replicas x{world}", "precision": "mixed",
+                   "backward": True},
         "fp64": {"value": fp64_value, "ms_per_step": fp64_ms / args.steps,
                  "speedup_mixed_over_fp64": value / fp64_value,
                  "rel_err_field": err_fp64},

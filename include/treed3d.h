@@ -18,7 +18,10 @@
  *     by the matching *_workspace_size query; the library allocates nothing;
  *   - return value: TD3_OK, or an error code below (launch errors are TD3_ECUDA with
  *     the CUDA error kept for td3_last_error).
- * Entry points are re-entrant and keep no state between calls.
+ * Entry points are re-entrant and keep no state between calls, with one exception:
+ * td3_direct_sum_noalloc keeps its scratch in one fixed device array shared by all of
+ * its calls (and caches that array's address per device), so its calls must not
+ * overlap on the GPU; its block below gives the details.
  */
 #ifndef TREED3D_H
 #define TREED3D_H
@@ -74,9 +77,11 @@ int td3_direct_sum(int kernel, const double* targets, int64_t n_targets, const i
  * it, kept until exit), enough for at most TD3_DIRECT_NOALLOC_MAX_TARGETS targets and
  * any number of sources; more targets return TD3_ETOOLARGE (td3_last_error says why).
  * The first call on a device looks up the array's device address (once per device,
- * with that device current); make that first call before any stream capture.  Every
- * call shares the array: calls that overlap on the GPU (other streams, other threads)
- * race on it.  Results equal td3_direct_sum's. */
+ * with that device current); make that first call before any stream capture.  The
+ * address stays cached until the process exits: do not reset a device
+ * (cudaDeviceReset) between calls of this entry point.  Every call shares the array:
+ * calls that overlap on the GPU (other streams, other threads) race on it, so
+ * serialise them.  Results equal td3_direct_sum's. */
 #define TD3_DIRECT_NOALLOC_MAX_TARGETS 65536
 int td3_direct_sum_noalloc(int kernel, const double* targets, int64_t n_targets,
                            const int64_t* exclude, const double* pos, const double* charge,

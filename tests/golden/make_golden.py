@@ -1,9 +1,10 @@
 """Generate the golden fixtures of the field solver from the reference implementation.
 
-Run in a checkout where the reference package tree-d-3d is available (its ``src``
-directory is passed with ``--reference``, default ``/root/reference/src``)::
+Run where the reference package tree-d-3d is available: its ``src`` directory is
+passed with ``--reference`` or, failing that, in the ``TD3_REFERENCE_SRC``
+environment variable::
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference <tree-d-3d checkout>/src
 
 It imports the reference's own ``tree_d_3d.flat_tree`` unmodified, behind minimal
 stand-ins for the packages it imports but does not need for one process on the CPU
@@ -23,6 +24,7 @@ import argparse
 import ast
 import importlib
 import importlib.util
+import os
 import sys
 import textwrap
 import types
@@ -400,10 +402,14 @@ def make_strip():
 
 def main() -> None:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference/src")
+    parser.add_argument("--reference", default=os.environ.get("TD3_REFERENCE_SRC"),
+                        help="the reference's src directory (default: $TD3_REFERENCE_SRC)")
     parser.add_argument("--python", action="store_true", help="plain Python kernels")
     parser.add_argument("--only", nargs="*", help="the fixture groups to write (default all)")
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("the reference's src directory is required: pass --reference or set "
+                     "TD3_REFERENCE_SRC")
     install_stubs(Path(args.reference), use_numba=not args.python)
     ft = importlib.import_module("tree_d_3d.flat_tree")
     from tree_d_3d.quad import Quad

@@ -137,3 +137,29 @@ def test_strip_arguments_are_checked_like_the_reference():
         GroundedStripField(1.0, cutoff=1.0)
     strip = GroundedStripField(2.0)
     assert (strip.order, strip.theta, strip.leaf_capacity, strip.cutoff) == (14, 0.5, 32, 6.0)
+
+
+def test_trace_regions_follow_the_reference_names_and_are_off_by_default():
+    """NVTX ranges named as the reference's scope-profiler regions
+    (src/tree_d_3d/_profiling.py:10-13): off by default, nested when on."""
+    from tree_d_3d_b200 import _trace
+
+    was = _trace.enabled()
+    _trace.opened.clear()
+    try:
+        _trace.enable(False)
+        with _trace.region("flat_tree.fmm"):
+            pass
+        assert _trace.opened == []
+
+        @_trace.profile("flat_tree.evaluate")
+        def walk(x):
+            with _trace.region("flat_tree.traverse"):
+                return 2 * x
+
+        _trace.enable(True)
+        assert walk(3) == 6
+        assert _trace.opened == ["tree_d_3d.flat_tree.evaluate", "tree_d_3d.flat_tree.traverse"]
+    finally:
+        _trace.enable(was)
+        _trace.opened.clear()

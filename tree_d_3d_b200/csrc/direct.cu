@@ -266,7 +266,10 @@ double* g_scratch_address[NOALLOC_MAX_DEVICES] = {};
 
 // The device address of g_direct_scratch on the current device, looked up once per
 // device.  In host code the array's name is only a host-side stand-in, so the address
-// must come from cudaGetSymbolAddress with that device current.
+// must come from cudaGetSymbolAddress with that device current.  The address is kept
+// for the life of the process; a cudaDeviceReset (which destroys the context that
+// holds the array) would leave it stale, so callers of this entry point must not
+// reset the device between calls (stated in the header).
 int noalloc_scratch(double** out) {
     int dev = 0;
     TD3_TRY(cudaGetDevice(&dev));

@@ -14,6 +14,7 @@ import numpy as np
 import torch
 
 from tree_d_3d_b200 import _lib
+from tree_d_3d_b200._trace import profile, region
 from tree_d_3d_b200._utils import (
     _check,
     _device,
@@ -64,6 +65,7 @@ def _direct(targets, exclude, pos, charge, softening, kernel, potential=True):
     return phi, field
 
 
+@profile("flat_tree.direct_field")
 def direct_field(targets, pos, charge, *, softening=0.0, exclude=None, compiled=True,
                  kernel="coulomb"):
     """Exact potential (M,) and field (2, M) at ``targets`` (2, M), without ``k_e``.
@@ -267,11 +269,13 @@ class FlatQuadtree:
         if not n:
             self._empty()
             return
-        count = self._build()
+        with region("flat_tree.build"):
+            count = self._build()
         self.node_count = int(count)
         for name in _NODE_ARRAYS:  # views of the first `count` rows of the build's buffers
             setattr(self, name, getattr(self, name)[:count])
-        self._moments()
+        with region("flat_tree.moments"):
+            self._moments()
 
     # ------------------------------------------------------------------ build
     def _empty(self) -> None:
@@ -473,6 +477,7 @@ class FlatQuadtree:
             status.data_ptr(), ws.data_ptr(), ws.numel(), _lib.stream(self.device),
         )
 
+    @profile("flat_tree.evaluate")
     def evaluate(self, targets, *, exclude=None, theta=0.5, softening=0.0, potential=True):
         """Potential (M,) and field (2, M) at ``targets`` (2, M) by the Barnes-Hut walk,
         without ``k_e`` (ft:987-1061).
@@ -565,16 +570,22 @@ class FlatQuadtree:
         """The interaction lists of ``theta``, their rows and the near-field plan, kept
         across set_charges (ft:1496-1498): they depend on the cells only."""
         if theta not in self._traversals:
-            m2l, p2p = self._traverse(theta)
-            m2l_rows, m2l_partners, m2l_entry = self._rows(m2l, mutual=True, entry_rows=True)
-            p2p_rows, p2p_partners = self._rows(p2p, mutual=True)
-            lists = {
-                "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
-                "m2l_entry_row": m2l_entry, "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
-            }
-            lists["plan"] = _nearfield_plan(p2p_rows, self, 2 * p2p.shape[0])
-            self._traversals[theta] = lists
+            with region("flat_tree.traverse"):
+                self._traversals[theta] = self._new_lists(theta)
         return self._traversals[theta]
+
+    def _new_lists(self, theta: float) -> dict:
+        """The mutual lists of ``theta`` (ft:1318-1358), their CSR rows and the
+        near-field plan."""
+        m2l, p2p = self._traverse(theta)
+        m2l_rows, m2l_partners, m2l_entry = self._rows(m2l, mutual=True, entry_rows=True)
+        p2p_rows, p2p_partners = self._rows(p2p, mutual=True)
+        lists = {
+            "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
+            "m2l_entry_row": m2l_entry, "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
+        }
+        lists["plan"] = _nearfield_plan(p2p_rows, self, 2 * p2p.shape[0])
+        return lists
 
     def _m2l_matrix(self) -> torch.Tensor:
         key = ("m2l_coefficients", self.order, self.symmetric)
@@ -582,6 +593,7 @@ class FlatQuadtree:
                              self.device)
 
     # ------------------------------------------------------------------ FMM
+    @profile("flat_tree.fmm")
     def fmm(self, *, theta: float = 0.5, softening: float = 0.0, potential: bool = True,
             _status: torch.Tensor | None = None):
         """Potential (N,) and field (2, N) at every source by the FMM, without ``k_e``
@@ -724,6 +736,7 @@ class FlatQuadtree:
                   local_im.data_ptr(), stream)
 
     # ------------------------------------------------------------------ backward
+    @profile("flat_tree.fmm_backward")
     def _fmm_adjoint(self, theta: float, softening: float, weight: torch.Tensor,
                      dipole: torch.Tensor, efield: torch.Tensor):
         """The backward of ``fmm`` at the sources: for upstream gradients ``weight`` =
@@ -863,6 +876,7 @@ class FlatQuadtree:
         self._plans[key] = (targets.clone(), tree, lists)
         return tree, lists
 
+    @profile("flat_tree.fmm_at")
     def fmm_at(self, targets, *, exclude=None, theta: float = 0.5, softening: float = 0.0,
                potential: bool = True, leaf_capacity: int | None = None):
         """Potential (M,) and field (2, M) at ``targets`` (2, M) by the FMM, without
