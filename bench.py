@@ -7,7 +7,8 @@ A step takes the 1M particles of the workload (8-Gaussian mixture, +-1 charges o
 zero; log kernel, order 12, theta 0.5, leaf 8, unsoftened), builds a fresh tree
 (build, moments, traversal, interaction lists) and evaluates the FMM potential and
 field at every particle in mixed precision (FP32 near field with compensated sums,
-FP32 M2L on size-scaled expansions, FP64 M2M / L2L / L2P), then runs the hand-written
+M2L as 3xTF32 tensor-core products grouped by translation on size-scaled expansions,
+FP64 M2M / L2L / L2P), then runs the hand-written
 backward of L = sum w phi + sum e . E (fixed seeded w, e) to dL/dq and dL/dx.
 ``value`` is whole-job particles/s with the inputs resident in HBM; the same step in
 the plain FP64 form is timed beside it (``fp64``), and the mixed field error against
@@ -49,8 +50,6 @@ L2_FLUSH_BYTES = 256 << 20
 METRIC = "FMM particles/s at N=1M p=12: mixed-prec vs FP64 GPU at rel err<=1e-6, +backward"
 WORKLOAD = ("log-kernel FMM field + backward, 1M particles, 8-Gaussian mixture, p=12, "
             "theta=0.5, leaf 8, fresh tree per step")
-FP32_PEAK = 148 * 128 * 2 * 1.965e9 / 1e12  # FP32 FMA lanes x 2 flop x max SM clock
-FP64_PEAK = 148 * 64 * 2 * 1.965e9 / 1e12
 
 
 def _args():
@@ -290,9 +289,11 @@ def count_our_launches(fn, torch):
     return counts
 
 
-def time_m2l_mixed(tree, torch, reps, tensor=0):
-    """The mixed M2L kernel alone (CUDA events on its stream), average ms per launch;
-    tensor=1 the tensor-core form, 0 the FP32 CUDA-core form."""
+def time_m2l_mixed(tree, torch, reps, form="grouped"):
+    """One mixed M2L form alone (CUDA events on its stream), average ms per launch:
+    "grouped" the tensor-core products grouped by translation (the step's form), "lanes"
+    the FP32 CUDA-core form (a lane per translation), "tile" the per-translation
+    tensor-core form."""
     from tree_d_3d_b200 import _lib
     from tree_d_3d_b200.flat_tree import _m2l_coefficients
 
@@ -302,25 +303,46 @@ def time_m2l_mixed(tree, torch, reps, tensor=0):
     lim = torch.zeros_like(lre)
     hat = tree._scaled_moments((tree.moment_re, tree.moment_im))
     stream = _lib.stream(tree.device)
-    coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
-    status = torch.zeros(1, dtype=torch.int64, device=tree.device)
-    args = (lists["m2l_rows"].data_ptr(), lists["m2l_entry_row"].data_ptr(),
-            lists["m2l_partners"].data_ptr(), count,
-            tree.node_center.data_ptr(), tree.node_half.data_ptr(), tree.node_center.data_ptr(),
-            tree.node_half.data_ptr(), hat.data_ptr(), tree.order, coeff.ctypes.data,
-            tree._unit, tensor, lre.data_ptr(), lim.data_ptr(), status.data_ptr(), stream)
-    _lib.call("td3_fmm_m2l_mixed", *args)
+    status = tree._tensor_status()
+    if form == "grouped":
+        groups = lists["groups"]
+
+        def launch():
+            tree._m2l_grouped(groups, hat, lre, lim)
+    else:
+        coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
+        args = (lists["m2l_rows"].data_ptr(), lists["m2l_entry_row"].data_ptr(),
+                lists["m2l_partners"].data_ptr(), count,
+                tree.node_center.data_ptr(), tree.node_half.data_ptr(), tree.node_center.data_ptr(),
+                tree.node_half.data_ptr(), hat.data_ptr(), tree.order, coeff.ctypes.data,
+                tree._unit, 1 if form == "tile" else 0, lre.data_ptr(), lim.data_ptr(),
+                status.data_ptr(), stream)
+
+        def launch():
+            _lib.call("td3_fmm_m2l_mixed", *args)
+    launch()
     cur = torch.cuda.current_stream()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     start.record(cur)
     for _ in range(reps):
-        _lib.call("td3_fmm_m2l_mixed", *args)
+        launch()
     stop.record(cur)
     torch.cuda.synchronize()
-    if int(status.item()):
-        raise RuntimeError("the tensor-core M2L timed out")
+    tree._check_tensor_cores()
     return start.elapsed_time(stop) / reps, int(lists["m2l"].shape[0])
+
+
+def _peaks():
+    """Measured peaks of this pool (MEASURED_PEAKS.json) or the stated fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            data = json.load(f)
+        bf16 = float(data.get("bf16_tflops") or data.get("bf16_tflops_burst"))
+        return bf16, "of measured (MEASURED_PEAKS.json bf16_tflops)"
+    except (OSError, ValueError, TypeError):
+        return 1590.0, "of fallback (1.59 PFLOP/s bf16, no MEASURED_PEAKS.json)"
 
 
 def field_error(pos, q, precision, torch, n_sample=4096):
@@ -419,28 +441,37 @@ def run_ours(args):
     launches = count_our_launches(lambda: gpu_step(pos, q, w, e, "mixed"), torch)
     err_mixed, tree = field_error(pos, q, "mixed", torch)
     err_fp64, _ = field_error(pos, q, "fp64", torch)
-    # the product's form (FP32 CUDA cores); the tensor-core form is reported beside it
-    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, tensor=0)
-    m2l_tc_ms, _ = time_m2l_mixed(tree, torch, reps=5, tensor=1)
+    # the step's M2L form (tensor-core products grouped by translation); the FP32 CUDA-core
+    # form and the per-translation tensor-core form are timed beside it
+    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, form="grouped")
+    m2l_lanes_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="lanes")
+    m2l_tile_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="tile")
+    groups = tree._lists(THETA)["groups"]
+    n_runs = int(groups["tile_run"][-1].item())
     width = ORDER + 1
     flops = 2 * n_m2l * 8 * width * width  # directed translations x 8 (p + 1)^2
     achieved = flops / (m2l_ms * 1e-3) / 1e12
+    bf16, peak_note = _peaks()
+    tf32 = bf16 / 2  # dense TF32 runs at half the BF16 rate on the tensor cores
+    # per run: D[128 x 64] += A_hi [128 x 32] B^T and D[128 x 32] += A_lo B_hi^T
+    issued = n_runs * 2 * 128 * 32 * (64 + 32)
     roofline = {
-        "kernel": "k_m2l_mixed<12> (FP32 M2L, forward)",
-        "bound": "fp32",
+        "kernel": "k_m2l_grouped<12> (3xTF32 tcgen05 M2L grouped by translation, forward)",
+        "bound": "tensor",
         "achieved": achieved,
-        "peak": FP32_PEAK,
+        "peak": tf32,
         "unit": "TFLOP/s",
-        "frac": achieved / FP32_PEAK,
-        "peak_source": ("nominal FP32 FMA rate at the max SM clock (148 SM x 128 lanes x 2 x "
-                        "1965 MHz); MEASURED_PEAKS.json has no FP32 CUDA-core figure"),
-        # dram read + write of one ncu capture of this kernel at 300k particles (86.4 MB
-        # for 3.745M translations), scaled by the translations of this launch
-        "traffic": 86.4e6 * (2 * n_m2l) / 3.745e6,
-        "traffic_unit": "bytes per launch (scaled from a 300k-particle ncu capture)",
+        "frac": achieved / tf32,
+        "peak_source": f"dense TF32 = half the BF16 tensor rate, {peak_note}",
+        "algorithmic": "8 (p + 1)^2 flop per directed translation (the reference's count)",
+        "issued_tensor_tflops": issued / (m2l_ms * 1e-3) / 1e12,
+        "issued_frac": issued / (m2l_ms * 1e-3) / 1e12 / tf32,
+        "runs_per_launch": n_runs,
+        "traffic": None,
         "ms_per_launch": m2l_ms,
         "flop_per_launch": flops,
-        "tensor_core_form_ms_per_launch": m2l_tc_ms,
+        "fp32_lanes_form_ms_per_launch": m2l_lanes_ms,
+        "tile_form_ms_per_launch": m2l_tile_ms,
     }
     clock = clocks.summary()
     if dist:

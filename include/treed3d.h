@@ -306,6 +306,43 @@ int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
                       double unit, int tensor_cores, double* local_re, double* local_im,
                       int64_t* status, void* stream);
 
+/* The mixed-precision log M2L of the mutual lists of one tree as dense tensor-core
+ * products grouped by translation (tcgen05.mma, 3xTF32 with FP32 accumulation), orders
+ * up to TD3_M2L_GROUPED_MAX_ORDER.  A translation between cells whose depths differ by
+ * dl = -1, 0, 1 and whose centres differ by t = u h_min (u an integer vector with
+ * |u_x|, |u_y| <= span, h_min the smaller half-width) is the fixed matrix of the key
+ * (dl, u) on size-scaled expansions; the other translations take the per-translation
+ * FP32 formula.  Three calls:
+ *   td3_m2l_operators: the 3 (2 span + 1)^2 keys' matrices into `ops`
+ *     (td3_m2l_operators_size(span) bytes, float; coeff the reference's M2L matrix,
+ *     DEVICE, (order + 1)^2); depends on (order, coeff, span) only;
+ *   td3_m2l_groups: the directed translations of `pairs` (n_pairs, 2) sorted by
+ *     (tile of 128 destinations, key) into keys / values (2 n_pairs each), the run
+ *     starts run_start (2 n_pairs + 1) and the first run of every tile tile_run
+ *     (ceil(n_nodes / 128) + 1); levels HOST (n_levels + 1, the first node of each
+ *     depth, then n_nodes); n_nodes < 2^25; depends on the tree and the lists only;
+ *   td3_fmm_m2l_grouped: the products into local_re / local_im (FP64, added), from the
+ *     scaled moments `hat` of td3_scale_moments; coeff HOST; smem_operands = 1 keeps
+ *     the A operand in shared memory instead of tensor memory (same results).
+ * `status` (zeroed by the caller) receives 1 if a wait for the copies or the tensor
+ * cores ran out.  Replaces fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/
+ * fmm_m2l_host_pyccel.py:16-105) for fmm (src/tree_d_3d/flat_tree.py:1505-1539). */
+#define TD3_M2L_GROUPED_MAX_ORDER 14
+size_t td3_m2l_operators_size(int span);
+int td3_m2l_operators(int order, const double* coeff, int span, float* ops, void* stream);
+size_t td3_m2l_groups_workspace_size(int64_t n_pairs);
+int td3_m2l_groups(const int64_t* pairs, int64_t n_pairs, const double* node_center,
+                   const double* node_half, const int64_t* node_depth, const int64_t* levels,
+                   int64_t n_levels, int64_t n_nodes, int span, uint32_t* keys, uint32_t* values,
+                   int32_t* tile_run, int32_t* run_start, void* workspace,
+                   size_t workspace_bytes, void* stream);
+int td3_fmm_m2l_grouped(const int32_t* tile_run, const int32_t* run_start,
+                        const uint32_t* keys, const uint32_t* values, int64_t n_nodes,
+                        const int64_t* levels, int64_t n_levels, const double* node_center,
+                        const double* node_half, const float* hat, int order, const float* ops,
+                        int span, const double* coeff, int smem_operands, double* local_re,
+                        double* local_im, int64_t* status, void* stream);
+
 /* The parent of every node (node_parent (count), int32; -1 for the root), from
  * node_child.  No reference counterpart (its walks keep explicit stacks). */
 int td3_node_parents(int64_t count, const int64_t* node_child, int32_t* node_parent,
@@ -321,6 +358,18 @@ int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const double* node
                      const int32_t* node_parent, const int64_t* node_start,
                      const int64_t* node_end, int order, const double* binomial,
                      int binomial_size, double* local_re, double* local_im, void* stream);
+
+/* The downward pass in one launch: every non-empty leaf's local becomes its own M2L
+ * local plus the own M2L local of each ancestor shifted straight to the leaf's centre
+ * (the L2L shift above, an exact re-expansion: equal to the level-by-level pass up to
+ * rounding).  Internal cells keep their own M2L locals: only leaves feed L2P.
+ * Replaces fmm_downward's per-level loop (src/tree_d_3d/flat_tree.py:1540-1552,
+ * src/tree_d_3d/kernels/fmm_downward/fmm_downward_pyccel.py:15-64) for the FMM. */
+int td3_fmm_downward_leaves(int64_t count, int order, const double* node_center,
+                            const int32_t* node_parent, const int64_t* node_start,
+                            const int64_t* node_end, const int64_t* node_child,
+                            const double* binomial, int binomial_size, double* local_re,
+                            double* local_im, void* stream);
 
 /* ------------------------------------------------------------------ Coulomb FMM */
 
@@ -338,6 +387,18 @@ int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, int64_t n_ds
                  const double* dst_center, const double* src_center, const double* moments,
                  int order, double softening, const int* row_a, const int* row_g,
                  const double* row_coef, const int* b_start, double* local, void* stream);
+
+/* The mixed-precision td3_cart_m2l for orders up to 16: the same translations in FP32
+ * on expansions scaled by the source cell's half-width (t / h_src, eps / h_src,
+ * m_a / h_src^|a|), the partners' sums brought to the destination's scale by exact
+ * powers of two and added to the FP64 locals with h_dst^(-1-|b|) in FP64; dst_half and
+ * src_half the cells' half-widths.  Replaces cart_m2l_host (src/tree_d_3d/kernels/
+ * cart_m2l_host/cart_m2l_host_pyccel.py:16-80) in the mixed form. */
+int td3_cart_m2l_mixed(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                       const double* dst_center, const double* dst_half,
+                       const double* src_center, const double* src_half,
+                       const double* moments, int order, double softening, double* local,
+                       void* stream);
 
 /* L2L of the Cartesian local expansions from the root down (levels HOST, n_levels + 1):
  * T_b(child) += C(g, b) T_g s^(g - b) over the shift rows regrouped by b (l2l_start

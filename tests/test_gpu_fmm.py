@@ -99,3 +99,22 @@ def test_fmm_lists_survive_set_charges():
     assert tree._lists(0.5) is lists
     fresh = FlatQuadtree(pos, second, Quad(0, 0, 1), kernel="log", leaf_capacity=16)
     np.testing.assert_allclose(tree.fmm()[1], fresh.fmm()[1], rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("order", [12, 40])
+def test_downward_in_one_launch_equals_the_level_by_level_pass(order, monkeypatch):
+    """Each leaf's local from its ancestors' own locals (one launch) against the
+    reference's level-by-level L2L: the same leaf locals up to rounding."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, flat_tree, synthetic
+
+    pos, q = synthetic.mixture8(100_000, seed=4)
+    tree = FlatQuadtree(torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda"),
+                        Quad(0, 0, 1), kernel="log", order=order)
+    lists = tree._lists(0.5)
+    leaves = ((tree.node_child < 0) & (tree.node_end > tree.node_start)).cpu().numpy()
+    monkeypatch.setattr(flat_tree, "DOWNWARD_LEAVES", True)
+    one = [_np(t)[leaves] for t in tree._log_locals(lists)]
+    monkeypatch.setattr(flat_tree, "DOWNWARD_LEAVES", False)
+    levels = [_np(t)[leaves] for t in tree._log_locals(lists)]
+    for a, b in zip(one, levels):
+        assert relative(a, b) < 1e-13

@@ -143,6 +143,7 @@ def test_tensor_core_m2l_matches_cuda_core_m2l_and_fp64(order, monkeypatch):
     (fixed summation order per destination)."""
     from tree_d_3d_b200 import FlatQuadtree, Quad, flat_tree, synthetic
 
+    monkeypatch.setattr(flat_tree, "M2L_GROUPED", False)  # the per-translation forms
     pos, q = synthetic.mixture8(150_000, seed=40 + order)
     P, Q = torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda")
     ref = FlatQuadtree(P, Q, Quad(0, 0, 1), kernel="log", order=order)
@@ -161,3 +162,21 @@ def test_tensor_core_m2l_matches_cuda_core_m2l_and_fp64(order, monkeypatch):
         assert relative(runs[True][part], fp64[part]) < 1e-6
         assert relative(runs[True][part], runs[False][part]) < 1e-6
         assert np.array_equal(again[part], runs[True][part])
+
+
+@pytest.mark.parametrize("order", [4, 8, 12, 16])
+def test_mixed_cartesian_m2l_matches_fp64(order):
+    """The FP32 Cartesian M2L on size-scaled expansions (td3_cart_m2l_mixed) against the
+    FP64 one on the same lists and moments: the locals to FP32 accuracy."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, synthetic
+
+    pos, q = synthetic.mixture8(120_000, seed=50 + order)
+    P, Q = torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda")
+    out = {}
+    for precision in ("fp64", "mixed"):
+        tree = FlatQuadtree(P, Q, Quad(0, 0, 1), kernel="coulomb", order=order,
+                            precision=precision)
+        lists = tree._lists(0.5)
+        out[precision] = tree._cart_locals(lists["m2l_rows"], lists["m2l_partners"],
+                                           lists["m2l"].shape[0], tree, 1e-3).cpu().numpy()
+    assert relative(out["mixed"], out["fp64"]) < TOL

@@ -182,6 +182,133 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
     }
 }
 
+// The mixed-precision form of k_m2l_cart_lanes: the same partners-by-eight layout in
+// FP32 on expansions scaled by the source cell's half-width h_s.  With t' = t / h_s,
+// eps' = eps / h_s and m'_a = m_a / h_s^|a|, A_g(t; eps) = h_s^(-1-|g|) A_g(t'; eps'),
+// so T_b = (1 / b!) h_d^(-1-|b|) sum_partners (h_d / h_s)^(1+|b|) S'_b with
+// S'_b = sum_a m~'_a A~'_(a+b) (every FP32 quantity O(1); h_d / h_s a power of two,
+// applied exactly), summed per destination in FP32 and added to the FP64 locals with
+// the factor h_d^(-1-|b|) / b! in FP64.
+template <int P>
+__global__ void __launch_bounds__(32 * CM2L_WARPS)
+k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ partners,
+                 i64 n_dst, const double* __restrict__ dst_center,
+                 const double* __restrict__ dst_half, const double* __restrict__ src_center,
+                 const double* __restrict__ src_half, const double* __restrict__ moments,
+                 int order, double eps2, const CartScale C, double* __restrict__ local) {
+    constexpr int W = P + 1;
+    extern __shared__ float cart_smem_f[];
+    td3_chain_wait();
+    td3_chain_release();
+    int n_coef = (order + 1) * (order + 2) / 2;
+    int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int p = lane & (CART_GROUP - 1), q = lane >> 3;
+    float* At = cart_smem_f + (size_t)wib * (2 * CART_GROUP + 1) * n_coef;
+    float* Mt = At + CART_GROUP * n_coef;
+    float* T = Mt + CART_GROUP * n_coef;
+    for (i64 dst = (i64)blockIdx.x * CM2L_WARPS + wib; dst < n_dst;
+         dst += (i64)gridDim.x * CM2L_WARPS) {
+        i64 e0 = row_start[dst], e1 = row_start[dst + 1];
+        if (e0 == e1) continue;
+        double cx = dst_center[2 * dst], cy = dst_center[2 * dst + 1], hd = dst_half[dst];
+        for (int b = lane; b < n_coef; b += 32) T[b] = 0.0f;
+        for (i64 base = e0; base < e1; base += CART_GROUP) {
+            __syncwarp();
+            bool live = base + p < e1;
+            i64 src = live ? partners[base + p] : 0;
+            double hs = src_half[src];
+            // h_d / h_s = 2^dl exactly
+            int dl;
+            frexp(hd / hs, &dl);
+            dl -= 1;
+            if (lane < CART_GROUP) {
+                double inv_h = 1.0 / hs;
+                float tx = (float)((cx - src_center[2 * src]) * inv_h);
+                float ty = (float)((cy - src_center[2 * src + 1]) * inv_h);
+                float r2 = live ? (float)((double)tx * tx + (double)ty * ty + eps2 * inv_h * inv_h)
+                                : 1.0f;
+                float prev2[W], prev1[W], cur[W];
+                prev1[0] = live ? rsqrtf(r2) : 0.0f;
+                At[p] = prev1[0];
+                float inv_r2 = 1.0f / r2;
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    if (n > order) break;
+                    float scale = -inv_r2 / n;
+#pragma unroll
+                    for (int gy = 0; gy <= n; ++gy) {
+                        int gx = n - gy;
+                        float s = 0.0f;
+                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy];
+                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[gy - 1];
+                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy];
+                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[gy - 2];
+                        cur[gy] = s * scale;
+                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = cur[gy];
+                    }
+#pragma unroll
+                    for (int k = 0; k < W; ++k) {
+                        prev2[k] = prev1[k];
+                        prev1[k] = cur[k];
+                    }
+                }
+            } else if (lane < 2 * CART_GROUP) {
+                const double* m = moments + src * n_coef;
+                double inv_h = 1.0 / hs, pw = 1.0;
+                for (int n = 0, a = 0; n <= order; ++n, pw *= inv_h) {
+                    for (int y = 0; y <= n; ++y, ++a) {
+                        double v = live ? m[a] * C.inv_fact2[a] * pw : 0.0;
+                        Mt[a * CART_GROUP + p] = (float)((n & 1) ? -v : v);
+                    }
+                }
+            }
+            __syncwarp();
+            for (int j0 = 0; j0 < n_coef; j0 += 4) {
+                int b = j0 + q;
+                float acc = 0.0f;
+                if (b < n_coef) {
+                    int bx = C.bx[b], by = C.by[b], nb = bx + by;
+                    for (int na = 0; na + nb <= order; ++na) {
+                        int ng = na + nb;
+                        const float* mrow = Mt + (na * (na + 1) / 2) * CART_GROUP + p;
+                        const float* grow = At + (ng * (ng + 1) / 2 + by) * CART_GROUP + p;
+                        for (int ay = 0; ay <= na; ++ay)
+                            acc += mrow[ay * CART_GROUP] * grow[ay * CART_GROUP];
+                    }
+                    acc = ldexpf(acc, dl * (1 + nb));
+                }
+                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
+                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
+                if (p == 0 && b < n_coef) T[b] += acc;
+            }
+        }
+        __syncwarp();
+        double inv_hd = 1.0 / hd;
+        for (int b = lane; b < n_coef; b += 32) {
+            int nb = C.bx[b] + C.by[b];
+            double scale = inv_hd;
+            for (int k = 0; k < nb; ++k) scale *= inv_hd;
+            local[dst * n_coef + b] += (double)T[b] * C.inv_fact2[b] * scale;
+        }
+    }
+}
+
+CartScale cart_scale(int order) {
+    CartScale C{};
+    double f[CART_LANE_MAX + 1];
+    f[0] = 1.0;
+    for (int k = 1; k <= CART_LANE_MAX; ++k) f[k] = f[k - 1] * k;
+    for (int n = 0; n <= order; ++n)
+        for (int y = 0; y <= n; ++y) {
+            int i = n * (n + 1) / 2 + y;
+            C.bx[i] = (short)(n - y);
+            C.by[i] = (short)y;
+            C.inv_fact2[i] = 1.0 / (f[n - y] * f[y]);
+        }
+    return C;
+}
+
 // L2L of one level: a block per (node, child), thread b: T_b(child) += sum_g C(g, b) T_g
 // s^(g-b) over the rows of b (g, d = g - b, coef).  The monomials s^d are built once per
 // block into shared memory, column d_y by thread d_y as the reference's mono recurrence
@@ -289,4 +416,31 @@ extern "C" int td3_cart_downward(const int64_t* levels, int64_t n_levels, const 
     }
     TD3_CHECK_LAUNCH();
     return TD3_OK;
+}
+
+extern "C" int td3_cart_m2l_mixed(const int64_t* row_start, const int64_t* partners,
+                                  int64_t n_dst, const double* dst_center,
+                                  const double* dst_half, const double* src_center,
+                                  const double* src_half, const double* moments, int order,
+                                  double softening, double* local, void* stream) {
+    if (n_dst < 0 || order < 0 || order > CART_LANE_MAX) return TD3_EINVAL;
+    if (n_dst == 0) return TD3_OK;
+    cudaStream_t s = td3_stream(stream);
+    int n_coef = (order + 1) * (order + 2) / 2;
+    CartScale C = cart_scale(order);
+    size_t smem = sizeof(float) * (2 * CART_GROUP + 1) * n_coef * CM2L_WARPS;
+    i64 nb = (n_dst + CM2L_WARPS - 1) / CM2L_WARPS;
+    unsigned grid = (unsigned)(nb < 148 * 64 ? nb : 148 * 64);
+    auto run = [&](auto kernel) -> int {
+        TD3_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)smem));
+        TD3_TRY(td3_launch_chained(kernel, grid, 32 * CM2L_WARPS, smem, s, row_start, partners,
+                                   n_dst, dst_center, dst_half, src_center, src_half, moments,
+                                   order, softening * softening, C, local));
+        return TD3_OK;
+    };
+    if (order <= 4) return run(k_m2l_cart_mixed<4>);
+    if (order <= 8) return run(k_m2l_cart_mixed<8>);
+    if (order <= 12) return run(k_m2l_cart_mixed<12>);
+    return run(k_m2l_cart_mixed<16>);
 }

@@ -151,6 +151,53 @@ __global__ void k_l2l_log_level(i64 lo, i64 hi, int order, const double* __restr
     local_im[ch * w + m] += acc_im;
 }
 
+// The downward pass in one launch: the local expansion of every non-empty leaf is its
+// own M2L local plus the own M2L local of each of its ancestors shifted straight to the
+// leaf's centre, b_m(leaf) += sum_{l>=m} C(l, m) b_l(a) s^(l-m), s = c_leaf - c_a.  The
+// shift re-expands a polynomial exactly, so the sum equals the level-by-level L2L of the
+// reference (K/fmm_downward/fmm_downward_pyccel.py:15-64) up to rounding; internal
+// cells keep their own M2L locals (L2P reads leaves only).  A warp per node (non-leaves
+// and empty leaves leave at once), a lane per coefficient m; the ancestors in order
+// from the parent up, a fixed order per leaf.
+__global__ void k_l2l_leaves(i64 count, int order, const double* __restrict__ center,
+                             const int* __restrict__ parent, const i64* __restrict__ start,
+                             const i64* __restrict__ end, const i64* __restrict__ child,
+                             const double* __restrict__ binomial, int bsize,
+                             double* __restrict__ local_re, double* __restrict__ local_im) {
+    const int lane = threadIdx.x & 31;
+    const int w = order + 1;
+    const i64 warps = (i64)gridDim.x * (blockDim.x >> 5);
+    for (i64 leaf = (i64)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); leaf < count;
+         leaf += warps) {
+        if (child[leaf] >= 0 || end[leaf] == start[leaf]) continue;
+        const double cx = center[2 * leaf], cy = center[2 * leaf + 1];
+        for (int m0 = 0; m0 < w; m0 += 32) {
+            const int m = m0 + lane;
+            double acc_re = 0.0, acc_im = 0.0;
+            for (int a = parent[leaf]; a >= 0; a = parent[a]) {
+                if (m >= w) continue;
+                double s_re = cx - center[2 * a], s_im = cy - center[2 * a + 1];
+                double p_re = 1.0, p_im = 0.0;
+                const double* bre = local_re + (i64)a * w;
+                const double* bim = local_im + (i64)a * w;
+                for (int l = m; l <= order; ++l) {
+                    double cb = binomial[l * bsize + m];
+                    double b_re = bre[l] * cb, b_im = bim[l] * cb;
+                    acc_re += b_re * p_re - b_im * p_im;
+                    acc_im += b_re * p_im + b_im * p_re;
+                    double nr = p_re * s_re - p_im * s_im;
+                    p_im = p_re * s_im + p_im * s_re;
+                    p_re = nr;
+                }
+            }
+            if (m < w) {
+                local_re[leaf * w + m] += acc_re;
+                local_im[leaf * w + m] += acc_im;
+            }
+        }
+    }
+}
+
 __global__ void k_node_parents(i64 count, const i64* __restrict__ node_child,
                                int* __restrict__ parent) {
     i64 p = (i64)blockIdx.x * blockDim.x + threadIdx.x;
@@ -405,6 +452,24 @@ extern "C" int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const d
                                    order, node_center, node_parent, node_start, node_end,
                                    binomial, binomial_size, local_re, local_im));
     }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+extern "C" int td3_fmm_downward_leaves(int64_t count, int order, const double* node_center,
+                                       const int32_t* node_parent, const int64_t* node_start,
+                                       const int64_t* node_end, const int64_t* node_child,
+                                       const double* binomial, int binomial_size,
+                                       double* local_re, double* local_im, void* stream) {
+    if (count < 1 || count > 0x7fffffffLL || order < 0 || order > TD3_MAX_ORDER ||
+        binomial_size < order + 1)
+        return TD3_EINVAL;
+    constexpr int threads = 256;
+    i64 blocks = (count + threads / 32 - 1) / (threads / 32);
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    k_l2l_leaves<<<(unsigned)blocks, threads, 0, td3_stream(stream)>>>(
+        count, order, node_center, node_parent, node_start, node_end, node_child, binomial,
+        binomial_size, local_re, local_im);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }

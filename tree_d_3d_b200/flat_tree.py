@@ -10,6 +10,9 @@ give CUDA tensor results; NumPy or list inputs give NumPy results.
 
 from __future__ import annotations
 
+import math
+import weakref
+
 import numpy as np
 import torch
 
@@ -177,6 +180,39 @@ NEAR_SEGMENT = 256
 #: to 15) instead of FP32 CUDA-core arithmetic.  Off by default: the tensor-core form is
 #: correct but, waiting on each 128-row tile, still slower than the CUDA-core form.
 M2L_TENSOR_CORES = False
+
+#: the log kernel's downward pass in one launch (each leaf's local from its ancestors'
+#: own locals) instead of one L2L launch per level
+DOWNWARD_LEAVES = True
+
+#: the mixed-precision M2L of ``fmm`` (mutual lists, log kernel, orders up to 14) as
+#: tensor-core products grouped by translation (td3_m2l_groups, td3_fmm_m2l_grouped)
+M2L_GROUPED = True
+#: keep the grouped products' A operand in shared memory instead of tensor memory
+M2L_GROUPED_SMEM = False
+
+
+def _group_span(theta: float) -> int:
+    """Offsets (in units of the smaller half-width) covered by the grouped M2L's
+    operator table: the lists of ``theta`` reach about 4.5 / theta; rarer, farther
+    translations take the per-translation formula."""
+    return int(min(max(math.ceil(5.5 / theta), 8), 24))
+
+
+class _Lists(dict):
+    """The interaction lists of one theta.  The CSR rows of the M2L list are made on
+    first use: the grouped tensor-core M2L of the mixed form reads its own order."""
+
+    def __init__(self, tree, **items):
+        super().__init__(**items)
+        self._tree = weakref.ref(tree)
+
+    def __missing__(self, key):
+        if key in ("m2l_rows", "m2l_partners", "m2l_entry_row") and "m2l" in self:
+            rows, partners, entry = self._tree()._rows(self["m2l"], mutual=True, entry_rows=True)
+            self.update(m2l_rows=rows, m2l_partners=partners, m2l_entry_row=entry)
+            return dict.__getitem__(self, key)
+        raise KeyError(key)
 
 
 def _nearfield_plan(rows: torch.Tensor, tree, entries: int) -> dict:
@@ -575,17 +611,74 @@ class FlatQuadtree:
         return self._traversals[theta]
 
     def _new_lists(self, theta: float) -> dict:
-        """The mutual lists of ``theta`` (ft:1318-1358), their CSR rows and the
-        near-field plan."""
+        """The mutual lists of ``theta`` (ft:1318-1358), the M2L translations in the
+        order their M2L reads (CSR rows by destination, or the grouped order of the
+        tensor-core form) and the near-field rows and plan."""
         m2l, p2p = self._traverse(theta)
-        m2l_rows, m2l_partners, m2l_entry = self._rows(m2l, mutual=True, entry_rows=True)
+        lists = _Lists(self, m2l=m2l, p2p=p2p)
+        if self._grouped_m2l():
+            lists["groups"] = self._m2l_groups(m2l, theta)
+        else:
+            lists["m2l_rows"]  # the CSR rows, made now
         p2p_rows, p2p_partners = self._rows(p2p, mutual=True)
-        lists = {
-            "m2l": m2l, "p2p": p2p, "m2l_rows": m2l_rows, "m2l_partners": m2l_partners,
-            "m2l_entry_row": m2l_entry, "p2p_rows": p2p_rows, "p2p_partners": p2p_partners,
-        }
+        lists.update(p2p_rows=p2p_rows, p2p_partners=p2p_partners)
         lists["plan"] = _nearfield_plan(p2p_rows, self, 2 * p2p.shape[0])
         return lists
+
+    def _grouped_m2l(self) -> bool:
+        """Whether this tree's fmm takes the grouped tensor-core M2L."""
+        return (M2L_GROUPED and self.kernel == "log" and self.precision == "mixed"
+                and self.order <= 14 and self.node_count < (1 << 25)
+                and 1 <= len(self.levels) - 1 <= 64)
+
+    def _m2l_groups(self, m2l: torch.Tensor, theta: float) -> dict:
+        """The directed translations of the mutual M2L list sorted by (tile of 128
+        destinations, operator key), with the runs and tiles of that order
+        (td3_m2l_groups)."""
+        dev = self.device
+        n_pairs = int(m2l.shape[0])
+        e = 2 * n_pairs
+        n_tiles = (self.node_count + 127) // 128
+        span = _group_span(theta)
+        keys = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
+        vals = torch.empty(max(e, 1), dtype=torch.int32, device=dev)
+        tile_run = torch.empty(n_tiles + 1, dtype=torch.int32, device=dev)
+        run_start = torch.empty(e + 1, dtype=torch.int32, device=dev)
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        ws = _lib.workspace(_lib.query("td3_m2l_groups_workspace_size", n_pairs), dev)
+        _lib.call("td3_m2l_groups", m2l.data_ptr(), n_pairs, self.node_center.data_ptr(),
+                  self.node_half.data_ptr(), self.node_depth.data_ptr(), levels.ctypes.data,
+                  len(levels) - 1, self.node_count, span, keys.data_ptr(), vals.data_ptr(),
+                  tile_run.data_ptr(), run_start.data_ptr(), ws.data_ptr(), ws.numel(),
+                  _lib.stream(dev))
+        return {"keys": keys, "vals": vals, "tile_run": tile_run, "run_start": run_start,
+                "span": span}
+
+    def _m2l_operators(self, span: int) -> torch.Tensor:
+        """The grouped M2L's operator table for this order (td3_m2l_operators), made
+        once per device."""
+        key = (("m2l_ops", self.order, self.symmetric, span), self.device)
+        if key not in _TABLES:
+            nbytes = _lib.query("td3_m2l_operators_size", span)
+            ops = torch.empty(nbytes // 4, dtype=torch.float32, device=self.device)
+            _lib.call("td3_m2l_operators", self.order, self._m2l_matrix().data_ptr(), span,
+                      ops.data_ptr(), _lib.stream(self.device))
+            _TABLES[key] = ops
+        return _TABLES[key]
+
+    def _m2l_grouped(self, groups: dict, hat: torch.Tensor, local_re, local_im) -> None:
+        """The grouped tensor-core M2L (td3_fmm_m2l_grouped) into the locals."""
+        span = groups["span"]
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
+        _lib.call("td3_fmm_m2l_grouped", groups["tile_run"].data_ptr(),
+                  groups["run_start"].data_ptr(), groups["keys"].data_ptr(),
+                  groups["vals"].data_ptr(), self.node_count, levels.ctypes.data,
+                  len(levels) - 1, self.node_center.data_ptr(), self.node_half.data_ptr(),
+                  hat.data_ptr(), self.order, self._m2l_operators(span).data_ptr(), span,
+                  coeff.ctypes.data, 1 if M2L_GROUPED_SMEM else 0, local_re.data_ptr(),
+                  local_im.data_ptr(), self._tensor_status().data_ptr(),
+                  _lib.stream(self.device))
 
     def _m2l_matrix(self) -> torch.Tensor:
         key = ("m2l_coefficients", self.order, self.symmetric)
@@ -651,8 +744,17 @@ class FlatQuadtree:
         return self._node_parent
 
     def _downward(self, local_re, local_im, order, binom) -> None:
-        """L2L of complex locals of ``order`` from the root down this tree
-        (td3_fmm_downward; ``binom`` the binomial table)."""
+        """L2L of complex locals of ``order`` from the root down this tree (``binom`` the
+        binomial table): in one launch, every leaf's local from its ancestors' own
+        locals (td3_fmm_downward_leaves; internal cells keep their own M2L locals), or
+        level by level as the reference (td3_fmm_downward) with DOWNWARD_LEAVES off."""
+        if DOWNWARD_LEAVES:
+            _lib.call("td3_fmm_downward_leaves", self.node_count, order,
+                      self.node_center.data_ptr(), self._parents().data_ptr(),
+                      self.node_start.data_ptr(), self.node_end.data_ptr(),
+                      self.node_child.data_ptr(), binom.data_ptr(), binom.shape[0],
+                      local_re.data_ptr(), local_im.data_ptr(), _lib.stream(self.device))
+            return
         levels = np.ascontiguousarray(self.levels, dtype=np.int64)
         _lib.call("td3_fmm_downward", levels.ctypes.data, len(levels) - 1,
                   self.node_center.data_ptr(), self._parents().data_ptr(),
@@ -717,9 +819,13 @@ class FlatQuadtree:
         for orders up to 15 (M2L_TENSOR_CORES)."""
         stream = _lib.stream(self.device)
         mre, mim = moments
-        rows, partners = lists["m2l_rows"], lists["m2l_partners"]
         if self.precision == "mixed" and self.order <= 20:
             hat = self._scaled_moments(moments)
+            groups = lists.get("groups") if dst is self else None
+            if groups is not None:
+                self._m2l_grouped(groups, hat, local_re, local_im)
+                return
+            rows, partners = lists["m2l_rows"], lists["m2l_partners"]
             coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
             tensor = 1 if M2L_TENSOR_CORES and self.order <= 15 else 0
             _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), lists["m2l_entry_row"].data_ptr(),
@@ -730,6 +836,7 @@ class FlatQuadtree:
                       local_im.data_ptr(), self._tensor_status().data_ptr() if tensor else 0,
                       stream)
             return
+        rows, partners = lists["m2l_rows"], lists["m2l_partners"]
         _lib.call("td3_fmm_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                   dst.node_center.data_ptr(), self.node_center.data_ptr(), mre.data_ptr(),
                   mim.data_ptr(), self.order, self._m2l_matrix().data_ptr(), local_re.data_ptr(),
@@ -939,7 +1046,8 @@ class FlatQuadtree:
 
     def _cart_locals(self, rows, partners, n_m2l, dst, softening, moments=None):
         """Cartesian M2L from this tree's cells into the cells of ``dst`` (this tree for
-        fmm, the target tree for fmm_at), then L2L down ``dst`` (ft:1371-1396)."""
+        fmm, the target tree for fmm_at), then L2L down ``dst`` (ft:1371-1396); the M2L
+        in FP32 on size-scaled expansions for ``precision="mixed"`` (orders up to 16)."""
         from tree_d_3d_b200 import _cartesian
 
         t = self._cartesian_tables()
@@ -948,7 +1056,12 @@ class FlatQuadtree:
         if moments is None:
             moments = self._cartesian_moments()
         local = torch.zeros((dst.node_count, n_coef), dtype=torch.float64, device=self.device)
-        if n_m2l:
+        if n_m2l and self.precision == "mixed" and self.order <= 16:
+            _lib.call("td3_cart_m2l_mixed", rows.data_ptr(), partners.data_ptr(), dst.node_count,
+                      dst.node_center.data_ptr(), dst.node_half.data_ptr(),
+                      self.node_center.data_ptr(), self.node_half.data_ptr(),
+                      moments.data_ptr(), self.order, float(softening), local.data_ptr(), stream)
+        elif n_m2l:
             _lib.call("td3_cart_m2l", rows.data_ptr(), partners.data_ptr(), dst.node_count,
                       dst.node_center.data_ptr(), self.node_center.data_ptr(),
                       moments.data_ptr(), self.order, float(softening),
