@@ -65,6 +65,10 @@ def _args():
                         "the headline line")
     p.add_argument("--trace-only", action="store_true",
                    help="timed mixed steps only (no e2e, FP64 arm, counts or errors): for ncu")
+    p.add_argument("--kernel", choices=("log", "coulomb"), default="log",
+                   help="the kernel of the --trace-only steps (the headline is the log kernel)")
+    p.add_argument("--precision", choices=("mixed", "fp64"), default="mixed",
+                   help="the precision of the --trace-only steps")
     return p.parse_args()
 
 
@@ -245,15 +249,20 @@ def max_over_ranks(value: float, dist, device) -> float:
     return float(t.item())
 
 
-def gpu_step(pos, q, w, e, precision, backward=True):
+#: the Coulomb kernel's softening in its workload line (config 3)
+COULOMB_SOFTENING = 1e-3
+
+
+def gpu_step(pos, q, w, e, precision, backward=True, kernel="log"):
     """One step: a fresh tree, the FMM field at every particle and its backward."""
     from tree_d_3d_b200 import Quad
     from tree_d_3d_b200.autograd import fmm_field
 
     p = pos.detach().requires_grad_(backward)
     c = q.detach().requires_grad_(backward)
-    phi, field = fmm_field(p, c, Quad(0.0, 0.0, 1.0), kernel="log", order=ORDER, theta=THETA,
-                           softening=SOFTENING, leaf_capacity=LEAF, precision=precision)
+    eps = SOFTENING if kernel == "log" else COULOMB_SOFTENING
+    phi, field = fmm_field(p, c, Quad(0.0, 0.0, 1.0), kernel=kernel, order=ORDER, theta=THETA,
+                           softening=eps, leaf_capacity=LEAF, precision=precision)
     if backward:
         ((w * phi).sum() + (e * field).sum()).backward()
     return phi.detach(), field.detach(), p.grad, c.grad
@@ -345,16 +354,17 @@ def _peaks():
         return 1590.0, "of fallback (1.59 PFLOP/s bf16, no MEASURED_PEAKS.json)"
 
 
-def field_error(pos, q, precision, torch, n_sample=4096):
+def field_error(pos, q, precision, torch, n_sample=4096, kernel="log"):
     """Normwise relative field error against the FP64 direct sum on sampled particles."""
     from tree_d_3d_b200 import FlatQuadtree, Quad, direct_field
 
-    tree = FlatQuadtree(pos, q, Quad(0.0, 0.0, 1.0), kernel="log", order=ORDER,
+    eps = SOFTENING if kernel == "log" else COULOMB_SOFTENING
+    tree = FlatQuadtree(pos, q, Quad(0.0, 0.0, 1.0), kernel=kernel, order=ORDER,
                         leaf_capacity=LEAF, precision=precision)
-    _, field = tree.fmm(theta=THETA, softening=SOFTENING)
+    _, field = tree.fmm(theta=THETA, softening=eps)
     idx = torch.tensor(np.random.default_rng(0).choice(pos.shape[1], n_sample, replace=False),
                        device=pos.device)
-    _, ref = direct_field(pos[:, idx], pos, q, softening=SOFTENING, exclude=idx, kernel="log")
+    _, ref = direct_field(pos[:, idx], pos, q, softening=eps, exclude=idx, kernel=kernel)
     diff = (field[:, idx] - ref).abs().max() / ref.abs().max()
     return float(diff), tree
 
@@ -387,14 +397,18 @@ def run_ours(args):
     e = torch.tensor(e_np, device=dev)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
 
+    kernel, precision = ("log", "mixed")
+    if args.trace_only:
+        kernel, precision = args.kernel, args.precision
     for _ in range(args.warmup):
-        gpu_step(pos, q, w, e, "mixed")
+        gpu_step(pos, q, w, e, precision, kernel=kernel)
     torch.cuda.synchronize()
     if dist:
         dist.barrier()
     with ClockSampler(local) as clocks:
         torch.cuda.synchronize()
-        total_ms = time_steps(lambda: gpu_step(pos, q, w, e, "mixed"), args.steps, flush, torch)
+        total_ms = time_steps(lambda: gpu_step(pos, q, w, e, precision, kernel=kernel),
+                              args.steps, flush, torch)
         torch.cuda.synchronize()
     if dist:
         dist.barrier()
@@ -419,6 +433,18 @@ def run_ours(args):
     fwd_fp64 = time_steps(lambda: gpu_step(pos, q, w, e, "fp64", backward=False), 3, flush,
                           torch) / 3
 
+    # the same step with the Coulomb kernel (config 3's kernel; softening 1e-3): mixed and
+    # FP64, and the mixed field error against the FP64 direct sum
+    coulomb = {}
+    for prec in ("mixed", "fp64"):
+        gpu_step(pos, q, w, e, prec, kernel="coulomb")
+        reps = 3
+        c_ms = max_over_ranks(time_steps(lambda: gpu_step(pos, q, w, e, prec, kernel="coulomb"),
+                                         reps, flush, torch), dist, dev) / reps
+        coulomb[prec] = {"ms_per_step": c_ms, "value": world * n / (c_ms / 1e3)}
+    coulomb["speedup_mixed_over_fp64"] = coulomb["mixed"]["value"] / coulomb["fp64"]["value"]
+    coulomb["softening"] = COULOMB_SOFTENING
+
     # end to end through the public API: pinned host inputs in, host results out
     pos_h, q_h = torch.tensor(pos_np).pin_memory(), torch.tensor(q_np).pin_memory()
     w_h, e_h = torch.tensor(w_np).pin_memory(), torch.tensor(e_np).pin_memory()
@@ -441,6 +467,8 @@ def run_ours(args):
     launches = count_our_launches(lambda: gpu_step(pos, q, w, e, "mixed"), torch)
     err_mixed, tree = field_error(pos, q, "mixed", torch)
     err_fp64, _ = field_error(pos, q, "fp64", torch)
+    for prec in ("mixed", "fp64"):
+        coulomb[prec]["rel_err_field"], _ = field_error(pos, q, prec, torch, kernel="coulomb")
     # the step's M2L form (tensor-core products grouped by translation); the FP32 CUDA-core
     # form and the per-translation tensor-core form are timed beside it
     m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, form="grouped")
@@ -499,6 +527,7 @@ def run_ours(args):
                  "rel_err_field": err_fp64},
         "rel_err_field": err_mixed,
         "forward_only_ms": {"mixed": fwd_mixed, "fp64": fwd_fp64},
+        "coulomb": coulomb,
         "e2e": {"value": e2e_value, "unit": "particles/s",
                 "h2d_bytes_per_step": 8 * n * (2 + 1 + 1 + 2),
                 "d2h_bytes_per_step": 8 * n * (1 + 2 + 2 + 1)},

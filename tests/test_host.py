@@ -65,7 +65,8 @@ def test_validation_messages_match_the_reference():
         FlatQuadtree([[0.0], [0.0]], [1.0], Quad(0, 0, 0))
     with pytest.raises(ValueError, match="leaf_capacity must be a positive integer"):
         FlatQuadtree([[0.0], [0.0]], [1.0], Quad(0, 0, 1), leaf_capacity=0)
-    with pytest.raises(NotImplementedError, match="comm"):
+    # comm is a torch.distributed process group; without an initialised group it is refused
+    with pytest.raises(ValueError, match="comm must be a torch.distributed process group"):
         FlatQuadtree([[0.0], [0.0]], [1.0], Quad(0, 0, 1), comm=object())
     with pytest.raises(ValueError, match="kernel must be one of"):
         direct_field([[0.0], [0.0]], [[0.0], [0.0]], [1.0], kernel="yukawa")
@@ -163,3 +164,17 @@ def test_trace_regions_follow_the_reference_names_and_are_off_by_default():
     finally:
         _trace.enable(was)
         _trace.opened.clear()
+
+
+def test_panel_tree_root_is_the_widened_bounding_square():
+    """electrodes.py:1143-1146: centre of the bounding box, half the larger side times
+    (1 + 1e-9) plus 1e-300."""
+    import torch
+
+    from tree_d_3d_b200.electrodes import FMM_AT_RATIO, FMM_AT_THETA, WALK_THETA, bounding_quad
+
+    pts = torch.tensor([[-0.5, 0.25, 0.75], [0.1, -0.3, 0.2]], dtype=torch.float64)
+    q = bounding_quad(pts)
+    assert (q.xmid, q.ymid) == (0.125, -0.04999999999999999)
+    assert q.half == 0.5 * 1.25 * (1 + 1e-9) + 1e-300
+    assert (FMM_AT_THETA, FMM_AT_RATIO, WALK_THETA) == (0.5, 8, 0.7)

@@ -16,7 +16,7 @@ import weakref
 import numpy as np
 import torch
 
-from tree_d_3d_b200 import _lib
+from tree_d_3d_b200 import _lib, _shards
 from tree_d_3d_b200._trace import profile, region
 from tree_d_3d_b200._utils import (
     _check,
@@ -215,10 +215,11 @@ class _Lists(dict):
         raise KeyError(key)
 
 
-def _nearfield_plan(rows: torch.Tensor, tree, entries: int) -> dict:
+def _nearfield_plan(rows: torch.Tensor, tree, entries: int, end: torch.Tensor | None = None) -> dict:
     """The near-field work plan of one tree's leaf rows (td3_nearfield_plan): leaf rows
     cut into segments of at most NEAR_SEGMENT partners, and the partial-sum buffer of
-    the rows that take several segments.  ``entries`` bounds the rows' partner count."""
+    the rows that take several segments.  ``entries`` bounds the rows' partner count;
+    ``end`` (default the tree's node_end) set to node_start leaves a leaf out."""
     dev = rows.device
     n_nodes = rows.shape[0] - 1
     capacity = n_nodes + entries // NEAR_SEGMENT + 1
@@ -227,8 +228,9 @@ def _nearfield_plan(rows: torch.Tensor, tree, entries: int) -> dict:
     seg_out = torch.empty(capacity, dtype=torch.int64, device=dev)
     sizes = np.zeros(2, dtype=np.int64)
     ws = _lib.workspace(_lib.query("td3_nearfield_plan_workspace_size", n_nodes), dev)
+    end = tree.node_end if end is None else end
     _lib.call("td3_nearfield_plan", rows.data_ptr(), n_nodes, tree.node_child.data_ptr(),
-              tree.node_start.data_ptr(), tree.node_end.data_ptr(), NEAR_SEGMENT,
+              tree.node_start.data_ptr(), end.data_ptr(), NEAR_SEGMENT,
               seg_leaf.data_ptr(), seg_range.data_ptr(), seg_out.data_ptr(), capacity,
               sizes.ctypes.data, ws.data_ptr(), ws.numel(), _lib.stream(dev))
     n_seg = int(sizes[0])
@@ -273,12 +275,18 @@ class FlatQuadtree:
         if order > MAX_ORDER:
             raise ValueError(f"order must be at most {MAX_ORDER}, got {order}")
         if comm is not None:
-            raise NotImplementedError("comm: the GPU tree runs on one device (comm=None)")
+            import torch.distributed as dist
+
+            if not (dist.is_available() and dist.is_initialized()):
+                raise ValueError("comm must be a torch.distributed process group (the ranks "
+                                 "that share the FMM), with the default group initialised")
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
         self.kernel = kernel
         self.order = int(order)
-        self.comm = None
+        #: the process group whose ranks share the FMM's work (None: one process)
+        self.comm = comm if compiled else None
+        self._rank, self._world = (0, 1) if self.comm is None else _shards.rank_and_world(comm)
         self.symmetric = bool(symmetric)
         self.precision = precision
         self._compiled = bool(compiled)
@@ -300,6 +308,7 @@ class FlatQuadtree:
         self.max_depth = int(max_depth)
         self.root_quad = Quad(float(root_quad.xmid), float(root_quad.ymid), float(root_quad.half))
         self._traversals: dict = {}
+        self._shard_cache: dict = {}
         self._cart_moments = None
         self._plans: dict = {}
         if not n:
@@ -707,6 +716,9 @@ class FlatQuadtree:
         field = torch.zeros((2, n), dtype=torch.float64, device=dev)
         if not n:
             return out((phi, field), self._numpy)
+        if self._world > 1:
+            self._fmm_sharded(theta, softening, potential, phi, field)
+            return out((phi, field), self._numpy)
         if self.kernel != "log":
             self._coulomb_fmm(theta, softening, phi, field, _status)
             return out((phi, field), self._numpy)
@@ -722,9 +734,10 @@ class FlatQuadtree:
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
         return out((phi, field), self._numpy)
 
-    def _log_locals(self, lists: dict, moments=None):
+    def _log_locals(self, lists: dict, moments=None, downward: bool = True):
         """M2L into every cell's local expansion, then L2L down the tree (``moments``:
-        (moment_re, moment_im), by default the tree's own)."""
+        (moment_re, moment_im), by default the tree's own; ``downward=False`` stops
+        after the M2L)."""
         dev, count, w = self.device, self.node_count, self.order + 1
         mre, mim = moments if moments is not None else (self.moment_re, self.moment_im)
         local_re = torch.zeros((count, w), dtype=torch.float64, device=dev)
@@ -732,7 +745,8 @@ class FlatQuadtree:
         stream = _lib.stream(dev)
         if lists["m2l"].shape[0]:
             self._m2l_log(lists, self, (mre, mim), local_re, local_im)
-        self._downward(local_re, local_im, self.order, self._binomial())
+        if downward:
+            self._downward(local_re, local_im, self.order, self._binomial())
         return local_re, local_im
 
     def _parents(self) -> torch.Tensor:
@@ -1044,7 +1058,8 @@ class FlatQuadtree:
             phi.zero_()
         return out((phi, field), as_numpy)
 
-    def _cart_locals(self, rows, partners, n_m2l, dst, softening, moments=None):
+    def _cart_locals(self, rows, partners, n_m2l, dst, softening, moments=None,
+                     downward: bool = True):
         """Cartesian M2L from this tree's cells into the cells of ``dst`` (this tree for
         fmm, the target tree for fmm_at), then L2L down ``dst`` (ft:1371-1396); the M2L
         in FP32 on size-scaled expansions for ``precision="mixed"`` (orders up to 16)."""
@@ -1067,13 +1082,97 @@ class FlatQuadtree:
                       moments.data_ptr(), self.order, float(softening),
                       t["m2l_a"].data_ptr(), t["m2l_g"].data_ptr(), t["m2l_coef"].data_ptr(),
                       t["m2l_start32"].data_ptr(), local.data_ptr(), stream)
+        if downward:
+            self._cart_downward(dst, local)
+        return local
+
+    def _cart_downward(self, dst, local) -> None:
+        """L2L of Cartesian locals of this tree's order down the cells of ``dst``, level
+        by level (td3_cart_downward)."""
+        t = self._cartesian_tables()
         levels = np.ascontiguousarray(dst.levels, dtype=np.int64)
         _lib.call("td3_cart_downward", levels.ctypes.data, len(levels) - 1,
                   dst.node_center.data_ptr(), dst.node_child.data_ptr(), self.order,
                   t["ex"].data_ptr(), t["ey"].data_ptr(), t["l2l_start"].data_ptr(),
                   t["l2l_g"].data_ptr(), t["l2l_d"].data_ptr(), t["l2l_coef"].data_ptr(),
-                  local.data_ptr(), stream)
-        return local
+                  local.data_ptr(), _lib.stream(self.device))
+
+    # ------------------------------------------------------------------ ranks
+    def _shard(self, theta: float, rank: int, world: int) -> dict:
+        """Rank ``rank``'s share of the FMM of ``theta`` among ``world`` ranks, as the
+        reference's _fmm_shares (ft:830-851): an even run of the M2L pairs (with the
+        order the M2L kernel reads) and a run of leaves with about an even share of the
+        near-field work (a near-field plan of those leaves only)."""
+        key = (theta, rank, world)
+        if key not in self._shard_cache:
+            lists = self._lists(theta)
+            m2l = lists["m2l"]
+            pairs = _shards.share(torch.ones(m2l.shape[0], device=self.device), rank, world)
+            mine = m2l[pairs]
+            part = _Lists(self, m2l=mine)
+            if self._grouped_m2l():
+                part["groups"] = self._m2l_groups(mine, theta)
+            else:
+                part["m2l_rows"]  # the CSR rows of this run, made now
+            work = _shards.leaf_work(self, lists["p2p_rows"], lists["p2p_partners"])
+            leaves = _shards.share(work, rank, world)
+            idx = torch.arange(self.node_count, device=self.device)
+            inside = (idx >= leaves.start) & (idx < leaves.stop)
+            end = torch.where(inside, self.node_end, self.node_start).contiguous()
+            part["p2p"] = lists["p2p"]
+            part["p2p_partners"] = lists["p2p_partners"]
+            part["plan"] = _nearfield_plan(lists["p2p_rows"], self, 2 * lists["p2p"].shape[0],
+                                           end=end)
+            part["pairs"], part["leaves"] = pairs, leaves
+            self._shard_cache[key] = part
+        return self._shard_cache[key]
+
+    def _shard_locals(self, part: dict, softening: float):
+        """The M2L of a share's pairs into zeroed locals (no L2L): the rank's part of
+        the locals, completed by a sum over the ranks."""
+        if self.kernel == "log":
+            return self._log_locals(part, downward=False)
+        local = self._cart_locals(part["m2l_rows"], part["m2l_partners"], part["m2l"].shape[0],
+                                  self, softening, downward=False)
+        return local, local
+
+    def _shard_near(self, part: dict, local_a, local_b, softening, potential, phi, field,
+                    status) -> None:
+        """L2P + P2P of a share's leaves into phi and field (zero elsewhere)."""
+        kernel = _lib.KERNEL_LOG if self.kernel == "log" else _lib.KERNEL_COULOMB
+        with_pot = potential if self.kernel == "log" else True
+        self._evaluate_near(part, kernel, local_a, local_b, softening, with_pot, phi, field,
+                            status)
+
+    def _full_downward(self, local_a, local_b) -> None:
+        if self.kernel == "log":
+            self._downward(local_a, local_b, self.order, self._binomial())
+        else:
+            self._cart_downward(self, local_a)
+
+    def _fmm_sharded(self, theta, softening, potential, phi, field) -> None:
+        """fmm over the ranks of ``comm`` (ft:1505-1539, :1600-1631): the same tree and
+        lists on every rank; this rank's M2L pairs into its locals, summed over the
+        ranks; L2L everywhere; this rank's leaves' near field, the potential and field
+        summed over the ranks and the coincidence status maximised."""
+        part = self._shard(theta, self._rank, self._world)
+        local_a, local_b = self._shard_locals(part, softening)
+        _shards.allsum(local_a, self.comm)
+        if local_b is not local_a:
+            _shards.allsum(local_b, self.comm)
+        self._full_downward(local_a, local_b)
+        status = status_word(self.device)
+        self._shard_near(part, local_a, local_b, softening, potential, phi, field, status)
+        _shards.allsum(phi, self.comm)
+        _shards.allsum(field, self.comm)
+        _shards.allmax(status, self.comm)
+        _check(status)
+        self._check_tensor_cores()
+        self._fwd_locals = None
+        lists = self._lists(theta)
+        self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
+        if not potential:
+            phi.zero_()
 
     def _coulomb_fmm(self, theta, softening, phi, field, status=None):
         """ft:1360-1428: the Coulomb FMM with Cartesian expansions (the potential is
