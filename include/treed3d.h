@@ -157,6 +157,22 @@ int td3_log_moments(const int64_t* levels, int64_t n_levels, int order,
                     const double* binomial, int binomial_size, double* node_qabs,
                     double* moment_re, double* moment_im, void* stream);
 
+/* td3_log_moments (sorted_dipole null) or td3_log_moments_adjoint (sorted_dipole the
+ * (2, n) point dipoles) in one launch, orders up to 12: a thread per node forms its
+ * leaf's moments, and the last of four children to finish forms their parent by M2M
+ * (an atomic arrival counter per node in `arrive`, count int32, zeroed by the call),
+ * with the operations of the level-by-level pass: the same bits.  node_parent from
+ * td3_node_parents.  Replaces the per-level loop of log_moments_upward
+ * (src/tree_d_3d/kernels/log_moments_upward/log_moments_upward_pyccel.py:14-93,
+ * src/tree_d_3d/flat_tree.py:689-713) in one launch. */
+int td3_log_moments_tree(int64_t count, int order, const double* sorted_pos,
+                         const double* sorted_charge, const double* sorted_dipole, int64_t n,
+                         const double* node_center, const int64_t* node_start,
+                         const int64_t* node_end, const int64_t* node_child,
+                         const int32_t* node_parent, const double* binomial, int binomial_size,
+                         double* node_qabs, double* moment_re, double* moment_im,
+                         int32_t* arrive, void* stream);
+
 /* Cartesian multipole moments m_g = sum q (r - c)^g, |g| <= order, of every node
  * (moments (nodes, n_coef)), with the index tables of the reference's _cartesian.tables
  * (src/tree_d_3d/_cartesian.py:40-107): ex, ey (n_coef), shift (n_shift, 3) rows

@@ -221,3 +221,30 @@ def test_build_of_fine_clusters_matches_the_oracle(oracle, scale, depth):
         np.testing.assert_array_equal(_np(getattr(tree, name)), getattr(ref, name)[: ref.node_count]
                                       if name != "perm" else ref.perm, err_msg=name)
     np.testing.assert_array_equal(tree.levels, ref.levels)
+
+
+@pytest.mark.parametrize("order", [4, 8, 12])
+def test_moments_in_one_launch_are_the_bits_of_the_level_pass(order, monkeypatch):
+    """The one-launch upward pass (the last child forms its parent) against the
+    level-by-level pass, for the forward moments and the adjoint ones (monopoles and
+    point dipoles): identical arrays."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, flat_tree, synthetic
+
+    pos, q = synthetic.mixture8(200_000, seed=70 + order)
+    tree = FlatQuadtree(torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda"),
+                        Quad(0, 0, 1), kernel="log", order=order)
+    rng = np.random.default_rng(order)
+    w = torch.tensor(rng.normal(size=pos.shape[1]), device="cuda")
+    d = torch.tensor(rng.normal(size=pos.shape), device="cuda")
+    binom = tree._binomial()
+    runs = {}
+    for one in (True, False):
+        monkeypatch.setattr(flat_tree, "MOMENTS_ONE_LAUNCH", one)
+        tree._moments()
+        out = [_np(tree.moment_re).copy(), _np(tree.moment_im).copy(), _np(tree.node_qabs).copy()]
+        mre, mim = torch.empty_like(tree.moment_re), torch.empty_like(tree.moment_im)
+        wabs = torch.empty_like(tree.node_qabs)
+        tree._log_moments_into(w, d, binom, wabs, mre, mim)
+        runs[one] = out + [_np(mre), _np(mim), _np(wabs)]
+    for a, b in zip(runs[True], runs[False]):
+        np.testing.assert_array_equal(a, b)

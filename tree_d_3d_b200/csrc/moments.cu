@@ -283,6 +283,124 @@ k_log_m2m_level(i64 lo, i64 hi, int order, const double* __restrict__ node_cente
     }
 }
 
+// The whole upward pass in one launch (orders up to P): a thread per node.  A leaf's
+// thread forms its moments from its particles with the operations of
+// k_log_leaf_moments, then arrives at its parent; the fourth child to arrive forms the
+// parent by M2M with the operations of k_log_m2m_level (each child's shifted
+// coefficients c_n = sum_m C(n, m) a_m s^(n-m), the children added in order) and goes on
+// up.  The moments are therefore the same bits as the level-by-level pass.  No thread
+// waits for another: the last arrival does the work, a fence before each arrival
+// publishes the arriving node's moments, and the children are read through L2.
+template <int P>
+__global__ void __launch_bounds__(MOM_THREADS)
+k_log_moments_tree(i64 count, int order, const double* __restrict__ spos,
+                   const double* __restrict__ scharge, i64 n_particles,
+                   const double* __restrict__ node_center, const i64* __restrict__ node_start,
+                   const i64* __restrict__ node_end, const i64* __restrict__ node_child,
+                   const int* __restrict__ parent, const double* __restrict__ binomial,
+                   int bsize, double* node_qabs, double* moment_re, double* moment_im,
+                   const double* __restrict__ sdip, int* arrive) {
+    constexpr int W = P + 1;
+    i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= count || node_child[node] >= 0) return;
+    const int w = order + 1;
+    {
+        double xmid = node_center[2 * node], ymid = node_center[2 * node + 1];
+        double ar[W], ai[W];
+#pragma unroll
+        for (int n = 0; n < W; ++n) ar[n] = ai[n] = 0.0;
+        double qabs = 0.0;
+        for (i64 k = node_start[node]; k < node_end[node]; ++k) {
+            double q = scharge[k];
+            qabs += fabs(q);
+            double dx = spos[k] - xmid, dy = spos[n_particles + k] - ymid;
+            double pr = q, pi = 0.0;
+#pragma unroll
+            for (int n = 0; n < W; ++n) {
+                ar[n] += pr;
+                ai[n] += pi;
+                double next_re = pr * dx - pi * dy;
+                pi = pr * dy + pi * dx;
+                pr = next_re;
+            }
+            if (sdip) {
+                double er = sdip[k], ei = sdip[n_particles + k];
+                double zr = 1.0, zi = 0.0;
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    ar[n] -= n * (er * zr - ei * zi);
+                    ai[n] -= n * (er * zi + ei * zr);
+                    double nr = zr * dx - zi * dy;
+                    zi = zr * dy + zi * dx;
+                    zr = nr;
+                }
+            }
+        }
+#pragma unroll
+        for (int n = 0; n < W; ++n) {
+            if (n < w) {
+                moment_re[node * w + n] = ar[n];
+                moment_im[node * w + n] = ai[n];
+            }
+        }
+        node_qabs[node] = qabs;
+    }
+    for (i64 cur = node;;) {
+        int up = parent[cur];
+        if (up < 0) return;
+        __threadfence();
+        if (atomicAdd(&arrive[up], 1) != 3) return;
+        __threadfence();
+        i64 first = node_child[up];
+        double xmid = node_center[2 * up], ymid = node_center[2 * up + 1];
+        double acc_re[W], acc_im[W];
+#pragma unroll
+        for (int n = 0; n < W; ++n) acc_re[n] = acc_im[n] = 0.0;
+        double qabs = 0.0;
+        for (i64 child = first; child < first + 4; ++child) {
+            qabs += __ldcg(node_qabs + child);
+            if (node_end[child] == node_start[child]) continue;
+            double s_re = node_center[2 * child] - xmid;
+            double s_im = node_center[2 * child + 1] - ymid;
+            double sh_re[W], sh_im[W], cr[W], ci[W];
+            sh_re[0] = 1.0;
+            sh_im[0] = 0.0;
+#pragma unroll
+            for (int n = 1; n < W; ++n) {
+                sh_re[n] = sh_re[n - 1] * s_re - sh_im[n - 1] * s_im;
+                sh_im[n] = sh_re[n - 1] * s_im + sh_im[n - 1] * s_re;
+            }
+#pragma unroll
+            for (int m = 0; m < W; ++m) {
+                cr[m] = m < w ? __ldcg(moment_re + child * w + m) : 0.0;
+                ci[m] = m < w ? __ldcg(moment_im + child * w + m) : 0.0;
+            }
+#pragma unroll
+            for (int n = 0; n < W; ++n) {
+                double c_re = 0.0, c_im = 0.0;
+#pragma unroll
+                for (int m = 0; m <= n; ++m) {
+                    double b = binomial[n * bsize + m];
+                    double a_re = cr[m] * b, a_im = ci[m] * b;
+                    c_re += a_re * sh_re[n - m] - a_im * sh_im[n - m];
+                    c_im += a_re * sh_im[n - m] + a_im * sh_re[n - m];
+                }
+                acc_re[n] += c_re;
+                acc_im[n] += c_im;
+            }
+        }
+#pragma unroll
+        for (int n = 0; n < W; ++n) {
+            if (n < w) {
+                moment_re[up * w + n] = acc_re[n];
+                moment_im[up * w + n] = acc_im[n];
+            }
+        }
+        node_qabs[up] = qabs;
+        cur = up;
+    }
+}
+
 // Moments of every node.  Orders up to 15: every leaf in one launch (leaves depend on
 // nothing), then the internal nodes level by level, deepest first, a thread per (node,
 // child); higher orders: thread per (node, coefficient), level by level.
@@ -537,4 +655,37 @@ extern "C" int td3_cart_moments_adjoint(const int64_t* levels, int64_t n_levels,
     return launch_cart_moments(levels, n_levels, sorted_pos, sorted_weight, n, node_center,
                                node_start, node_end, node_child, shift, shift_coef, shift_start,
                                n_coef, moments, sorted_dipole, td3_stream(stream));
+}
+
+extern "C" int td3_log_moments_tree(int64_t count, int order, const double* sorted_pos,
+                                    const double* sorted_charge, const double* sorted_dipole,
+                                    int64_t n, const double* node_center,
+                                    const int64_t* node_start, const int64_t* node_end,
+                                    const int64_t* node_child, const int32_t* node_parent,
+                                    const double* binomial, int binomial_size, double* node_qabs,
+                                    double* moment_re, double* moment_im, int32_t* arrive,
+                                    void* stream) {
+    if (count < 1 || count > 0x7fffffffLL || order < 0 || order > 12 ||
+        binomial_size < order + 1)
+        return TD3_EINVAL;
+    cudaStream_t s = td3_stream(stream);
+    TD3_TRY(cudaMemsetAsync(arrive, 0, sizeof(int32_t) * count, s));
+    unsigned nb = td3_blocks(count, MOM_THREADS);
+    if (order <= 4)
+        k_log_moments_tree<4><<<nb, MOM_THREADS, 0, s>>>(
+            count, order, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
+            node_child, node_parent, binomial, binomial_size, node_qabs, moment_re, moment_im,
+            sorted_dipole, arrive);
+    else if (order <= 8)
+        k_log_moments_tree<8><<<nb, MOM_THREADS, 0, s>>>(
+            count, order, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
+            node_child, node_parent, binomial, binomial_size, node_qabs, moment_re, moment_im,
+            sorted_dipole, arrive);
+    else
+        k_log_moments_tree<12><<<nb, MOM_THREADS, 0, s>>>(
+            count, order, sorted_pos, sorted_charge, n, node_center, node_start, node_end,
+            node_child, node_parent, binomial, binomial_size, node_qabs, moment_re, moment_im,
+            sorted_dipole, arrive);
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
 }

@@ -274,26 +274,31 @@ __device__ __forceinline__ double pair_unit(double unit) {
 // (with the charges in FP64, qsum) and 2 q d' / r'^2.
 template <int KERNEL, bool POT>
 __device__ __forceinline__ void pair_mixed(double dx64, double dy64, double qj, double inv_unit,
-                                           float eps2f, KahanF& p, KahanF& x, KahanF& y,
+                                           float eps2f, float& p, float& x, float& y,
                                            double& qsum) {
     float dx = (float)(dx64 * inv_unit), dy = (float)(dy64 * inv_unit), q = (float)qj;
     float r2 = dx * dx + dy * dy + eps2f;
     if (KERNEL == TD3_KERNEL_LOG) {
         if (POT) {
-            p.add(-q * __logf(r2));
+            p += -q * __logf(r2);
             qsum += qj;
         }
         float f = __fdividef(2.0f * q, r2);
-        x.add(f * dx);
-        y.add(f * dy);
+        x += f * dx;
+        y += f * dy;
     } else {
         float inv_r = rsqrtf(r2);
         float qr3 = q * inv_r * inv_r * inv_r;
-        p.add(q * inv_r);
-        x.add(qr3 * dx);
-        y.add(qr3 * dy);
+        p += q * inv_r;
+        x += qr3 * dx;
+        y += qr3 * dy;
     }
 }
+
+// Pairs summed in plain FP32 before one compensated addition: each lane adds the terms
+// of NF_BLOCK consecutive pairs of its slice, then the block's sum to the compensated
+// accumulator (the rounding of a 16-term sum, then compensated across blocks).
+constexpr int NF_BLOCK = 16;
 
 // One warp per segment.  OTHER: targets and sources are different point sets (fmm_at):
 // zero charges and source exclude[i] are skipped and any coincidence is an error.
@@ -345,39 +350,56 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
         double qsum = 0.0;
         for_source_windows<NF_CAP>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
             if (!valid) return;
-            for (int p = slice; p < wn; p += slices) {
-                double qj = win.q[p];
-                i64 tag = win.tag[p];
-                if (OTHER) {
-                    if (qj == 0.0 || tag == skip) continue;
-                } else if (tag == skip) {
-                    continue;
+            if constexpr (MIXED) {
+                for (int p0 = slice; p0 < wn; p0 += NF_BLOCK * slices) {
+                    float bp = 0.0f, bx = 0.0f, by = 0.0f;
+                    int p1 = p0 + NF_BLOCK * slices < wn ? p0 + NF_BLOCK * slices : wn;
+                    for (int p = p0; p < p1; p += slices) {
+                        double qj = win.q[p];
+                        i64 tag = win.tag[p];
+                        if (OTHER) {
+                            if (qj == 0.0 || tag == skip) continue;
+                        } else if (tag == skip) {
+                            continue;
+                        }
+                        double dx = xi - win.x[p], dy = yi - win.y[p];
+                        if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) {
+                            bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
+                            continue;
+                        }
+                        pair_mixed<KERNEL, POT>(dx, dy, qj, inv_unit, eps2f, bp, bx, by, qsum);
+                    }
+                    if (POT || KERNEL != TD3_KERNEL_LOG) kp.add(bp);
+                    kx.add(bx);
+                    ky.add(by);
                 }
-                double dx = xi - win.x[p], dy = yi - win.y[p];
-                if (MIXED) {
-                    if (dx == 0.0 && dy == 0.0 && eps2 == 0.0) {
+            } else {
+                for (int p = slice; p < wn; p += slices) {
+                    double qj = win.q[p];
+                    i64 tag = win.tag[p];
+                    if (OTHER) {
+                        if (qj == 0.0 || tag == skip) continue;
+                    } else if (tag == skip) {
+                        continue;
+                    }
+                    double dx = xi - win.x[p], dy = yi - win.y[p];
+                    double r2 = dx * dx + dy * dy + eps2;
+                    if (r2 == 0.0) {
                         bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
                         continue;
                     }
-                    pair_mixed<KERNEL, POT>(dx, dy, qj, inv_unit, eps2f, kp, kx, ky, qsum);
-                    continue;
-                }
-                double r2 = dx * dx + dy * dy + eps2;
-                if (r2 == 0.0) {
-                    bad |= OTHER ? true : (qi != 0.0 && qj != 0.0);
-                    continue;
-                }
-                if (KERNEL == TD3_KERNEL_LOG) {
-                    if (POT) pot -= qj * log(r2);
-                    double f = 2.0 * qj / r2;
-                    ex += f * dx;
-                    ey += f * dy;
-                } else {
-                    double inv_r = rsqrt(r2);
-                    double inv_r3 = inv_r * inv_r * inv_r;
-                    pot += qj * inv_r;
-                    ex += qj * inv_r3 * dx;
-                    ey += qj * inv_r3 * dy;
+                    if (KERNEL == TD3_KERNEL_LOG) {
+                        if (POT) pot -= qj * log(r2);
+                        double f = 2.0 * qj / r2;
+                        ex += f * dx;
+                        ey += f * dy;
+                    } else {
+                        double inv_r = rsqrt(r2);
+                        double inv_r3 = inv_r * inv_r * inv_r;
+                        pot += qj * inv_r;
+                        ex += qj * inv_r3 * dx;
+                        ey += qj * inv_r3 * dy;
+                    }
                 }
             }
         });
@@ -536,31 +558,31 @@ __device__ __forceinline__ void adjoint_pair(double dx, double dy, double eps2, 
 // after an FP64 subtraction).
 template <int KERNEL>
 __device__ __forceinline__ void adjoint_pair_mixed(float dx, float dy, float eps2, float qj,
-                                                   float wj, float exj, float eyj, KahanF* acc) {
+                                                   float wj, float exj, float eyj, float* acc) {
     float s = dx * dx + dy * dy + eps2;
     float de = exj * dx + eyj * dy;
     if (KERNEL == TD3_KERNEL_LOG) {
         float inv = __frcp_rn(s);
-        acc[0].add(-wj * __logf(s) - 2.0f * de * inv);
+        acc[0] += -wj * __logf(s) - 2.0f * de * inv;
         float t = 4.0f * de * inv * inv;
-        acc[1].add(-2.0f * inv * (wj * dx + exj) + t * dx);
-        acc[2].add(-2.0f * inv * (wj * dy + eyj) + t * dy);
+        acc[1] += -2.0f * inv * (wj * dx + exj) + t * dx;
+        acc[2] += -2.0f * inv * (wj * dy + eyj) + t * dy;
         float q4 = 4.0f * qj * inv * inv;
-        acc[3].add(-2.0f * qj * inv + q4 * dx * dx);
-        acc[4].add(q4 * dx * dy);
-        acc[5].add(-2.0f * qj * inv + q4 * dy * dy);
+        acc[3] += -2.0f * qj * inv + q4 * dx * dx;
+        acc[4] += q4 * dx * dy;
+        acc[5] += -2.0f * qj * inv + q4 * dy * dy;
     } else {
         float r = rsqrtf(s);
         float r3 = r * r * r;
         float r5 = r3 * r * r;
-        acc[0].add(wj * r - de * r3);
+        acc[0] += wj * r - de * r3;
         float t = 3.0f * de * r5;
-        acc[1].add(-r3 * (wj * dx + exj) + t * dx);
-        acc[2].add(-r3 * (wj * dy + eyj) + t * dy);
+        acc[1] += -r3 * (wj * dx + exj) + t * dx;
+        acc[2] += -r3 * (wj * dy + eyj) + t * dy;
         float q3 = 3.0f * qj * r5;
-        acc[3].add(-qj * r3 + q3 * dx * dx);
-        acc[4].add(q3 * dx * dy);
-        acc[5].add(-qj * r3 + q3 * dy * dy);
+        acc[3] += -qj * r3 + q3 * dx * dx;
+        acc[4] += q3 * dx * dy;
+        acc[5] += -qj * r3 + q3 * dy * dy;
     }
 }
 
@@ -665,17 +687,27 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
         double wsum = 0.0;
         for_source_windows<NF_CAP_ADJ>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
             if (!valid) return;
-            for (int p = slice; p < wn; p += slices) {
-                if (win.tag[p] == self) continue;
-                double dx = xs - win.x[p], dy = ys - win.y[p];
-                if constexpr (MIXED) {
-                    float dxf = (float)dx, dyf = (float)dy;
-                    if (dxf == 0.0f && dyf == 0.0f && eps2 == 0.0 && dx == 0.0 && dy == 0.0)
-                        continue;
-                    if (KERNEL == TD3_KERNEL_LOG) wsum += win.w[p];
-                    adjoint_pair_mixed<KERNEL>(dxf, dyf, eps2f, win.qf[p], win.wf[p], win.exf[p],
-                                               win.eyf[p], kacc);
-                } else {
+            if constexpr (MIXED) {
+                for (int p0 = slice; p0 < wn; p0 += NF_BLOCK * slices) {
+                    float blk[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                    int p1 = p0 + NF_BLOCK * slices < wn ? p0 + NF_BLOCK * slices : wn;
+                    for (int p = p0; p < p1; p += slices) {
+                        if (win.tag[p] == self) continue;
+                        double dx = xs - win.x[p], dy = ys - win.y[p];
+                        float dxf = (float)dx, dyf = (float)dy;
+                        if (dxf == 0.0f && dyf == 0.0f && eps2 == 0.0 && dx == 0.0 && dy == 0.0)
+                            continue;
+                        if (KERNEL == TD3_KERNEL_LOG) wsum += win.w[p];
+                        adjoint_pair_mixed<KERNEL>(dxf, dyf, eps2f, win.qf[p], win.wf[p],
+                                                   win.exf[p], win.eyf[p], blk);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 6; ++c) kacc[c].add(blk[c]);
+                }
+            } else {
+                for (int p = slice; p < wn; p += slices) {
+                    if (win.tag[p] == self) continue;
+                    double dx = xs - win.x[p], dy = ys - win.y[p];
                     if (dx * dx + dy * dy + eps2 == 0.0) continue;
                     adjoint_pair<KERNEL>(dx, dy, eps2, win.q[p], win.w[p], win.ex[p], win.ey[p],
                                          acc);

@@ -185,6 +185,10 @@ M2L_TENSOR_CORES = False
 #: own locals) instead of one L2L launch per level
 DOWNWARD_LEAVES = True
 
+#: the log kernel's upward pass in one launch (orders up to 12; the last child to finish
+#: forms its parent) instead of one M2M launch per level; the same bits either way
+MOMENTS_ONE_LAUNCH = True
+
 #: the mixed-precision M2L of ``fmm`` (mutual lists, log kernel, orders up to 14) as
 #: tensor-core products grouped by translation (td3_m2l_groups, td3_fmm_m2l_grouped)
 M2L_GROUPED = True
@@ -413,9 +417,8 @@ class FlatQuadtree:
             self.moment_re = torch.empty((count, self.order + 1), dtype=f64, device=dev)
             self.moment_im = torch.empty((count, self.order + 1), dtype=f64, device=dev)
             binom = self._binomial()
-            _lib.call("td3_log_moments", levels.ctypes.data, len(levels) - 1, self.order, *common,
-                      binom.data_ptr(), binom.shape[0], self.node_qabs.data_ptr(),
-                      self.moment_re.data_ptr(), self.moment_im.data_ptr(), stream)
+            self._log_moments_into(self._sorted_charge, None, binom, self.node_qabs,
+                                   self.moment_re, self.moment_im)
             self.node_q = self.moment_re[:, 0].clone()
             self.node_p = torch.stack((self.moment_re[:, 1], self.moment_im[:, 1]), dim=1)
             self.node_s = torch.zeros((count, 3), dtype=f64, device=dev)
@@ -428,6 +431,36 @@ class FlatQuadtree:
         _lib.call("td3_quadtree_moments", levels.ctypes.data, len(levels) - 1, *common,
                   self.node_q.data_ptr(), self.node_qabs.data_ptr(), self.node_p.data_ptr(),
                   self.node_s.data_ptr(), stream)
+
+    def _log_moments_into(self, weight, dipole, binom, qabs, mre, mim) -> None:
+        """Complex moments of monopoles ``weight`` (tree order) and, when given, point
+        dipoles ``dipole`` (2, N) into mre / mim: in one launch for orders up to 12
+        (td3_log_moments_tree), else level by level (td3_log_moments[_adjoint]); the
+        same bits either way."""
+        n, stream = self.pos.shape[1], _lib.stream(self.device)
+        if MOMENTS_ONE_LAUNCH and self.order <= 12:
+            arrive = torch.empty(self.node_count, dtype=torch.int32, device=self.device)
+            _lib.call("td3_log_moments_tree", self.node_count, self.order,
+                      self._sorted_pos.data_ptr(), weight.data_ptr(),
+                      0 if dipole is None else dipole.data_ptr(), n,
+                      self.node_center.data_ptr(), self.node_start.data_ptr(),
+                      self.node_end.data_ptr(), self.node_child.data_ptr(),
+                      self._parents().data_ptr(), binom.data_ptr(), binom.shape[0],
+                      qabs.data_ptr(), mre.data_ptr(), mim.data_ptr(), arrive.data_ptr(), stream)
+            return
+        levels = np.ascontiguousarray(self.levels, dtype=np.int64)
+        nodes = (self.node_center.data_ptr(), self.node_start.data_ptr(),
+                 self.node_end.data_ptr(), self.node_child.data_ptr())
+        if dipole is None:
+            _lib.call("td3_log_moments", levels.ctypes.data, len(levels) - 1, self.order,
+                      self._sorted_pos.data_ptr(), weight.data_ptr(), n, *nodes,
+                      binom.data_ptr(), binom.shape[0], qabs.data_ptr(), mre.data_ptr(),
+                      mim.data_ptr(), stream)
+        else:
+            _lib.call("td3_log_moments_adjoint", levels.ctypes.data, len(levels) - 1, self.order,
+                      self._sorted_pos.data_ptr(), weight.data_ptr(), dipole.data_ptr(), n,
+                      *nodes, binom.data_ptr(), binom.shape[0], qabs.data_ptr(),
+                      mre.data_ptr(), mim.data_ptr(), stream)
 
     def _cartesian_tables(self):
         from tree_d_3d_b200 import _cartesian
@@ -883,11 +916,7 @@ class FlatQuadtree:
             mim = torch.empty_like(mre)
             wabs = torch.empty(count, dtype=torch.float64, device=dev)
             binom = self._binomial()
-            _lib.call("td3_log_moments_adjoint", levels.ctypes.data, len(levels) - 1, self.order,
-                      self._sorted_pos.data_ptr(), sw.data_ptr(), sd.data_ptr(), n,
-                      self.node_center.data_ptr(), self.node_start.data_ptr(),
-                      self.node_end.data_ptr(), self.node_child.data_ptr(), binom.data_ptr(),
-                      binom.shape[0], wabs.data_ptr(), mre.data_ptr(), mim.data_ptr(), stream)
+            self._log_moments_into(sw, sd, binom, wabs, mre, mim)
             adj_a, adj_b = self._log_locals(lists, moments=(mre, mim))
             kernel = _lib.KERNEL_LOG
         else:
