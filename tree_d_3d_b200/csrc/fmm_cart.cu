@@ -88,11 +88,59 @@ k_m2l_cart(const i64* __restrict__ row_start, const i64* __restrict__ partners, 
 constexpr int CART_GROUP = 8;
 constexpr int CART_LANE_MAX = 16;
 
+constexpr int CART_CHUNK = 4;     // coefficients b of one degree per lane and pass
+constexpr int CART_MAX_CHUNKS = 48;
+
 struct CartScale {
     short bx[(CART_LANE_MAX + 1) * (CART_LANE_MAX + 2) / 2];
     short by[(CART_LANE_MAX + 1) * (CART_LANE_MAX + 2) / 2];
     double inv_fact2[(CART_LANE_MAX + 1) * (CART_LANE_MAX + 2) / 2];  // 1 / (a_x! a_y!)
+    // runs of CART_CHUNK coefficients of one degree: degree nb, first b_y
+    short chunk_nb[CART_MAX_CHUNKS], chunk_by[CART_MAX_CHUNKS];
+    int n_chunks;
 };
+
+// Partner p's share of T~_b for the coefficients b = (nb - by, by), by = by0 ..
+// by0 + CART_CHUNK - 1 (those with by <= nb): for each degree na of a the run of m~ (na +
+// 1 values) and the run of A~ of degree na + nb from b_y = by0 on are read once, through
+// a window of CART_CHUNK values of A~ that slides by one per a_y, so each value serves
+// CART_CHUNK coefficients.  Each acc[r] sums over na, then a_y, in the order of the
+// one-coefficient loop (the same bits).
+template <typename T>
+__device__ __forceinline__ void cart_chunk(const T* __restrict__ Mt, const T* __restrict__ At,
+                                           int p, int nb, int by0, int order,
+                                           T (&acc)[CART_CHUNK]) {
+#pragma unroll
+    for (int r = 0; r < CART_CHUNK; ++r) acc[r] = T(0);
+    for (int na = 0; na + nb <= order; ++na) {
+        int ng = na + nb, lim = ng - by0;  // the run of degree ng holds indices 0..lim
+        const T* mrow = Mt + (na * (na + 1) / 2) * CART_GROUP + p;
+        const T* grow = At + (ng * (ng + 1) / 2 + by0) * CART_GROUP + p;
+        T w[CART_CHUNK];
+#pragma unroll
+        for (int r = 0; r < CART_CHUNK; ++r) w[r] = r <= lim ? grow[r * CART_GROUP] : T(0);
+        for (int ay = 0; ay <= na; ++ay) {
+            T m = mrow[ay * CART_GROUP];
+#pragma unroll
+            for (int r = 0; r < CART_CHUNK; ++r) acc[r] += m * w[r];
+#pragma unroll
+            for (int r = 0; r + 1 < CART_CHUNK; ++r) w[r] = w[r + 1];
+            int k = ay + CART_CHUNK;
+            w[CART_CHUNK - 1] = k <= lim ? grow[k * CART_GROUP] : T(0);
+        }
+    }
+}
+
+// The coefficient runs of cart_chunk for orders up to CART_LANE_MAX, degree by degree.
+void cart_chunks(int order, CartScale& C) {
+    C.n_chunks = 0;
+    for (int nb = 0; nb <= order; ++nb)
+        for (int by0 = 0; by0 <= nb; by0 += CART_CHUNK) {
+            C.chunk_nb[C.n_chunks] = (short)nb;
+            C.chunk_by[C.n_chunks] = (short)by0;
+            ++C.n_chunks;
+        }
+}
 
 template <int P>
 __global__ void __launch_bounds__(32 * CM2L_WARPS)
@@ -158,23 +206,26 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
                 }
             }
             __syncwarp();
-            for (int j0 = 0; j0 < n_coef; j0 += 4) {
-                int b = j0 + q;
-                double acc = 0.0;
-                if (b < n_coef) {
-                    int bx = C.bx[b], by = C.by[b], nb = bx + by;
-                    for (int na = 0; na + nb <= order; ++na) {
-                        int ng = na + nb;
-                        const double* mrow = Mt + (na * (na + 1) / 2) * CART_GROUP + p;
-                        const double* grow = At + (ng * (ng + 1) / 2 + by) * CART_GROUP + p;
-                        for (int ay = 0; ay <= na; ++ay)
-                            acc += mrow[ay * CART_GROUP] * grow[ay * CART_GROUP];
-                    }
+            // lane (q, p): chunks q, q + 4, ... of partner p, then 3 butterfly steps over p
+            for (int k0 = 0; k0 < C.n_chunks; k0 += 4) {
+                int k = k0 + q;
+                int nb = k < C.n_chunks ? C.chunk_nb[k] : 0, by0 = k < C.n_chunks ? C.chunk_by[k] : 0;
+                double acc[CART_CHUNK];
+                if (k < C.n_chunks) {
+                    cart_chunk<double>(Mt, At, p, nb, by0, order, acc);
+                } else {
+#pragma unroll
+                    for (int r = 0; r < CART_CHUNK; ++r) acc[r] = 0.0;
                 }
-                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                if (p == 0 && b < n_coef) T[b] += acc;
+#pragma unroll
+                for (int r = 0; r < CART_CHUNK; ++r) {
+                    double a = acc[r];
+                    a += __shfl_xor_sync(0xffffffffu, a, 4);
+                    a += __shfl_xor_sync(0xffffffffu, a, 2);
+                    a += __shfl_xor_sync(0xffffffffu, a, 1);
+                    if (p == 0 && k < C.n_chunks && by0 + r <= nb)
+                        T[nb * (nb + 1) / 2 + by0 + r] += a;
+                }
             }
         }
         __syncwarp();
@@ -263,24 +314,25 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
                 }
             }
             __syncwarp();
-            for (int j0 = 0; j0 < n_coef; j0 += 4) {
-                int b = j0 + q;
-                float acc = 0.0f;
-                if (b < n_coef) {
-                    int bx = C.bx[b], by = C.by[b], nb = bx + by;
-                    for (int na = 0; na + nb <= order; ++na) {
-                        int ng = na + nb;
-                        const float* mrow = Mt + (na * (na + 1) / 2) * CART_GROUP + p;
-                        const float* grow = At + (ng * (ng + 1) / 2 + by) * CART_GROUP + p;
-                        for (int ay = 0; ay <= na; ++ay)
-                            acc += mrow[ay * CART_GROUP] * grow[ay * CART_GROUP];
-                    }
-                    acc = ldexpf(acc, dl * (1 + nb));
+            for (int k0 = 0; k0 < C.n_chunks; k0 += 4) {
+                int k = k0 + q;
+                int nb = k < C.n_chunks ? C.chunk_nb[k] : 0, by0 = k < C.n_chunks ? C.chunk_by[k] : 0;
+                float acc[CART_CHUNK];
+                if (k < C.n_chunks) {
+                    cart_chunk<float>(Mt, At, p, nb, by0, order, acc);
+                } else {
+#pragma unroll
+                    for (int r = 0; r < CART_CHUNK; ++r) acc[r] = 0.0f;
                 }
-                acc += __shfl_xor_sync(0xffffffffu, acc, 4);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 2);
-                acc += __shfl_xor_sync(0xffffffffu, acc, 1);
-                if (p == 0 && b < n_coef) T[b] += acc;
+#pragma unroll
+                for (int r = 0; r < CART_CHUNK; ++r) {
+                    float a = ldexpf(acc[r], dl * (1 + nb));
+                    a += __shfl_xor_sync(0xffffffffu, a, 4);
+                    a += __shfl_xor_sync(0xffffffffu, a, 2);
+                    a += __shfl_xor_sync(0xffffffffu, a, 1);
+                    if (p == 0 && k < C.n_chunks && by0 + r <= nb)
+                        T[nb * (nb + 1) / 2 + by0 + r] += a;
+                }
             }
         }
         __syncwarp();
@@ -306,6 +358,7 @@ CartScale cart_scale(int order) {
             C.by[i] = (short)y;
             C.inv_fact2[i] = 1.0 / (f[n - y] * f[y]);
         }
+    cart_chunks(order, C);
     return C;
 }
 
@@ -363,6 +416,7 @@ extern "C" int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, i
                 C.by[i] = (short)y;
                 C.inv_fact2[i] = 1.0 / (f[n - y] * f[y]);
             }
+        cart_chunks(order, C);
         size_t lane_smem = sizeof(double) * (2 * CART_GROUP + 1) * n_coef * CM2L_WARPS;
         i64 nb = (n_dst + CM2L_WARPS - 1) / CM2L_WARPS;
         unsigned grid = (unsigned)(nb < 148 * 64 ? nb : 148 * 64);
