@@ -338,8 +338,9 @@ int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
  *     (ceil(n_nodes / 128) + 1); levels HOST (n_levels + 1, the first node of each
  *     depth, then n_nodes); n_nodes < 2^25; depends on the tree and the lists only;
  *   td3_fmm_m2l_grouped: the products into local_re / local_im (FP64, added), from the
- *     scaled moments `hat` of td3_scale_moments; coeff HOST; smem_operands = 1 keeps
- *     the A operand in shared memory instead of tensor memory (same results).
+ *     scaled moments `hat` of td3_scale_moments; every 128-row run's product is summed
+ *     per destination in FP64; coeff HOST; smem_operands = 1 keeps the A operand in
+ *     shared memory instead of tensor memory (same results).
  * `status` (zeroed by the caller) receives 1 if a wait for the copies or the tensor
  * cores ran out.  Replaces fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/
  * fmm_m2l_host_pyccel.py:16-105) for fmm (src/tree_d_3d/flat_tree.py:1505-1539). */

@@ -65,8 +65,8 @@ def test_repeated_products_reuse_the_tree_and_plan_and_match_the_oracle(oracle):
 def test_few_targets_take_the_walk(oracle):
     from tree_d_3d_b200.electrodes import FMM_LEAF, FMM_ORDER, WALK_THETA, PanelSums
 
-    nodes, targets, _ = _panels(4000)
-    few = np.ascontiguousarray(targets[:, ::40])
+    nodes, targets, exclude = _panels(4000)
+    few = np.ascontiguousarray(targets[:, exclude < 0][:, ::40])  # midpoints only
     sums = PanelSums(nodes, few)
     charges = np.random.default_rng(5).normal(size=nodes.shape[1])
     phi, field = sums(charges)

@@ -237,9 +237,9 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
 // FP32 on expansions scaled by the source cell's half-width h_s.  With t' = t / h_s,
 // eps' = eps / h_s and m'_a = m_a / h_s^|a|, A_g(t; eps) = h_s^(-1-|g|) A_g(t'; eps'),
 // so T_b = (1 / b!) h_d^(-1-|b|) sum_partners (h_d / h_s)^(1+|b|) S'_b with
-// S'_b = sum_a m~'_a A~'_(a+b) (every FP32 quantity O(1); h_d / h_s a power of two,
-// applied exactly), summed per destination in FP32 and added to the FP64 locals with
-// the factor h_d^(-1-|b|) / b! in FP64.
+// S'_b = sum_a m~'_a A~'_(a+b) (every FP32 quantity O(1); inside one tree h_d / h_s is a
+// power of two and the factor exact), summed per destination in FP32 and added to the
+// FP64 locals with the factor h_d^(-1-|b|) / b! in FP64.
 template <int P>
 __global__ void __launch_bounds__(32 * CM2L_WARPS)
 k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ partners,
@@ -268,10 +268,10 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
             bool live = base + p < e1;
             i64 src = live ? partners[base + p] : 0;
             double hs = src_half[src];
-            // h_d / h_s = 2^dl exactly
-            int dl;
-            frexp(hd / hs, &dl);
-            dl -= 1;
+            // (h_d / h_s)^(1 + |b|) brings a partner's sums to the destination's scale (an
+            // exact power of two inside one tree, any ratio between a target tree and the
+            // source tree)
+            const double ratio = hd / hs;
             if (lane < CART_GROUP) {
                 double inv_h = 1.0 / hs;
                 float tx = (float)((cx - src_center[2 * src]) * inv_h);
@@ -318,6 +318,7 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
                 int k = k0 + q;
                 int nb = k < C.n_chunks ? C.chunk_nb[k] : 0, by0 = k < C.n_chunks ? C.chunk_by[k] : 0;
                 float acc[CART_CHUNK];
+                const float sc = (float)pow(ratio, (double)(1 + nb));
                 if (k < C.n_chunks) {
                     cart_chunk<float>(Mt, At, p, nb, by0, order, acc);
                 } else {
@@ -326,7 +327,7 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
                 }
 #pragma unroll
                 for (int r = 0; r < CART_CHUNK; ++r) {
-                    float a = ldexpf(acc[r], dl * (1 + nb));
+                    float a = acc[r] * sc;
                     a += __shfl_xor_sync(0xffffffffu, a, 4);
                     a += __shfl_xor_sync(0xffffffffu, a, 2);
                     a += __shfl_xor_sync(0xffffffffu, a, 1);

@@ -16,7 +16,7 @@
 // by dl lie on the lattice of the smaller half-width, t = u h_min with integer u, so T
 // depends on the key (dl, u) alone.  Every key's T is made once (FP64, split into TF32
 // hi + lo) as a 32 x 32 real matrix B: output row 2l + c, input column 2k + c' (c, c' =
-// real, imaginary; the interleaving of the scaled-moment rows), and two more rows that
+// real, imaginary; the interleaving of the scaled-moment rows), and rows 30 and 31 that
 // copy a_0 for the ln h_dst term.
 //
 // Grouping.  Destination cells are ordered, within each depth, by their quadrant in
@@ -24,25 +24,27 @@
 // lower-right: cells in the same quadrant of neighbouring parents see the same offsets)
 // and cut into tiles of 128.  The directed translations are sorted by (tile, key): a
 // (tile, key) run holds at most one translation per destination, so it is one product
-// D += A B^T of 128 rows, row m of A the scaled moments of destination m's partner at
-// that key (zero if it has none).  A tile's CTA keeps D in tensor memory across all of
-// its keys (a fixed order: deterministic sums) and adds it to the FP64 locals once.
+// D = A B^T of 128 rows, row m of A the scaled moments of destination m's partner at
+// that key (zero if it has none).  A tile's CTA sums its runs' products per destination
+// in FP64, in the runs' order (deterministic sums), and adds them to the locals once.
 // Translations off the operator table (depth differences beyond one, offsets beyond
 // the table, centres off the lattice) sort last in their tile and take the
 // per-translation FP32 formula on the CUDA cores of the same CTA.
 //
 // Per CTA (one tile, 4 warps, one row of the tile per thread):
-//   produce: the source rows of a run are fetched by bulk asynchronous copies (one per
-//     translation, into the destination's row of a shared-memory stage) and the key's
-//     B (8 KB) by one more, all counted on the stage's mbarrier; stages run up to
+//   produce: the source rows of a run are fetched by cp.async (16-byte pieces issued by
+//     the thread of each translation, into the destination's row of a shared-memory
+//     stage) and the key's B (8 KB) by one bulk copy, all counted on the stage's
+//     mbarrier (an arrival per thread and the bulk copy's bytes); stages run up to
 //     G_STAGES - 1 runs ahead;
 //   consume: each thread splits its row into TF32 hi + lo and writes it to tensor
 //     memory (tcgen05.st; or to shared memory in the canonical operand layout, the
-//     shared-memory form), then one thread issues D[:, 0:64] += A_hi [B_hi; B_lo]^T and
-//     D[:, 0:32] += A_lo B_hi^T (M = 128, K = 32 as four steps of 8) and commits them to
-//     an mbarrier; A is double-buffered, so the next run's rows go in while the
-//     products run;
-//   finish: D[:, 0:32] + D[:, 32:64] per row, the off-table translations, FP64 locals.
+//     shared-memory form), then one thread issues D = A_hi [B_hi; B_lo]^T (64 columns)
+//     and D[:, 0:32] += A_lo B_hi^T (M = 128, K = 32 as four steps of 8) into a fresh D
+//     and commits them to an mbarrier; A and D are double-buffered, so the next run's
+//     rows go in while the products run, and each run's D[:, 0:32] + D[:, 32:64] is
+//     added to the row's FP64 sums (one rounding of FP32 partial sums per run);
+//   finish: the off-table translations and the FP64 locals.
 // Every wait is bounded (a status word and a drain of the copies and products in
 // flight before the CTA releases its tensor memory).
 #include "common.cuh"
@@ -55,12 +57,15 @@ constexpr int G_STAGES = 4;
 constexpr int G_B_BYTES = 8192;   // one key: 64 rows (B_hi, B_lo) x 32 columns of TF32
 constexpr int G_LBO = 128;        // bytes between core matrices along K
 constexpr int G_SBO = 1024;       // bytes between groups of 8 rows (K = 32)
-constexpr int G_TMEM_COLS = 256;  // D [0, 64), A buffers [64, 128) and [128, 192)
+constexpr int G_TMEM_COLS = 256;  // D buffers [0, 64), [64, 128); A buffers [128, 192), [192, 256)
 constexpr int G_D_COL = 0;
-constexpr int G_A_COL = 64;
+constexpr int G_A_COL = 128;
 constexpr int G_MAX_LEVELS = 64;
 constexpr int G_MAX_SPAN = 40;
 constexpr uint32_t G_WAIT = 1u << 24;
+// output columns 30 and 31 copy a_0 (for the a_0 ln h_dst term): free for every order up
+// to 14, whose 2 (order + 1) outputs take columns 0..29
+constexpr int G_A0_ROW = 30;
 
 // The first node of every depth (start[n] = the node count), for the quadrant order.
 struct GLevels {
@@ -221,9 +226,9 @@ __global__ void k_m2l_operators(int order, const double* __restrict__ coeff, int
                 if (l == 0 && j == 0) tr += 0.5 * log(z2);
                 v = co == 0 ? (ci == 0 ? tr : -ti) : (ci == 0 ? ti : tr);
             }
-        } else if (n == 2 * W) {
+        } else if (n == G_A0_ROW) {
             v = k == 0 ? 1.0 : 0.0;
-        } else if (n == 2 * W + 1) {
+        } else if (n == G_A0_ROW + 1) {
             v = k == 1 ? 1.0 : 0.0;
         }
     }
@@ -290,12 +295,20 @@ __device__ __forceinline__ void offtable_translation(float (&v)[32], i64 d, i64 
         qi = qr * wdi + qi * wdr;
         qr = nr;
     }
+    v[G_A0_ROW] += ar[0];
+    v[G_A0_ROW + 1] += ai[0];
+}
+
+// This thread's row of a run's D (64 columns at taddr): D[:, 0:32] + D[:, 32:64] added to
+// the FP64 sums (when the row took part in the run).
+template <int V>
+__device__ __forceinline__ void read_out(uint32_t taddr, bool use, double (&acc)[V]) {
+    float d0[32], d1[32];
+    td3tc::tmem_load32(taddr, d0);
+    td3tc::tmem_load32(taddr + 32, d1);
+    if (use) {
 #pragma unroll
-    for (int j = 0; j < 32; j += 2) {
-        if (j == 2 * w) {
-            v[j] += ar[0];
-            v[j + 1] += ai[0];
-        }
+        for (int k = 0; k < V; ++k) acc[k] += (double)d0[k] + (double)d1[k];
     }
 }
 
@@ -308,6 +321,7 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
               int key_bits, unsigned offtable_key, const GCoef<P> C,
               double* __restrict__ local_re, double* __restrict__ local_im, i64* status) {
     using S = GShape<P>;
+    constexpr int V = 32;  // outputs per row: bhat_l (re, im) in 0..2P+1, a_0 in 30, 31
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
     const int tile = blockIdx.x;
@@ -317,7 +331,6 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
     const int jm = (keys[run_start[j1 - 1]] & key_mask) == offtable_key ? j1 - 1 : j1;
     const int n_mma = jm - j0;
     const int w = order + 1, hw = td3_hat_width(order);
-    const uint32_t row_bytes = (uint32_t)hw * 8;
     const int chunks = hw / 2;  // 16-byte chunks of a row
 
     unsigned char* stage_b = smem + S::OFF_B;
@@ -329,7 +342,9 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_mma + 2);
 
     if (tid == 0) {
-        for (int s = 0; s < G_STAGES; ++s) td3tc::mbar_init(&bar_stage[s], 1);
+        // a stage completes when every thread's row copies have landed (one arrival per
+        // thread) and the key's B (bytes) is in
+        for (int s = 0; s < G_STAGES; ++s) td3tc::mbar_init(&bar_stage[s], G_THREADS);
         td3tc::mbar_init(&bar_mma[0], 1);
         td3tc::mbar_init(&bar_mma[1], 1);
     }
@@ -341,13 +356,14 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
     const uint32_t tmem = *tmem_slot;
     const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
 
-    // run j0 + i into stage i % G_STAGES
+    // run j0 + i into stage i % G_STAGES: the rows by cp.async (each by the thread of its
+    // translation), B by one bulk copy; every thread arrives once
     auto produce = [&](int i) {
         int s = i % G_STAGES, j = j0 + i;
         int a = run_start[j], cnt = run_start[j + 1] - a;
-        unsigned key = keys[a] & key_mask;
         if (tid == 0) {
-            td3tc::mbar_arrive_expect_tx(&bar_stage[s], (uint32_t)cnt * row_bytes + G_B_BYTES);
+            unsigned key = keys[a] & key_mask;
+            td3tc::mbar_expect_tx(&bar_stage[s], G_B_BYTES);
             td3tc::bulk_g2s(stage_b + s * G_B_BYTES, ops + (size_t)key * (G_B_BYTES / 4), G_B_BYTES,
                             &bar_stage[s]);
         }
@@ -355,26 +371,30 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
             unsigned v = vals[a + tid];
             unsigned m = v & 127u;
             live[s * G_THREADS + m] = 1;
-            td3tc::bulk_g2s(stage_a + s * S::STAGE_A + m * S::STRIDE, hat + (size_t)(v >> 7) * hw,
-                            row_bytes, &bar_stage[s]);
+            const unsigned char* src =
+                reinterpret_cast<const unsigned char*>(hat + (size_t)(v >> 7) * hw);
+            unsigned char* dst = stage_a + s * S::STAGE_A + m * S::STRIDE;
+            for (int c = 0; c < chunks; ++c) td3tc::cp_async16(dst + 16 * c, src + 16 * c);
         }
+        td3tc::cp_async_arrive(&bar_stage[s]);
     };
 
-    bool failed = false, touched = false;
+    double acc[V];
+#pragma unroll
+    for (int k = 0; k < V; ++k) acc[k] = 0.0;
+    bool failed = false, warp_failed = false, touched = false, prev_live = false;
     int produced = 0, issued = 0;
     const int pre = n_mma < G_STAGES - 1 ? n_mma : G_STAGES - 1;
     for (; produced < pre; ++produced) produce(produced);
+
+    // D of run i in columns [64 (i & 1), +64); A of run i in [128 + 64 (i & 1), +64)
+
     for (int i = 0; i < n_mma; ++i) {
         const int s = i % G_STAGES;
         bool ok = td3tc::mbar_wait(&bar_stage[s], (uint32_t)(i / G_STAGES) & 1u, G_WAIT);
-        if (i >= 2) ok = ok && td3tc::mbar_wait(&bar_mma[i & 1], (uint32_t)((i - 2) >> 1) & 1u, G_WAIT);
-        if (!__syncthreads_and(ok)) {
-            failed = true;
-            break;
-        }
         // this thread's row: split into TF32 hi + lo
         float hi[32], lo[32];
-        const bool is_live = live[s * G_THREADS + tid] != 0;
+        const bool is_live = ok && live[s * G_THREADS + tid] != 0;
         touched |= is_live;
         const float4* row = reinterpret_cast<const float4*>(stage_a + s * S::STAGE_A + tid * S::STRIDE);
 #pragma unroll
@@ -406,24 +426,27 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
         }
         live[s * G_THREADS + tid] = 0;
         td3tc::fence_before_sync();
-        __syncthreads();
+        if (__syncthreads_or(!ok || warp_failed)) {  // one decision for the whole block
+            failed = true;
+            break;
+        }
         td3tc::fence_after_sync();
         if (tid == 0) {
             constexpr uint32_t id64 = td3tc::idesc_tf32(G_THREADS, 64);
             constexpr uint32_t id32 = td3tc::idesc_tf32(G_THREADS, 32);
             const uint32_t bb = td3tc::smem_addr(stage_b + s * G_B_BYTES);
+            const uint32_t d = tmem + G_D_COL + 64 * (i & 1);
 #pragma unroll
             for (int ks = 0; ks < 4; ++ks) {
                 uint64_t db = td3tc::smem_desc(bb + 2 * G_LBO * ks, G_LBO, G_SBO);
-                uint32_t acc = (i > 0 || ks > 0) ? 1u : 0u;
+                uint32_t accum = ks > 0 ? 1u : 0u;  // a fresh D for every run
                 if (SMEM_A) {
                     uint64_t da = td3tc::smem_desc(
                         td3tc::smem_addr(op_a + (i & 1) * (2 * G_THREADS * 128)) + 2 * G_LBO * ks,
                         G_LBO, G_SBO);
-                    td3tc::mma_tf32(tmem + G_D_COL, da, db, id64, acc);
+                    td3tc::mma_tf32(d, da, db, id64, accum);
                 } else {
-                    td3tc::mma_tf32_ts(tmem + G_D_COL, tmem + G_A_COL + 64 * (i & 1) + 8 * ks, db,
-                                       id64, acc);
+                    td3tc::mma_tf32_ts(d, tmem + G_A_COL + 64 * (i & 1) + 8 * ks, db, id64, accum);
                 }
             }
 #pragma unroll
@@ -434,80 +457,76 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                         td3tc::smem_addr(op_a + (i & 1) * (2 * G_THREADS * 128) + G_THREADS * 128) +
                             2 * G_LBO * ks,
                         G_LBO, G_SBO);
-                    td3tc::mma_tf32(tmem + G_D_COL, da, db, id32, 1u);
+                    td3tc::mma_tf32(d, da, db, id32, 1u);
                 } else {
-                    td3tc::mma_tf32_ts(tmem + G_D_COL, tmem + G_A_COL + 64 * (i & 1) + 32 + 8 * ks,
-                                       db, id32, 1u);
+                    td3tc::mma_tf32_ts(d, tmem + G_A_COL + 64 * (i & 1) + 32 + 8 * ks, db, id32,
+                                       1u);
                 }
             }
             td3tc::mma_commit(&bar_mma[i & 1]);
         }
         issued = i + 1;
-        // refill the stage of run i - 1 once its products (which read its B) are done
-        if (produced < n_mma) {
-            bool done = i < 1 ||
-                        td3tc::mbar_wait(&bar_mma[(i - 1) & 1], (uint32_t)((i - 1) >> 1) & 1u, G_WAIT);
-            if (!__syncthreads_and(done)) {
-                failed = true;
-                break;
+        // the previous run: its products are done, its D is summed in FP64 and its stage
+        // (whose B they read) takes the next run
+        if (i >= 1) {
+            bool done = td3tc::mbar_wait(&bar_mma[(i - 1) & 1], (uint32_t)((i - 1) >> 1) & 1u, G_WAIT);
+            done = __all_sync(0xffffffffu, done);
+            if (done) {
+                td3tc::fence_after_sync();
+                read_out<V>(tmem + lane_base + G_D_COL + 64 * ((i - 1) & 1), prev_live, acc);
+            } else {
+                warp_failed = true;
             }
+        }
+        prev_live = is_live;
+        if (produced < n_mma && !warp_failed) {
             produce(produced);
             ++produced;
         }
     }
-
-    float v[32];
-#pragma unroll
-    for (int k = 0; k < 32; ++k) v[k] = 0.0f;
     if (!failed && issued > 0) {
-        bool ok = td3tc::mbar_wait(&bar_mma[(issued - 1) & 1], (uint32_t)((issued - 1) >> 1) & 1u,
-                                   G_WAIT);
-        if (!__syncthreads_and(ok)) {
-            failed = true;
-        } else {
+        bool done = td3tc::mbar_wait(&bar_mma[(issued - 1) & 1], (uint32_t)((issued - 1) >> 1) & 1u,
+                                     G_WAIT);
+        if (__syncthreads_and(done)) {
             td3tc::fence_after_sync();
-            float d0[32], d1[32];
-            td3tc::tmem_load32(tmem + lane_base + G_D_COL, d0);
-            td3tc::tmem_load32(tmem + lane_base + G_D_COL + 32, d1);
-#pragma unroll
-            for (int k = 0; k < 32; ++k) v[k] = d0[k] + d1[k];
+            read_out<V>(tmem + lane_base + G_D_COL + 64 * ((issued - 1) & 1), prev_live, acc);
+        } else {
+            failed = true;
         }
     }
     if (failed) {
         if (tid == 0) td3_report(status, 1);
-        // drain: the copies of every produced, unconsumed stage and the last products
+        // drain: the copies of every produced stage not yet consumed and the products
         for (int i = issued; i < produced; ++i)
             td3tc::mbar_wait(&bar_stage[i % G_STAGES], (uint32_t)(i / G_STAGES) & 1u, G_WAIT);
-        if (issued > 0)
-            td3tc::mbar_wait(&bar_mma[(issued - 1) & 1], (uint32_t)((issued - 1) >> 1) & 1u, G_WAIT);
+        for (int i = issued - 2 < 0 ? 0 : issued - 2; i < issued; ++i)
+            td3tc::mbar_wait(&bar_mma[i & 1], (uint32_t)(i >> 1) & 1u, G_WAIT);
     } else {
         const i64 qp = (i64)tile * G_THREADS + tid;
         const i64 d = qp < n_nodes ? node_at(L, qp) : -1;
         // translations off the operator table: this row's, in the sorted order
         if (jm < j1 && d >= 0) {
+            float fv[32];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) fv[k] = 0.0f;
             for (int e = run_start[jm], e1 = run_start[jm + 1]; e < e1; ++e) {
                 unsigned val = vals[e];
                 if ((int)(val & 127u) != tid) continue;
-                offtable_translation<P>(v, d, (i64)(val >> 7), order, center, half, hat, C);
+                offtable_translation<P>(fv, d, (i64)(val >> 7), order, center, half, hat, C);
                 touched = true;
             }
+#pragma unroll
+            for (int k = 0; k < V; ++k) acc[k] += (double)fv[k];
         }
         if (touched && d >= 0) {
             double hd = half[d], inv_h = 1.0 / hd, ln_h = log(hd), scale = 1.0;
-            double a0r = 0.0, a0i = 0.0;
+            const double a0r = acc[G_A0_ROW], a0i = acc[G_A0_ROW + 1];
 #pragma unroll
-            for (int j = 0; j < 32; j += 2) {
-                if (j == 2 * w) {
-                    a0r = (double)v[j];
-                    a0i = (double)v[j + 1];
-                }
-            }
-#pragma unroll
-            for (int l = 0; l < 16; ++l) {
+            for (int l = 0; l <= P; ++l) {
                 if (l < w) {
                     double ur = l ? 0.0 : ln_h * a0r, ui = l ? 0.0 : ln_h * a0i;
-                    local_re[d * w + l] += (double)v[2 * l] * scale + ur;
-                    local_im[d * w + l] += (double)v[2 * l + 1] * scale + ui;
+                    local_re[d * w + l] += acc[2 * l] * scale + ur;
+                    local_im[d * w + l] += acc[2 * l + 1] * scale + ui;
                 }
                 scale *= inv_h;
             }

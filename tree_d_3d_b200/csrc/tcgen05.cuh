@@ -180,6 +180,29 @@ __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t by
                  : "memory");
 }
 
+// `bytes` more bytes of asynchronous copies expected in the current phase of `bar`,
+// without an arrival.
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// 16 bytes from global to shared memory through the load/store path (both addresses
+// 16-byte aligned), bypassing L1; completion tracked by cp_async_arrive.
+__device__ __forceinline__ void cp_async16(void* dst_smem, const void* src_global) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst_smem)),
+                 "l"(src_global)
+                 : "memory");
+}
+
+// One arrival on `bar`, made once every cp.async this thread issued before it has
+// landed (the barrier's expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_addr(bar))
+                 : "memory");
+}
+
 // Asynchronous copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
 // this GPU's global memory into this CTA's shared memory, its bytes counted on `bar`.
 // No multicast: the copy lands in the issuing CTA only.

@@ -182,12 +182,15 @@ NEAR_SEGMENT = 256
 M2L_TENSOR_CORES = False
 
 #: the log kernel's downward pass in one launch (each leaf's local from its ancestors'
-#: own locals) instead of one L2L launch per level
-DOWNWARD_LEAVES = True
+#: own locals) instead of one L2L launch per level.  Off: at 1M particles the ancestor
+#: walks take 1.5 ms per pass against 0.2 ms for the per-level launches.
+DOWNWARD_LEAVES = False
 
 #: the log kernel's upward pass in one launch (orders up to 12; the last child to finish
-#: forms its parent) instead of one M2M launch per level; the same bits either way
-MOMENTS_ONE_LAUNCH = True
+#: forms its parent) instead of one M2M launch per level; the same bits either way.
+#: Off: its register use (244 per thread) leaves it at 0.55 ms per pass at 1M against
+#: 0.22 ms for the per-level launches.
+MOMENTS_ONE_LAUNCH = False
 
 #: the mixed-precision M2L of ``fmm`` (mutual lists, log kernel, orders up to 14) as
 #: tensor-core products grouped by translation (td3_m2l_groups, td3_fmm_m2l_grouped)
