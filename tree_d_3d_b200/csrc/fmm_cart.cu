@@ -148,7 +148,6 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
                  i64 n_dst, const double* __restrict__ dst_center,
                  const double* __restrict__ src_center, const double* __restrict__ moments,
                  int order, double eps2, const CartScale C, double* __restrict__ local) {
-    constexpr int W = P + 1;
     extern __shared__ double cart_smem[];
     td3_chain_wait();
     td3_chain_release();
@@ -169,40 +168,43 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
             __syncwarp();
             bool live = base + p < e1;
             i64 src = live ? partners[base + p] : 0;
-            if (lane < CART_GROUP) {
+            // partner p's A~, degree by degree: its four lanes (q) share each degree's g_y
+            // (a degree reads the two below it)
+            {
                 double tx = cx - src_center[2 * src], ty = cy - src_center[2 * src + 1];
-                // a lane past the row's end builds a zero column (finite scale)
+                // a partner past the row's end builds a zero column (finite scale)
                 double r2 = live ? tx * tx + ty * ty + eps2 : 1.0;
-                double prev2[W], prev1[W], cur[W];
-                prev1[0] = live ? 1.0 / sqrt(r2) : 0.0;
-                At[p] = prev1[0];
                 double inv_r2 = 1.0 / r2;
-#pragma unroll
-                for (int n = 1; n < W; ++n) {
-                    if (n > order) break;
+                if (q == 0) At[p] = live ? 1.0 / sqrt(r2) : 0.0;
+                __syncwarp();
+#pragma unroll 1
+                for (int n = 1; n <= order; ++n) {
                     double scale = -inv_r2 / n;
-#pragma unroll
-                    for (int gy = 0; gy <= n; ++gy) {
+                    const double* prev1 = At + ((n - 1) * n / 2) * CART_GROUP + p;
+                    const double* prev2 = At + (n >= 2 ? (n - 2) * (n - 1) / 2 : 0) * CART_GROUP + p;
+                    for (int gy = q; gy <= n; gy += 4) {
                         int gx = n - gy;
                         double s = 0.0;
-                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy];
-                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[gy - 1];
-                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy];
-                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[gy - 2];
-                        cur[gy] = s * scale;
-                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = cur[gy];
+                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy * CART_GROUP];
+                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[(gy - 1) * CART_GROUP];
+                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy * CART_GROUP];
+                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[(gy - 2) * CART_GROUP];
+                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = s * scale;
                     }
-#pragma unroll
-                    for (int k = 0; k < W; ++k) {
-                        prev2[k] = prev1[k];
-                        prev1[k] = cur[k];
-                    }
+                    __syncwarp();
                 }
-            } else if (lane < 2 * CART_GROUP) {
-                const double* m = moments + src * n_coef;
-                for (int a = 0; a < n_coef; ++a) {
-                    double v = live ? m[a] * C.inv_fact2[a] : 0.0;
-                    Mt[a * CART_GROUP + p] = ((C.bx[a] + C.by[a]) & 1) ? -v : v;
+            }
+            // the eight partners' scaled moments, every lane loading consecutive
+            // coefficients of one partner (coalesced)
+            for (int i0 = 0; i0 < CART_GROUP * n_coef; i0 += 32) {
+                int idx = i0 + lane;
+                int pp = idx / n_coef;
+                i64 s2 = __shfl_sync(0xffffffffu, src, pp & (CART_GROUP - 1));
+                bool l2 = __shfl_sync(0xffffffffu, live, pp & (CART_GROUP - 1));
+                if (pp < CART_GROUP) {
+                    int a = idx - pp * n_coef;
+                    double v = l2 ? moments[s2 * n_coef + a] * C.inv_fact2[a] : 0.0;
+                    Mt[a * CART_GROUP + pp] = ((C.bx[a] + C.by[a]) & 1) ? -v : v;
                 }
             }
             __syncwarp();
@@ -247,7 +249,6 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
                  const double* __restrict__ dst_half, const double* __restrict__ src_center,
                  const double* __restrict__ src_half, const double* __restrict__ moments,
                  int order, double eps2, const CartScale C, double* __restrict__ local) {
-    constexpr int W = P + 1;
     extern __shared__ float cart_smem_f[];
     td3_chain_wait();
     td3_chain_release();
@@ -272,53 +273,60 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
             // exact power of two inside one tree, any ratio between a target tree and the
             // source tree)
             const double ratio = hd / hs;
-            if (lane < CART_GROUP) {
+            // partner p's A~ in units of h_s, degree by degree: its four lanes (q) share
+            // each degree's g_y
+            {
                 double inv_h = 1.0 / hs;
                 float tx = (float)((cx - src_center[2 * src]) * inv_h);
                 float ty = (float)((cy - src_center[2 * src + 1]) * inv_h);
                 float r2 = live ? (float)((double)tx * tx + (double)ty * ty + eps2 * inv_h * inv_h)
                                 : 1.0f;
-                float prev2[W], prev1[W], cur[W];
-                prev1[0] = live ? rsqrtf(r2) : 0.0f;
-                At[p] = prev1[0];
                 float inv_r2 = 1.0f / r2;
-#pragma unroll
-                for (int n = 1; n < W; ++n) {
-                    if (n > order) break;
+                if (q == 0) At[p] = live ? rsqrtf(r2) : 0.0f;
+                __syncwarp();
+#pragma unroll 1
+                for (int n = 1; n <= order; ++n) {
                     float scale = -inv_r2 / n;
-#pragma unroll
-                    for (int gy = 0; gy <= n; ++gy) {
+                    const float* prev1 = At + ((n - 1) * n / 2) * CART_GROUP + p;
+                    const float* prev2 = At + (n >= 2 ? (n - 2) * (n - 1) / 2 : 0) * CART_GROUP + p;
+                    for (int gy = q; gy <= n; gy += 4) {
                         int gx = n - gy;
                         float s = 0.0f;
-                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy];
-                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[gy - 1];
-                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy];
-                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[gy - 2];
-                        cur[gy] = s * scale;
-                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = cur[gy];
+                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy * CART_GROUP];
+                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[(gy - 1) * CART_GROUP];
+                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy * CART_GROUP];
+                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[(gy - 2) * CART_GROUP];
+                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = s * scale;
                     }
-#pragma unroll
-                    for (int k = 0; k < W; ++k) {
-                        prev2[k] = prev1[k];
-                        prev1[k] = cur[k];
-                    }
-                }
-            } else if (lane < 2 * CART_GROUP) {
-                const double* m = moments + src * n_coef;
-                double inv_h = 1.0 / hs, pw = 1.0;
-                for (int n = 0, a = 0; n <= order; ++n, pw *= inv_h) {
-                    for (int y = 0; y <= n; ++y, ++a) {
-                        double v = live ? m[a] * C.inv_fact2[a] * pw : 0.0;
-                        Mt[a * CART_GROUP + p] = (float)((n & 1) ? -v : v);
-                    }
+                    __syncwarp();
                 }
             }
+            // the eight partners' moments in units of their h_s, every lane loading
+            // consecutive coefficients of one partner (coalesced)
+            for (int i0 = 0; i0 < CART_GROUP * n_coef; i0 += 32) {
+                int idx = i0 + lane;
+                int pp = idx / n_coef;
+                i64 s2 = __shfl_sync(0xffffffffu, src, pp & (CART_GROUP - 1));
+                bool l2 = __shfl_sync(0xffffffffu, live, pp & (CART_GROUP - 1));
+                double h2 = __shfl_sync(0xffffffffu, hs, pp & (CART_GROUP - 1));
+                if (pp < CART_GROUP) {
+                    int a = idx - pp * n_coef, n = C.bx[a] + C.by[a];
+                    double inv_h = 1.0 / h2, pw = 1.0;
+                    for (int k = 0; k < n; ++k) pw *= inv_h;
+                    double v = l2 ? moments[s2 * n_coef + a] * C.inv_fact2[a] * pw : 0.0;
+                    Mt[a * CART_GROUP + pp] = (float)((n & 1) ? -v : v);
+                }
+            }
+            // ratio^(1 + nb) for this lane's chunks (their degrees only grow)
+            double rpow = ratio;
+            int rpow_nb = 0;
             __syncwarp();
             for (int k0 = 0; k0 < C.n_chunks; k0 += 4) {
                 int k = k0 + q;
                 int nb = k < C.n_chunks ? C.chunk_nb[k] : 0, by0 = k < C.n_chunks ? C.chunk_by[k] : 0;
                 float acc[CART_CHUNK];
-                const float sc = (float)pow(ratio, (double)(1 + nb));
+                for (; rpow_nb < nb; ++rpow_nb) rpow *= ratio;
+                const float sc = (float)rpow;
                 if (k < C.n_chunks) {
                     cart_chunk<float>(Mt, At, p, nb, by0, order, acc);
                 } else {
