@@ -299,16 +299,18 @@ __device__ __forceinline__ void offtable_translation(float (&v)[32], i64 d, i64 
     v[G_A0_ROW + 1] += ai[0];
 }
 
-// This thread's row of a run's D (64 columns at taddr): D[:, 0:32] + D[:, 32:64] added to
-// the FP64 sums (when the row took part in the run).
-template <int V>
+// This thread's row of a run's D (64 columns at taddr): D[:, 0:32] + D[:, 32:64] (the
+// second half a correction about 2^-11 of the first, added in FP32) added to the FP64
+// sums, for the columns an order up to P uses (when the row took part in the run).
+template <int P, int V>
 __device__ __forceinline__ void read_out(uint32_t taddr, bool use, double (&acc)[V]) {
     float d0[32], d1[32];
     td3tc::tmem_load32(taddr, d0);
     td3tc::tmem_load32(taddr + 32, d1);
     if (use) {
 #pragma unroll
-        for (int k = 0; k < V; ++k) acc[k] += (double)d0[k] + (double)d1[k];
+        for (int k = 0; k < V; ++k)
+            if (k < 2 * (P + 1) || k >= G_A0_ROW) acc[k] += (double)(d0[k] + d1[k]);
     }
 }
 
@@ -473,7 +475,7 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
             done = __all_sync(0xffffffffu, done);
             if (done) {
                 td3tc::fence_after_sync();
-                read_out<V>(tmem + lane_base + G_D_COL + 64 * ((i - 1) & 1), prev_live, acc);
+                read_out<P, V>(tmem + lane_base + G_D_COL + 64 * ((i - 1) & 1), prev_live, acc);
             } else {
                 warp_failed = true;
             }
@@ -489,7 +491,7 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                                      G_WAIT);
         if (__syncthreads_and(done)) {
             td3tc::fence_after_sync();
-            read_out<V>(tmem + lane_base + G_D_COL + 64 * ((issued - 1) & 1), prev_live, acc);
+            read_out<P, V>(tmem + lane_base + G_D_COL + 64 * ((issued - 1) & 1), prev_live, acc);
         } else {
             failed = true;
         }
