@@ -328,19 +328,20 @@ int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
  * dl = -1, 0, 1 and whose centres differ by t = u h_min (u an integer vector with
  * |u_x|, |u_y| <= span, h_min the smaller half-width) is the fixed matrix of the key
  * (dl, u) on size-scaled expansions; the other translations take the per-translation
- * FP32 formula.  Three calls:
+ * formula in FP64.  Three calls:
  *   td3_m2l_operators: the 3 (2 span + 1)^2 keys' matrices into `ops`
  *     (td3_m2l_operators_size(span) bytes, float; coeff the reference's M2L matrix,
  *     DEVICE, (order + 1)^2); depends on (order, coeff, span) only;
  *   td3_m2l_groups: the directed translations of `pairs` (n_pairs, 2) sorted by
- *     (tile of 128 destinations, key) into keys / values (2 n_pairs each), the run
+ *     (tile of 128 destinations, key; an off-table translation's key is
+ *     3 (2 span + 1)^2 + its row in the tile) into keys / values (2 n_pairs each), the run
  *     starts run_start (2 n_pairs + 1) and the first run of every tile tile_run
  *     (ceil(n_nodes / 128) + 1); levels HOST (n_levels + 1, the first node of each
  *     depth, then n_nodes); n_nodes < 2^25; depends on the tree and the lists only;
  *   td3_fmm_m2l_grouped: the products into local_re / local_im (FP64, added), from the
- *     scaled moments `hat` of td3_scale_moments; every 128-row run's product is summed
- *     per destination in FP64; coeff HOST; smem_operands = 1 keeps the A operand in
- *     shared memory instead of tensor memory (same results).
+ *     scaled moments `hat` of td3_scale_moments; the products of up to 4 runs of a tile
+ *     are summed in FP32 on the tensor cores, then per destination in FP64, in the runs'
+ *     order (deterministic); coeff HOST.
  * `status` (zeroed by the caller) receives 1 if a wait for the copies or the tensor
  * cores ran out.  Replaces fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/
  * fmm_m2l_host_pyccel.py:16-105) for fmm (src/tree_d_3d/flat_tree.py:1505-1539). */
@@ -357,8 +358,8 @@ int td3_fmm_m2l_grouped(const int32_t* tile_run, const int32_t* run_start,
                         const uint32_t* keys, const uint32_t* values, int64_t n_nodes,
                         const int64_t* levels, int64_t n_levels, const double* node_center,
                         const double* node_half, const float* hat, int order, const float* ops,
-                        int span, const double* coeff, int smem_operands, double* local_re,
-                        double* local_im, int64_t* status, void* stream);
+                        int span, const double* coeff, double* local_re, double* local_im,
+                        int64_t* status, void* stream);
 
 /* The parent of every node (node_parent (count), int32; -1 for the root), from
  * node_child.  No reference counterpart (its walks keep explicit stacks). */

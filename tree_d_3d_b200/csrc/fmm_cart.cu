@@ -148,6 +148,7 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
                  i64 n_dst, const double* __restrict__ dst_center,
                  const double* __restrict__ src_center, const double* __restrict__ moments,
                  int order, double eps2, const CartScale C, double* __restrict__ local) {
+    constexpr int W = P + 1;
     extern __shared__ double cart_smem[];
     td3_chain_wait();
     td3_chain_release();
@@ -168,43 +169,40 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
             __syncwarp();
             bool live = base + p < e1;
             i64 src = live ? partners[base + p] : 0;
-            // partner p's A~, degree by degree: its four lanes (q) share each degree's g_y
-            // (a degree reads the two below it)
-            {
+            if (lane < CART_GROUP) {
                 double tx = cx - src_center[2 * src], ty = cy - src_center[2 * src + 1];
-                // a partner past the row's end builds a zero column (finite scale)
+                // a lane past the row's end builds a zero column (finite scale)
                 double r2 = live ? tx * tx + ty * ty + eps2 : 1.0;
+                double prev2[W], prev1[W], cur[W];
+                prev1[0] = live ? 1.0 / sqrt(r2) : 0.0;
+                At[p] = prev1[0];
                 double inv_r2 = 1.0 / r2;
-                if (q == 0) At[p] = live ? 1.0 / sqrt(r2) : 0.0;
-                __syncwarp();
-#pragma unroll 1
-                for (int n = 1; n <= order; ++n) {
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    if (n > order) break;
                     double scale = -inv_r2 / n;
-                    const double* prev1 = At + ((n - 1) * n / 2) * CART_GROUP + p;
-                    const double* prev2 = At + (n >= 2 ? (n - 2) * (n - 1) / 2 : 0) * CART_GROUP + p;
-                    for (int gy = q; gy <= n; gy += 4) {
+#pragma unroll
+                    for (int gy = 0; gy <= n; ++gy) {
                         int gx = n - gy;
                         double s = 0.0;
-                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy * CART_GROUP];
-                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[(gy - 1) * CART_GROUP];
-                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy * CART_GROUP];
-                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[(gy - 2) * CART_GROUP];
-                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = s * scale;
+                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy];
+                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[gy - 1];
+                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy];
+                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[gy - 2];
+                        cur[gy] = s * scale;
+                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = cur[gy];
                     }
-                    __syncwarp();
+#pragma unroll
+                    for (int k = 0; k < W; ++k) {
+                        prev2[k] = prev1[k];
+                        prev1[k] = cur[k];
+                    }
                 }
-            }
-            // the eight partners' scaled moments, every lane loading consecutive
-            // coefficients of one partner (coalesced)
-            for (int i0 = 0; i0 < CART_GROUP * n_coef; i0 += 32) {
-                int idx = i0 + lane;
-                int pp = idx / n_coef;
-                i64 s2 = __shfl_sync(0xffffffffu, src, pp & (CART_GROUP - 1));
-                bool l2 = __shfl_sync(0xffffffffu, live, pp & (CART_GROUP - 1));
-                if (pp < CART_GROUP) {
-                    int a = idx - pp * n_coef;
-                    double v = l2 ? moments[s2 * n_coef + a] * C.inv_fact2[a] : 0.0;
-                    Mt[a * CART_GROUP + pp] = ((C.bx[a] + C.by[a]) & 1) ? -v : v;
+            } else if (lane < 2 * CART_GROUP) {
+                const double* m = moments + src * n_coef;
+                for (int a = 0; a < n_coef; ++a) {
+                    double v = live ? m[a] * C.inv_fact2[a] : 0.0;
+                    Mt[a * CART_GROUP + p] = ((C.bx[a] + C.by[a]) & 1) ? -v : v;
                 }
             }
             __syncwarp();
@@ -236,12 +234,13 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
 }
 
 // The mixed-precision form of k_m2l_cart_lanes: the same partners-by-eight layout in
-// FP32 on expansions scaled by the source cell's half-width h_s.  With t' = t / h_s,
-// eps' = eps / h_s and m'_a = m_a / h_s^|a|, A_g(t; eps) = h_s^(-1-|g|) A_g(t'; eps'),
-// so T_b = (1 / b!) h_d^(-1-|b|) sum_partners (h_d / h_s)^(1+|b|) S'_b with
-// S'_b = sum_a m~'_a A~'_(a+b) (every FP32 quantity O(1); inside one tree h_d / h_s is a
-// power of two and the factor exact), summed per destination in FP32 and added to the
-// FP64 locals with the factor h_d^(-1-|b|) / b! in FP64.
+// FP32 on expansions scaled by a unit h = max(h_src, h_dst) per partner.  With t' = t / h,
+// eps' = eps / h and m'_a = m_a / h^|a|, A_g(t; eps) = h^(-1-|g|) A_g(t'; eps'), so
+// T_b = (1 / b!) h_d^(-1-|b|) sum_partners (h_d / h)^(1+|b|) S'_b with
+// S'_b = sum_a m~'_a A~'_(a+b): every FP32 quantity O(1) and the factor at most 1 (a
+// cell far smaller than its partner, which the lists hold, overflows neither way; inside
+// one tree the factor is a power of two and exact), summed per destination in FP32 and
+// added to the FP64 locals with the factor h_d^(-1-|b|) / b! in FP64.
 template <int P>
 __global__ void __launch_bounds__(32 * CM2L_WARPS)
 k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ partners,
@@ -249,6 +248,7 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
                  const double* __restrict__ dst_half, const double* __restrict__ src_center,
                  const double* __restrict__ src_half, const double* __restrict__ moments,
                  int order, double eps2, const CartScale C, double* __restrict__ local) {
+    constexpr int W = P + 1;
     extern __shared__ float cart_smem_f[];
     td3_chain_wait();
     td3_chain_release();
@@ -268,53 +268,50 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
             __syncwarp();
             bool live = base + p < e1;
             i64 src = live ? partners[base + p] : 0;
-            double hs = src_half[src];
-            // (h_d / h_s)^(1 + |b|) brings a partner's sums to the destination's scale (an
-            // exact power of two inside one tree, any ratio between a target tree and the
-            // source tree)
+            // the partner's unit h = max(h_s, h_d): the moments / h^|a| and A~ at t / h stay
+            // O(1), and (h_d / h)^(1 + |b|) <= 1 brings its sums to the destination's scale
+            // (an exact power of two inside one tree)
+            double hs = fmax(src_half[src], hd);
             const double ratio = hd / hs;
-            // partner p's A~ in units of h_s, degree by degree: its four lanes (q) share
-            // each degree's g_y
-            {
+            if (lane < CART_GROUP) {
                 double inv_h = 1.0 / hs;
                 float tx = (float)((cx - src_center[2 * src]) * inv_h);
                 float ty = (float)((cy - src_center[2 * src + 1]) * inv_h);
                 float r2 = live ? (float)((double)tx * tx + (double)ty * ty + eps2 * inv_h * inv_h)
                                 : 1.0f;
+                float prev2[W], prev1[W], cur[W];
+                prev1[0] = live ? rsqrtf(r2) : 0.0f;
+                At[p] = prev1[0];
                 float inv_r2 = 1.0f / r2;
-                if (q == 0) At[p] = live ? rsqrtf(r2) : 0.0f;
-                __syncwarp();
-#pragma unroll 1
-                for (int n = 1; n <= order; ++n) {
+#pragma unroll
+                for (int n = 1; n < W; ++n) {
+                    if (n > order) break;
                     float scale = -inv_r2 / n;
-                    const float* prev1 = At + ((n - 1) * n / 2) * CART_GROUP + p;
-                    const float* prev2 = At + (n >= 2 ? (n - 2) * (n - 1) / 2 : 0) * CART_GROUP + p;
-                    for (int gy = q; gy <= n; gy += 4) {
+#pragma unroll
+                    for (int gy = 0; gy <= n; ++gy) {
                         int gx = n - gy;
                         float s = 0.0f;
-                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy * CART_GROUP];
-                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[(gy - 1) * CART_GROUP];
-                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy * CART_GROUP];
-                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[(gy - 2) * CART_GROUP];
-                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = s * scale;
+                        if (gx >= 1) s += (2 * n - 1) * tx * gx * prev1[gy];
+                        if (gy >= 1) s += (2 * n - 1) * ty * gy * prev1[gy - 1];
+                        if (gx >= 2) s += (n - 1) * (gx * (gx - 1)) * prev2[gy];
+                        if (gy >= 2) s += (n - 1) * (gy * (gy - 1)) * prev2[gy - 2];
+                        cur[gy] = s * scale;
+                        At[(n * (n + 1) / 2 + gy) * CART_GROUP + p] = cur[gy];
                     }
-                    __syncwarp();
+#pragma unroll
+                    for (int k = 0; k < W; ++k) {
+                        prev2[k] = prev1[k];
+                        prev1[k] = cur[k];
+                    }
                 }
-            }
-            // the eight partners' moments in units of their h_s, every lane loading
-            // consecutive coefficients of one partner (coalesced)
-            for (int i0 = 0; i0 < CART_GROUP * n_coef; i0 += 32) {
-                int idx = i0 + lane;
-                int pp = idx / n_coef;
-                i64 s2 = __shfl_sync(0xffffffffu, src, pp & (CART_GROUP - 1));
-                bool l2 = __shfl_sync(0xffffffffu, live, pp & (CART_GROUP - 1));
-                double h2 = __shfl_sync(0xffffffffu, hs, pp & (CART_GROUP - 1));
-                if (pp < CART_GROUP) {
-                    int a = idx - pp * n_coef, n = C.bx[a] + C.by[a];
-                    double inv_h = 1.0 / h2, pw = 1.0;
-                    for (int k = 0; k < n; ++k) pw *= inv_h;
-                    double v = l2 ? moments[s2 * n_coef + a] * C.inv_fact2[a] * pw : 0.0;
-                    Mt[a * CART_GROUP + pp] = (float)((n & 1) ? -v : v);
+            } else if (lane < 2 * CART_GROUP) {
+                const double* m = moments + src * n_coef;
+                double inv_h = 1.0 / hs, pw = 1.0;
+                for (int n = 0, a = 0; n <= order; ++n, pw *= inv_h) {
+                    for (int y = 0; y <= n; ++y, ++a) {
+                        double v = live ? m[a] * C.inv_fact2[a] * pw : 0.0;
+                        Mt[a * CART_GROUP + p] = (float)((n & 1) ? -v : v);
+                    }
                 }
             }
             // ratio^(1 + nb) for this lane's chunks (their degrees only grow)

@@ -52,14 +52,33 @@
 
 namespace {
 
-constexpr int G_THREADS = 128;
-constexpr int G_STAGES = 4;
-constexpr int G_B_BYTES = 8192;   // one key: 64 rows (B_hi, B_lo) x 32 columns of TF32
-constexpr int G_LBO = 128;        // bytes between core matrices along K
-constexpr int G_SBO = 1024;       // bytes between groups of 8 rows (K = 32)
-constexpr int G_TMEM_COLS = 256;  // D buffers [0, 64), [64, 128); A buffers [128, 192), [192, 256)
-constexpr int G_D_COL = 0;
-constexpr int G_A_COL = 128;
+constexpr int G_ROWS = 128;            // destinations per tile; producer threads
+constexpr int G_BLOCK = G_ROWS + 32;   // + the MMA-issuing warp
+constexpr int G_STAGES = 4;            // A stages (tensor memory) and B stages (shared memory)
+constexpr int G_LAG = 3;               // a run's rows are stored 3 runs after their fetch
+constexpr int G_RSTAGES = G_LAG + 1;   // row stages in shared memory
+constexpr int G_GROUP = 4;             // runs of one tile summed in one accumulator
+constexpr int G_DBUF = 4;              // accumulators of 64 tensor-memory columns
+constexpr int G_FIFO = 8;              // groups waiting for their readout (at most 6)
+constexpr int G_B_BYTES = 8192;        // one key: 64 rows (B_hi, B_lo) x 32 columns of TF32
+constexpr int G_RSTRIDE = 144;         // bytes per row in a row stage (odd multiple of 16)
+constexpr int G_RSTAGE_BYTES = G_ROWS * G_RSTRIDE;
+constexpr int G_LBO = 128;             // bytes between core matrices along K
+constexpr int G_SBO = 1024;            // bytes between groups of 8 rows (K = 32)
+constexpr int G_D_COL = 0;             // accumulators: tensor-memory columns [0, 256)
+constexpr int G_A_COL = G_DBUF * 64;   // A stages (hi 32 + lo 32 columns): [256, 512)
+constexpr int G_TMEM_COLS = 512;
+constexpr int G_OFF_B = 0;
+constexpr int G_OFF_ROWS = G_OFF_B + G_STAGES * G_B_BYTES;
+constexpr int G_OFF_ROWSRC = G_OFF_ROWS + G_RSTAGES * G_RSTAGE_BYTES;  // int[2][128]
+constexpr int G_OFF_INFO = G_OFF_ROWSRC + 2 * G_ROWS * 4;               // int[G_STAGES]
+constexpr int G_OFF_FIFO = (G_OFF_INFO + G_STAGES * 4 + 15) & ~15;      // int4[G_FIFO]
+constexpr int G_OFF_BARS = G_OFF_FIFO + G_FIFO * 16;  // full, bfull, empty, dfull, dempty, drain
+constexpr int G_SMEM_USED = G_OFF_BARS + (3 * G_STAGES + 2 * G_DBUF + 1) * 8 + 16;
+// at least 116 KB: one CTA per SM (it holds all 512 tensor-memory columns)
+constexpr int G_SMEM = G_SMEM_USED > 116 * 1024 ? G_SMEM_USED : 116 * 1024;
+static_assert(G_SMEM <= 227 * 1024, "shared memory of one CTA");
+constexpr int G_FIRST = 1, G_LAST = 2, G_END = 16;  // stage info: bits 2-3 the accumulator
 constexpr int G_MAX_LEVELS = 64;
 constexpr int G_MAX_SPAN = 40;
 constexpr uint32_t G_WAIT = 1u << 24;
@@ -75,29 +94,7 @@ struct GLevels {
 
 template <int P>
 struct GCoef {
-    float c[(P + 1) * (P + 1)];
-};
-
-// Bytes between the rows of a shared-memory stage: the row itself (a multiple of 16),
-// plus 16 when its count of 16-byte chunks is even, so that the 8 lanes of a quarter
-// warp reading chunk c of 8 consecutive rows hit 8 different bank groups.
-__host__ __device__ constexpr int stage_stride(int row_bytes) {
-    return ((row_bytes / 16) & 1) ? row_bytes : row_bytes + 16;
-}
-
-template <int P>
-struct GShape {
-    static constexpr int HW = (P + 2) & ~1;  // pairs per scaled-moment row
-    static constexpr int ROW = HW * 8;
-    static constexpr int STRIDE = stage_stride(ROW);
-    static constexpr int STAGE_A = G_THREADS * STRIDE;
-    // dynamic shared memory: B stages, A stages, [shared-memory A operands], flags
-    static constexpr int OFF_B = 0;
-    static constexpr int OFF_A = OFF_B + G_STAGES * G_B_BYTES;
-    static constexpr int OFF_OP = (OFF_A + G_STAGES * STAGE_A + 1023) & ~1023;
-    static constexpr int OP_BYTES = 2 * 2 * G_THREADS * 32 * 4;  // 2 buffers x (hi, lo)
-    static constexpr int flags_at(bool smem_a) { return smem_a ? OFF_OP + OP_BYTES : OFF_OP; }
-    static constexpr int bytes(bool smem_a) { return flags_at(smem_a) + G_STAGES * G_THREADS + 256; }
+    double c[(P + 1) * (P + 1)];
 };
 
 __device__ __forceinline__ int level_of(const GLevels& L, i64 node) {
@@ -149,11 +146,13 @@ __global__ void k_group_keys(const i64* __restrict__ pairs, i64 n_pairs,
     double uy = (center[2 * d + 1] - center[2 * s + 1]) / hmin;
     double rx = rint(ux), ry = rint(uy);
     int side = span_side(span);
-    unsigned key = n_keys(span);  // off the table
+    i64 qp = quad_pos(L, d);
+    // off the table: a key per destination row past the table's keys, so that each row's
+    // off-table translations form one run at the end of its tile
+    unsigned key = n_keys(span) + (unsigned)(qp & 127);
     if (dl >= -1 && dl <= 1 && fabs(ux - rx) <= 1e-9 && fabs(uy - ry) <= 1e-9 &&
         fabs(rx) <= span && fabs(ry) <= span)
         key = (unsigned)(((int)(dl + 1) * side + (int)rx + span) * side + (int)ry + span);
-    i64 qp = quad_pos(L, d);
     keys[e] = ((unsigned)(qp >> 7) << key_bits) | key;
     vals[e] = ((unsigned)s << 7) | (unsigned)(qp & 127);
 }
@@ -240,298 +239,378 @@ __global__ void k_m2l_operators(int order, const double* __restrict__ coeff, int
 }
 
 // ------------------------------------------------------------------ products
-// Byte offset of element (row, k) of a 128 x 32 shared-memory A operand.
-__device__ __forceinline__ int a_offset(int row, int k) {
-    return (row >> 3) * G_SBO + (k >> 2) * G_LBO + (row & 7) * 16 + (k & 3) * 4;
+// The first i in [0, n) with a[i] >= value (n if none), a sorted; every thread of the
+// block calls it (a 128-way search: one load and one block barrier per round).
+__device__ int block_lower_bound(const int* __restrict__ a, int n, i64 value) {
+    int lo = 0, hi = n;
+    while (hi > lo) {
+        int stride = (hi - lo + 127) / 128;
+        int i = lo + (int)threadIdx.x * stride;
+        bool below = threadIdx.x < 128 && i < hi && (i64)a[i] < value;
+        int nb = __syncthreads_count(below);
+        if (nb == 0) break;
+        int nhi = lo + nb * stride;
+        lo += (nb - 1) * stride + 1;
+        hi = nhi < hi ? nhi : hi;
+    }
+    return lo;
 }
 
-// The per-translation FP32 formula (as k_m2l_mixed) for one off-table translation into
-// destination d, added to v (bhat_l in v[2l], v[2l + 1]; a_0 in v[2w], v[2w + 1]).
+// A wait that also gives up when another role of the CTA has raised `abort_flag`.
+__device__ __forceinline__ bool wait_or_abort(uint64_t* bar, uint32_t parity,
+                                              const volatile int* abort_flag) {
+    for (uint32_t i = 0; i < G_WAIT; ++i) {
+        if (td3tc::mbar_test(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (i > 64) __nanosleep(32);
+    }
+    return false;
+}
+
+// Barrier 1 among the producer warps, returning whether any of them passed `pred`.
+__device__ __forceinline__ bool producers_sync_or(bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, %2, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "n"(G_ROWS)
+        : "memory");
+    return r != 0;
+}
+
+// The table's products, one persistent CTA per SM over an even share of the runs (cut
+// at tile boundaries), warp-specialised:
+//   warps 0-3, thread m = row m of every tile (tensor-memory lane m): per run, the
+//     translations note their rows in a row table; thread m fetches its row's source
+//     (the FP32 scaled moments) by cp.async into its own slot of a row stage and, G_LAG
+//     runs later, splits it into TF32 hi + lo and stores both into the run's A stage in
+//     tensor memory (zeros for a row the run leaves out), then arrives on the stage's
+//     `full` barrier; thread 0 fetches the key's B (8 KB) into shared memory with a bulk
+//     copy one run after the run's rows are noted;
+//   warp 4, one thread: per run, waits `full` and `bfull`, issues D = A_hi [B_hi; B_lo]^T
+//     (N = 64) and D[:, 0:32] += A_lo B_hi^T (N = 32), K = 32 as four steps of 8, A from
+//     tensor memory and B from shared memory, and commits them to the stage's `empty`
+//     barrier; D accumulates G_GROUP runs of one tile (a fresh D at the group's first run)
+//     in one of G_DBUF accumulators, committed to `dfull`;
+//   warps 0-3 again: two runs after a group's last run was handed over, its accumulator
+//     (FP32 columns 0:32 + 32:64) is added to the row's FP64 sums and released (`dempty`);
+//     after a tile's last group the sums go to the locals.
+// Sums run in the runs' order: deterministic.  Every wait is bounded; a wait that runs
+// out raises the CTA's abort flag and the status word, and the CTA drains its copies and
+// products before it releases its tensor memory.
 template <int P>
-__device__ __forceinline__ void offtable_translation(float (&v)[32], i64 d, i64 src, int order,
-                                                     const double* __restrict__ center,
-                                                     const double* __restrict__ half,
-                                                     const float2* __restrict__ hat,
-                                                     const GCoef<P>& C) {
-    constexpr int W = P + 1;
-    const int w = order + 1;
-    double tr = center[2 * d] - center[2 * src], ti = center[2 * d + 1] - center[2 * src + 1];
-    double t2 = tr * tr + ti * ti, inv = 1.0 / t2, hd = half[d], hs = half[src];
-    float wsr = (float)(hs * tr * inv), wsi = (float)(-hs * ti * inv);
-    float wdr = (float)(hd * tr * inv), wdi = (float)(-hd * ti * inv);
-    float lnt = 0.5f * log_split(t2 / (hd * hd));
-    const float2* row = hat + src * td3_hat_width(order);
-    float ar[W], ai[W];
-    float pr = 1.0f, pi = 0.0f;
-#pragma unroll
-    for (int k = 0; k < W; ++k) {
-        float2 m = k < w ? row[k] : make_float2(0.0f, 0.0f);
-        ar[k] = m.x * pr - m.y * pi;
-        ai[k] = m.x * pi + m.y * pr;
-        float nr = pr * wsr - pi * wsi;
-        pi = pr * wsi + pi * wsr;
-        pr = nr;
-    }
-    float qr = 1.0f, qi = 0.0f;
-#pragma unroll
-    for (int l = 0; l < W; ++l) {
-        float sr = 0.0f, si = 0.0f;
-#pragma unroll
-        for (int k = 0; k < W; ++k) {
-            sr += C.c[k * W + l] * ar[k];
-            si += C.c[k * W + l] * ai[k];
-        }
-        if (l < w) {
-            if (l == 0) {
-                v[0] += ar[0] * lnt - sr;
-                v[1] += ai[0] * lnt - si;
-            } else {
-                float sign = (l & 1) ? 1.0f : -1.0f;
-                v[2 * l] += sign * (sr * qr - si * qi);
-                v[2 * l + 1] += sign * (sr * qi + si * qr);
-            }
-        }
-        float nr = qr * wdr - qi * wdi;
-        qi = qr * wdi + qi * wdr;
-        qr = nr;
-    }
-    v[G_A0_ROW] += ar[0];
-    v[G_A0_ROW + 1] += ai[0];
-}
-
-// This thread's row of a run's D (64 columns at taddr): D[:, 0:32] + D[:, 32:64] (the
-// second half a correction about 2^-11 of the first, added in FP32) added to the FP64
-// sums, for the columns an order up to P uses (when the row took part in the run).
-template <int P, int V>
-__device__ __forceinline__ void read_out(uint32_t taddr, bool use, double (&acc)[V]) {
-    float d0[32], d1[32];
-    td3tc::tmem_load32(taddr, d0);
-    td3tc::tmem_load32(taddr + 32, d1);
-    if (use) {
-#pragma unroll
-        for (int k = 0; k < V; ++k)
-            if (k < 2 * (P + 1) || k >= G_A0_ROW) acc[k] += (double)(d0[k] + d1[k]);
-    }
-}
-
-template <int P, bool SMEM_A>
-__global__ void __launch_bounds__(G_THREADS, SMEM_A ? 1 : 2)
+__global__ void __launch_bounds__(G_BLOCK, 1)
 k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_start,
-              const unsigned* __restrict__ keys, const unsigned* __restrict__ vals, i64 n_nodes,
-              GLevels L, const double* __restrict__ center, const double* __restrict__ half,
+              const unsigned* __restrict__ keys, const unsigned* __restrict__ vals, int n_tiles,
+              i64 n_nodes, GLevels L, const double* __restrict__ half,
               const float2* __restrict__ hat, int order, const float* __restrict__ ops,
-              int key_bits, unsigned offtable_key, const GCoef<P> C,
-              double* __restrict__ local_re, double* __restrict__ local_im, i64* status) {
-    using S = GShape<P>;
-    constexpr int V = 32;  // outputs per row: bhat_l (re, im) in 0..2P+1, a_0 in 30, 31
+              int key_bits, unsigned offtable_key, double* __restrict__ local_re,
+              double* __restrict__ local_im, i64* status) {
     extern __shared__ __align__(1024) unsigned char smem[];
     const int tid = threadIdx.x, warp = tid >> 5;
-    const int tile = blockIdx.x;
-    const int j0 = tile_run[tile], j1 = tile_run[tile + 1];
-    if (j0 == j1) return;
-    const unsigned key_mask = (1u << key_bits) - 1u;
-    const int jm = (keys[run_start[j1 - 1]] & key_mask) == offtable_key ? j1 - 1 : j1;
-    const int n_mma = jm - j0;
-    const int w = order + 1, hw = td3_hat_width(order);
-    const int chunks = hw / 2;  // 16-byte chunks of a row
+    unsigned char* bstage = smem + G_OFF_B;
+    unsigned char* rows = smem + G_OFF_ROWS;
+    int* row_src = reinterpret_cast<int*>(smem + G_OFF_ROWSRC);
+    int* info = reinterpret_cast<int*>(smem + G_OFF_INFO);
+    int4* fifo = reinterpret_cast<int4*>(smem + G_OFF_FIFO);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + G_OFF_BARS);
+    uint64_t* bfull = full + G_STAGES;
+    uint64_t* empty = bfull + G_STAGES;
+    uint64_t* dfull = empty + G_STAGES;
+    uint64_t* dempty = dfull + G_DBUF;
+    uint64_t* drain = dempty + G_DBUF;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
-    unsigned char* stage_b = smem + S::OFF_B;
-    unsigned char* stage_a = smem + S::OFF_A;
-    unsigned char* op_a = smem + S::OFF_OP;  // shared-memory A operands (SMEM_A)
-    unsigned char* live = smem + S::flags_at(SMEM_A);
-    uint64_t* bar_stage = reinterpret_cast<uint64_t*>(live + G_STAGES * G_THREADS);
-    uint64_t* bar_mma = bar_stage + G_STAGES;
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar_mma + 2);
+    // this CTA's runs [r0, r1)
+    const int total = tile_run[n_tiles];
+    const i64 share = ((i64)total + gridDim.x - 1) / gridDim.x;
+    int t0 = block_lower_bound(tile_run, n_tiles + 1, (i64)blockIdx.x * share);
+    int t1 = block_lower_bound(tile_run, n_tiles + 1, (i64)(blockIdx.x + 1) * share);
+    t0 = t0 < n_tiles ? t0 : n_tiles;
+    t1 = t1 < n_tiles ? t1 : n_tiles;
+    const int r0 = tile_run[t0], r1 = tile_run[t1];
 
     if (tid == 0) {
-        // a stage completes when every thread's row copies have landed (one arrival per
-        // thread) and the key's B (bytes) is in
-        for (int s = 0; s < G_STAGES; ++s) td3tc::mbar_init(&bar_stage[s], G_THREADS);
-        td3tc::mbar_init(&bar_mma[0], 1);
-        td3tc::mbar_init(&bar_mma[1], 1);
+        for (int s = 0; s < G_STAGES; ++s) {
+            td3tc::mbar_init(&full[s], G_ROWS);  // the rows' threads, after their stores
+            td3tc::mbar_init(&bfull[s], 1);      // the B copy's bytes
+            td3tc::mbar_init(&empty[s], 1);      // the products that read the stage
+        }
+        for (int b = 0; b < G_DBUF; ++b) {
+            td3tc::mbar_init(&dfull[b], 1);
+            td3tc::mbar_init(&dempty[b], G_ROWS);
+        }
+        td3tc::mbar_init(drain, 1);
+        *abort_flag = 0;
     }
-    for (int i = tid; i < G_STAGES * G_THREADS; i += G_THREADS) live[i] = 0;
+    for (int i = tid; i < 2 * G_ROWS; i += G_BLOCK) row_src[i] = 0;
     if (warp == 0) td3tc::tmem_alloc(tmem_slot, G_TMEM_COLS);
     td3tc::fence_before_sync();
     __syncthreads();
     td3tc::fence_after_sync();
     const uint32_t tmem = *tmem_slot;
-    const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
 
-    // run j0 + i into stage i % G_STAGES: the rows by cp.async (each by the thread of its
-    // translation), B by one bulk copy; every thread arrives once
-    auto produce = [&](int i) {
-        int s = i % G_STAGES, j = j0 + i;
-        int a = run_start[j], cnt = run_start[j + 1] - a;
-        if (tid == 0) {
-            unsigned key = keys[a] & key_mask;
-            td3tc::mbar_expect_tx(&bar_stage[s], G_B_BYTES);
-            td3tc::bulk_g2s(stage_b + s * G_B_BYTES, ops + (size_t)key * (G_B_BYTES / 4), G_B_BYTES,
-                            &bar_stage[s]);
-        }
-        if (tid < cnt) {
-            unsigned v = vals[a + tid];
-            unsigned m = v & 127u;
-            live[s * G_THREADS + m] = 1;
-            const unsigned char* src =
-                reinterpret_cast<const unsigned char*>(hat + (size_t)(v >> 7) * hw);
-            unsigned char* dst = stage_a + s * S::STAGE_A + m * S::STRIDE;
-            for (int c = 0; c < chunks; ++c) td3tc::cp_async16(dst + 16 * c, src + 16 * c);
-        }
-        td3tc::cp_async_arrive(&bar_stage[s]);
-    };
+    if (tid < G_ROWS) {
+        // ------------------------------------------------ producers and readout
+        const int w = order + 1, hw = td3_hat_width(order), chunks = hw / 2;
+        const unsigned key_mask = (1u << key_bits) - 1u;
+        const uint32_t lane_base = (uint32_t)(32 * warp) << 16;
+        unsigned char* my_row = rows + tid * G_RSTRIDE;
+        // run data loaded ahead: the starts of runs j .. j + 3, the keys of j .. j + 2
+        // (past r1: all ones, an off-table key of no tile) and this thread's entries of
+        // runs j and j + 1
+        auto start_of = [&](int j) { return run_start[j < r1 ? j : r1]; };
+        auto key_of = [&](int j, int start) { return j < r1 ? keys[start] : 0xffffffffu; };
+        int j = r0;
+        int s0 = start_of(j), s1 = start_of(j + 1), s2 = start_of(j + 2), s3 = start_of(j + 3);
+        unsigned k0 = key_of(j, s0), k1 = key_of(j + 1, s1), k2 = key_of(j + 2, s2);
+        unsigned v0 = j < r1 && tid < s1 - s0 ? vals[s0 + tid] : 0u;
+        unsigned v1 = j + 1 < r1 && tid < s2 - s1 ? vals[s1 + tid] : 0u;
 
-    double acc[V];
+        double acc[32];
 #pragma unroll
-    for (int k = 0; k < V; ++k) acc[k] = 0.0;
-    bool failed = false, warp_failed = false, touched = false, prev_live = false;
-    int produced = 0, issued = 0;
-    const int pre = n_mma < G_STAGES - 1 ? n_mma : G_STAGES - 1;
-    for (; produced < pre; ++produced) produce(produced);
+        for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+        // runs noted (rows fetched), runs whose B was fetched, runs consumed (A stored)
+        int qn = 0, qb = 0, qc = 0;
+        int grp = 0, in_grp = 0, head = 0, tail = 0;
+        unsigned live_bits = 0;  // bit i: this row takes part in run qn - 1 - i
+        unsigned pend_info = 0;  // thread 0: byte i, the stage info of run qn - 1 - i
+        unsigned last_key = 0;   // thread 0: the key of run qn - 1
+        bool ok = true;
 
-    // D of run i in columns [64 (i & 1), +64); A of run i in [128 + 64 (i & 1), +64)
-
-    for (int i = 0; i < n_mma; ++i) {
-        const int s = i % G_STAGES;
-        bool ok = td3tc::mbar_wait(&bar_stage[s], (uint32_t)(i / G_STAGES) & 1u, G_WAIT);
-        // this thread's row: split into TF32 hi + lo
-        float hi[32], lo[32];
-        const bool is_live = ok && live[s * G_THREADS + tid] != 0;
-        touched |= is_live;
-        const float4* row = reinterpret_cast<const float4*>(stage_a + s * S::STAGE_A + tid * S::STRIDE);
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            float4 q = (is_live && c < chunks) ? row[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            float x[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-                hi[4 * c + u] = td3tc::to_tf32(x[u]);
-                lo[4 * c + u] = td3tc::to_tf32(x[u] - hi[4 * c + u]);
-            }
-        }
-        if (SMEM_A) {
-            unsigned char* ah = op_a + (i & 1) * (2 * G_THREADS * 128);
-            unsigned char* al = ah + G_THREADS * 128;
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                *reinterpret_cast<float4*>(ah + a_offset(tid, 4 * c)) =
-                    make_float4(hi[4 * c], hi[4 * c + 1], hi[4 * c + 2], hi[4 * c + 3]);
-                *reinterpret_cast<float4*>(al + a_offset(tid, 4 * c)) =
-                    make_float4(lo[4 * c], lo[4 * c + 1], lo[4 * c + 2], lo[4 * c + 3]);
-            }
-            td3tc::fence_smem_for_async();
-        } else {
-            const uint32_t acol = G_A_COL + 64 * (i & 1);
-            td3tc::tmem_store32(tmem + lane_base + acol, hi);
-            td3tc::tmem_store32(tmem + lane_base + acol + 32, lo);
-            td3tc::tmem_wait_st();
-        }
-        live[s * G_THREADS + tid] = 0;
-        td3tc::fence_before_sync();
-        if (__syncthreads_or(!ok || warp_failed)) {  // one decision for the whole block
-            failed = true;
-            break;
-        }
-        td3tc::fence_after_sync();
-        if (tid == 0) {
-            constexpr uint32_t id64 = td3tc::idesc_tf32(G_THREADS, 64);
-            constexpr uint32_t id32 = td3tc::idesc_tf32(G_THREADS, 32);
-            const uint32_t bb = td3tc::smem_addr(stage_b + s * G_B_BYTES);
-            const uint32_t d = tmem + G_D_COL + 64 * (i & 1);
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-                uint64_t db = td3tc::smem_desc(bb + 2 * G_LBO * ks, G_LBO, G_SBO);
-                uint32_t accum = ks > 0 ? 1u : 0u;  // a fresh D for every run
-                if (SMEM_A) {
-                    uint64_t da = td3tc::smem_desc(
-                        td3tc::smem_addr(op_a + (i & 1) * (2 * G_THREADS * 128)) + 2 * G_LBO * ks,
-                        G_LBO, G_SBO);
-                    td3tc::mma_tf32(d, da, db, id64, accum);
-                } else {
-                    td3tc::mma_tf32_ts(d, tmem + G_A_COL + 64 * (i & 1) + 8 * ks, db, id64, accum);
-                }
-            }
-#pragma unroll
-            for (int ks = 0; ks < 4; ++ks) {
-                uint64_t db = td3tc::smem_desc(bb + 2 * G_LBO * ks, G_LBO, G_SBO);
-                if (SMEM_A) {
-                    uint64_t da = td3tc::smem_desc(
-                        td3tc::smem_addr(op_a + (i & 1) * (2 * G_THREADS * 128) + G_THREADS * 128) +
-                            2 * G_LBO * ks,
-                        G_LBO, G_SBO);
-                    td3tc::mma_tf32(d, da, db, id32, 1u);
-                } else {
-                    td3tc::mma_tf32_ts(d, tmem + G_A_COL + 64 * (i & 1) + 32 + 8 * ks, db, id32,
-                                       1u);
-                }
-            }
-            td3tc::mma_commit(&bar_mma[i & 1]);
-        }
-        issued = i + 1;
-        // the previous run: its products are done, its D is summed in FP64 and its stage
-        // (whose B they read) takes the next run
-        if (i >= 1) {
-            bool done = td3tc::mbar_wait(&bar_mma[(i - 1) & 1], (uint32_t)((i - 1) >> 1) & 1u, G_WAIT);
+        // the accumulator of group rec.y into the FP64 sums; after a tile's last group,
+        // the sums into the locals
+        auto readout = [&](int4 rec) {
+            const int g = rec.y, buf = g % G_DBUF;
+            bool done = td3tc::mbar_wait(&dfull[buf], (uint32_t)(g / G_DBUF) & 1u, G_WAIT);
             done = __all_sync(0xffffffffu, done);
             if (done) {
                 td3tc::fence_after_sync();
-                read_out<P, V>(tmem + lane_base + G_D_COL + 64 * ((i - 1) & 1), prev_live, acc);
-            } else {
-                warp_failed = true;
+                float d0[32], d1[32];
+                td3tc::tmem_load32(tmem + lane_base + G_D_COL + buf * 64, d0);
+                td3tc::tmem_load32(tmem + lane_base + G_D_COL + buf * 64 + 32, d1);
+#pragma unroll
+                for (int k = 0; k < 32; ++k)
+                    if (k < 2 * (P + 1) || k >= G_A0_ROW) acc[k] += (double)(d0[k] + d1[k]);
+                td3tc::fence_before_sync();
             }
-        }
-        prev_live = is_live;
-        if (produced < n_mma && !warp_failed) {
-            produce(produced);
-            ++produced;
-        }
-    }
-    if (!failed && issued > 0) {
-        bool done = td3tc::mbar_wait(&bar_mma[(issued - 1) & 1], (uint32_t)((issued - 1) >> 1) & 1u,
-                                     G_WAIT);
-        if (__syncthreads_and(done)) {
-            td3tc::fence_after_sync();
-            read_out<P, V>(tmem + lane_base + G_D_COL + 64 * ((issued - 1) & 1), prev_live, acc);
-        } else {
-            failed = true;
-        }
-    }
-    if (failed) {
-        if (tid == 0) td3_report(status, 1);
-        // drain: the copies of every produced stage not yet consumed and the products
-        for (int i = issued; i < produced; ++i)
-            td3tc::mbar_wait(&bar_stage[i % G_STAGES], (uint32_t)(i / G_STAGES) & 1u, G_WAIT);
-        for (int i = issued - 2 < 0 ? 0 : issued - 2; i < issued; ++i)
-            td3tc::mbar_wait(&bar_mma[i & 1], (uint32_t)(i >> 1) & 1u, G_WAIT);
-    } else {
-        const i64 qp = (i64)tile * G_THREADS + tid;
-        const i64 d = qp < n_nodes ? node_at(L, qp) : -1;
-        // translations off the operator table: this row's, in the sorted order
-        if (jm < j1 && d >= 0) {
-            float fv[32];
+            td3tc::mbar_arrive(&dempty[buf]);
+            ok = ok && done;
+            if (rec.w) {
+                const i64 qp = (i64)rec.z * G_ROWS + tid;
+                bool any = false;
 #pragma unroll
-            for (int k = 0; k < 32; ++k) fv[k] = 0.0f;
-            for (int e = run_start[jm], e1 = run_start[jm + 1]; e < e1; ++e) {
-                unsigned val = vals[e];
-                if ((int)(val & 127u) != tid) continue;
-                offtable_translation<P>(fv, d, (i64)(val >> 7), order, center, half, hat, C);
-                touched = true;
-            }
+                for (int k = 0; k < 32; ++k) any |= acc[k] != 0.0;
+                if (any && qp < n_nodes) {
+                    const i64 d = node_at(L, qp);
+                    double hd = half[d], inv_h = 1.0 / hd, ln_h = log(hd), scale = 1.0;
 #pragma unroll
-            for (int k = 0; k < V; ++k) acc[k] += (double)fv[k];
-        }
-        if (touched && d >= 0) {
-            double hd = half[d], inv_h = 1.0 / hd, ln_h = log(hd), scale = 1.0;
-            const double a0r = acc[G_A0_ROW], a0i = acc[G_A0_ROW + 1];
-#pragma unroll
-            for (int l = 0; l <= P; ++l) {
-                if (l < w) {
-                    double ur = l ? 0.0 : ln_h * a0r, ui = l ? 0.0 : ln_h * a0i;
-                    local_re[d * w + l] += acc[2 * l] * scale + ur;
-                    local_im[d * w + l] += acc[2 * l + 1] * scale + ui;
+                    for (int l = 0; l <= P; ++l) {
+                        if (l < w) {
+                            double ur = l ? 0.0 : ln_h * acc[G_A0_ROW];
+                            double ui = l ? 0.0 : ln_h * acc[G_A0_ROW + 1];
+                            local_re[d * w + l] += acc[2 * l] * scale + ur;
+                            local_im[d * w + l] += acc[2 * l + 1] * scale + ui;
+                        }
+                        scale *= inv_h;
+                    }
                 }
-                scale *= inv_h;
+#pragma unroll
+                for (int k = 0; k < 32; ++k) acc[k] = 0.0;
             }
+        };
+        // thread 0: the operator of run qb into its stage (once the products of the
+        // stage's last use are done)
+        auto fetch_b = [&](unsigned key) {
+            const int s = qb % G_STAGES;
+            if (qb >= G_STAGES)
+                ok = td3tc::mbar_wait(&empty[s], (uint32_t)(qb / G_STAGES - 1) & 1u, G_WAIT) && ok;
+            if (ok) {
+                td3tc::mbar_arrive_expect_tx(&bfull[s], G_B_BYTES);
+                td3tc::bulk_g2s(bstage + s * G_B_BYTES, ops + (size_t)key * (G_B_BYTES / 4),
+                                G_B_BYTES, &bfull[s]);
+            }
+            ++qb;
+        };
+        // run qc's A stage: this thread's row (landed G_LAG cp.async groups ago) split into
+        // TF32 hi + lo, stored into tensor memory once the stage's last products are done
+        auto consume = [&](bool drain_all) {
+            const int s = qc % G_STAGES, back = qn - 1 - qc;
+            const bool live = (live_bits >> back) & 1u;
+            const unsigned inf = (pend_info >> (8 * back)) & 0xffu;
+            if (drain_all) td3tc::cp_async_wait<0>();
+            else td3tc::cp_async_wait<G_LAG>();
+            float hi[32], lo[32];
+            const float4* row = reinterpret_cast<const float4*>(my_row + (qc % G_RSTAGES) * G_RSTAGE_BYTES);
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                float4 x4 = (live && c < chunks) ? row[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                float x[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    hi[4 * c + u] = td3tc::to_tf32(x[u]);
+                    lo[4 * c + u] = td3tc::to_tf32(x[u] - hi[4 * c + u]);
+                }
+            }
+            if (qc >= G_STAGES)
+                ok = td3tc::mbar_wait(&empty[s], (uint32_t)(qc / G_STAGES - 1) & 1u, G_WAIT) && ok;
+            td3tc::fence_after_sync();
+            const uint32_t a = tmem + lane_base + G_A_COL + 64 * s;
+            td3tc::tmem_store32(a, hi);
+            td3tc::tmem_store32(a + 32, lo);
+            td3tc::tmem_wait_st();
+            td3tc::fence_before_sync();
+            if (tid == 0) info[s] = (int)inf;
+            td3tc::mbar_arrive(&full[s]);
+            ++qc;
+        };
+        // the readouts of groups whose last run was handed over two runs ago
+        auto due_readouts = [&]() {
+            while (head < tail) {
+                int4 rec = fifo[head % G_FIFO];
+                if (qc < rec.x + 3) break;
+                readout(rec);
+                ++head;
+            }
+        };
+
+        for (; j < r1; ++j) {
+            const unsigned key = k0 & key_mask;
+            if (key < offtable_key) {
+                const int tile = (int)(k0 >> key_bits);
+                // note the run's rows; its flags; the group's readout record
+                if (tid < s1 - s0) row_src[(qn & 1) * G_ROWS + (v0 & 127u)] = (int)(v0 >> 7) + 1;
+                const bool first = in_grp == 0;
+                const bool last_of_tile =
+                    (k1 >> key_bits) != (unsigned)tile || (k1 & key_mask) >= offtable_key;
+                const bool last = last_of_tile || in_grp + 1 == G_GROUP;
+                const unsigned inf =
+                    (first ? G_FIRST : 0u) | (last ? G_LAST : 0u) | ((unsigned)(grp % G_DBUF) << 2);
+                if (tid == 0 && last) fifo[tail % G_FIFO] = make_int4(qn, grp, tile, last_of_tile ? 1 : 0);
+                if (producers_sync_or(!ok)) {  // one decision for the four warps
+                    ok = false;
+                    break;
+                }
+                // this thread's row of the run: fetch its source
+                const int src1 = row_src[(qn & 1) * G_ROWS + tid];
+                row_src[(qn & 1) * G_ROWS + tid] = 0;
+                if (src1) {
+                    const float2* hrow = hat + (size_t)(src1 - 1) * hw;
+                    unsigned char* dst = my_row + (qn % G_RSTAGES) * G_RSTAGE_BYTES;
+                    for (int c = 0; c < chunks; ++c) td3tc::cp_async16(dst + 16 * c, hrow + 2 * c);
+                }
+                td3tc::cp_async_commit();
+                live_bits = (live_bits << 1) | (src1 ? 1u : 0u);
+                pend_info = (pend_info << 8) | inf;
+                if (last) {
+                    ++tail;
+                    ++grp;
+                    in_grp = 0;
+                } else {
+                    ++in_grp;
+                }
+                ++qn;
+                // the operator of the previous run
+                if (tid == 0 && qn >= 2) fetch_b(last_key);
+                if (tid == 0) last_key = key;
+                // the A stage of run qn - 1 - G_LAG
+                if (qn > G_LAG) consume(false);
+                due_readouts();
+            }
+            s0 = s1;
+            s1 = s2;
+            s2 = s3;
+            s3 = start_of(j + 4);
+            k0 = k1;
+            k1 = k2;
+            k2 = key_of(j + 3, s2);
+            v0 = v1;
+            v1 = j + 2 < r1 && tid < s2 - s1 ? vals[s1 + tid] : 0u;
+        }
+        if (!producers_sync_or(!ok)) {
+            // the drain: the last operator, the last runs' A stages, the end marker,
+            // the last groups
+            if (tid == 0 && qb < qn) fetch_b(last_key);
+            while (qc < qn) {
+                consume(true);
+                due_readouts();
+            }
+            const int s = qn % G_STAGES;
+            if (qn >= G_STAGES)
+                ok = td3tc::mbar_wait(&empty[s], (uint32_t)(qn / G_STAGES - 1) & 1u, G_WAIT) && ok;
+            if (tid == 0) info[s] = G_END;
+            td3tc::mbar_arrive(&full[s]);
+            while (head < tail) {
+                readout(fifo[head % G_FIFO]);
+                ++head;
+            }
+        } else {
+            ok = false;
+        }
+        td3tc::cp_async_wait<0>();
+        if (!ok) {
+            *abort_flag = 1;
+            td3_report(status, 1);
+            // the operator copies still in flight (the last use of each slot)
+            if (tid == 0)
+                for (int r = qb - G_STAGES < 0 ? 0 : qb - G_STAGES; r < qb; ++r)
+                    td3tc::mbar_wait(&bfull[r % G_STAGES], (uint32_t)(r / G_STAGES) & 1u, G_WAIT);
+        }
+    } else if (tid == G_ROWS) {
+        // ------------------------------------------------ the MMA issuer
+        constexpr uint32_t id64 = td3tc::idesc_tf32(G_ROWS, 64);
+        constexpr uint32_t id32 = td3tc::idesc_tf32(G_ROWS, 32);
+        int q = 0, g = 0;
+        bool ok = true;
+        for (;;) {
+            const int s = q % G_STAGES;
+            if (!wait_or_abort(&full[s], (uint32_t)(q / G_STAGES) & 1u, abort_flag)) {
+                ok = false;
+                break;
+            }
+            const int inf = *reinterpret_cast<volatile int*>(&info[s]);
+            if (inf & G_END) break;
+            if (!wait_or_abort(&bfull[s], (uint32_t)(q / G_STAGES) & 1u, abort_flag)) {
+                ok = false;
+                break;
+            }
+            const int buf = (inf >> 2) & (G_DBUF - 1);
+            if ((inf & G_FIRST) && g >= G_DBUF &&
+                !wait_or_abort(&dempty[buf], (uint32_t)(g / G_DBUF - 1) & 1u, abort_flag)) {
+                ok = false;
+                break;
+            }
+            td3tc::fence_after_sync();
+            const uint32_t bb = td3tc::smem_addr(bstage + s * G_B_BYTES);
+            const uint32_t d = tmem + G_D_COL + buf * 64;
+            const uint32_t a = tmem + G_A_COL + 64 * s;
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                uint64_t db = td3tc::smem_desc(bb + 2 * G_LBO * ks, G_LBO, G_SBO);
+                td3tc::mma_tf32_ts(d, a + 8 * ks, db, id64, ((inf & G_FIRST) && ks == 0) ? 0u : 1u);
+            }
+#pragma unroll
+            for (int ks = 0; ks < 4; ++ks) {
+                uint64_t db = td3tc::smem_desc(bb + 2 * G_LBO * ks, G_LBO, G_SBO);
+                td3tc::mma_tf32_ts(d, a + 32 + 8 * ks, db, id32, 1u);
+            }
+            td3tc::mma_commit(&empty[s]);
+            if (inf & G_LAST) {
+                td3tc::mma_commit(&dfull[buf]);
+                ++g;
+            }
+            ++q;
+        }
+        // every product issued has completed before the tensor memory is released
+        td3tc::mma_commit(drain);
+        td3tc::mbar_wait(drain, 0, G_WAIT);
+        if (!ok) {
+            *abort_flag = 1;
+            td3_report(status, 1);
         }
     }
     td3tc::fence_before_sync();
@@ -540,13 +619,143 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
     if (warp == 0) td3tc::tmem_free(tmem, G_TMEM_COLS);
 }
 
+// The per-translation formula (as k_m2l_mixed) in FP64 for one off-table translation
+// into destination d, from the FP32 scaled moments: with ws = h_src / t and wd = h_dst / t,
+// a'_k = hat_k ws^k, s_l = sum_k coeff[k, l] a'_k, bhat_0 = a'_0 ln|t / h_dst| - s_0 and
+// bhat_l = -(-1)^l s_l wd^l, written to out[2l], out[2l + 1] (l <= P), then a_0 to
+// out[2 (P + 1)], out[2 (P + 1) + 1].  FP64 because these translations (large depth
+// differences) are few and their sums carry the largest coefficients.
+template <int P>
+__device__ __forceinline__ void offtable_translation(double* out, i64 d, i64 src, int order,
+                                                     const double* __restrict__ center,
+                                                     const double* __restrict__ half,
+                                                     const float2* __restrict__ hat,
+                                                     const GCoef<P>& C) {
+    constexpr int W = P + 1;
+    const int w = order + 1;
+    double tr = center[2 * d] - center[2 * src], ti = center[2 * d + 1] - center[2 * src + 1];
+    double t2 = tr * tr + ti * ti, inv = 1.0 / t2, hd = half[d], hs = half[src];
+    double wsr = hs * tr * inv, wsi = -hs * ti * inv;
+    double wdr = hd * tr * inv, wdi = -hd * ti * inv;
+    double lnt = 0.5 * log(t2 / (hd * hd));
+    const float2* row = hat + src * td3_hat_width(order);
+    double ar[W], ai[W];
+    double pr = 1.0, pi = 0.0;
+#pragma unroll
+    for (int k = 0; k < W; ++k) {
+        float2 m = k < w ? row[k] : make_float2(0.0f, 0.0f);
+        ar[k] = (double)m.x * pr - (double)m.y * pi;
+        ai[k] = (double)m.x * pi + (double)m.y * pr;
+        double nr = pr * wsr - pi * wsi;
+        pi = pr * wsi + pi * wsr;
+        pr = nr;
+    }
+    double qr = 1.0, qi = 0.0;
+#pragma unroll
+    for (int l = 0; l < W; ++l) {
+        double sr = 0.0, si = 0.0;
+#pragma unroll
+        for (int k = 0; k < W; ++k) {
+            sr += C.c[k * W + l] * ar[k];
+            si += C.c[k * W + l] * ai[k];
+        }
+        if (l == 0) {
+            out[0] = ar[0] * lnt - sr;
+            out[1] = ai[0] * lnt - si;
+        } else {
+            double sign = (l & 1) ? 1.0 : -1.0;
+            out[2 * l] = l < w ? sign * (sr * qr - si * qi) : 0.0;
+            out[2 * l + 1] = l < w ? sign * (sr * qi + si * qr) : 0.0;
+        }
+        double nr = qr * wdr - qi * wdi;
+        qi = qr * wdi + qi * wdr;
+        qr = nr;
+    }
+    out[2 * W] = ar[0];
+    out[2 * W + 1] = ai[0];
+}
+
+// The translations off the operator table, a CTA per tile (tiles without any return at
+// once): one run per destination row after the tile's table runs.  Thread t evaluates
+// entry t of each chunk of 128 into shared scratch, then each row's thread adds its own
+// entries, in order, in FP64, and adds the sums to the locals (after the table's
+// products: deterministic).
+template <int P>
+__global__ void __launch_bounds__(G_ROWS)
+k_m2l_offtable(const int* __restrict__ tile_run, const int* __restrict__ run_start,
+               const unsigned* __restrict__ keys, const unsigned* __restrict__ vals,
+               i64 n_nodes, GLevels L, const double* __restrict__ center,
+               const double* __restrict__ half, const float2* __restrict__ hat, int order,
+               int key_bits, unsigned offtable_key, const GCoef<P> C,
+               double* __restrict__ local_re, double* __restrict__ local_im) {
+    constexpr int NV = 2 * (P + 1) + 2;  // bhat_l (re, im), then a_0
+    constexpr int NS = NV + 1;           // doubles per scratch slot (odd: no bank conflicts)
+    extern __shared__ double off_scratch[];
+    const int tid = threadIdx.x, tile = blockIdx.x;
+    const int j0 = tile_run[tile], j1 = tile_run[tile + 1];
+    if (j0 == j1) return;
+    const unsigned key_mask = (1u << key_bits) - 1u;
+    const int n_off = __syncthreads_count(
+        tid < j1 - j0 && (keys[run_start[j1 - 1 - tid]] & key_mask) >= offtable_key);
+    if (n_off == 0) return;
+    const int jm = j1 - n_off;
+    int* own = reinterpret_cast<int*>(off_scratch + G_ROWS * NS);  // 2 x 128
+    own[tid] = 0;
+    own[G_ROWS + tid] = 0;
+    __syncthreads();
+    if (tid < n_off) {
+        int r = jm + tid, row = (int)((keys[run_start[r]] & key_mask) - offtable_key);
+        own[row] = run_start[r];
+        own[G_ROWS + row] = run_start[r + 1];
+    }
+    __syncthreads();
+    const int my0 = own[tid], my1 = own[G_ROWS + tid];
+    double acc[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+    const int e0 = run_start[jm], e1 = run_start[j1];
+    for (int base = e0; base < e1; base += G_ROWS) {
+        if (base + tid < e1) {
+            unsigned val = vals[base + tid];
+            i64 de = node_at(L, (i64)tile * G_ROWS + (val & 127u));
+            offtable_translation<P>(off_scratch + tid * NS, de, (i64)(val >> 7), order, center,
+                                    half, hat, C);
+        }
+        __syncthreads();
+        const int a = my0 > base ? my0 : base;
+        const int b = my1 < base + G_ROWS ? my1 : base + G_ROWS;
+        for (int x = a; x < b; ++x) {
+            const double* f = off_scratch + (x - base) * NS;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) acc[k] += f[k];
+        }
+        __syncthreads();
+    }
+    const i64 qp = (i64)tile * G_ROWS + tid;
+    if (my1 > my0 && qp < n_nodes) {
+        const int w = order + 1;
+        const i64 d = node_at(L, qp);
+        double hd = half[d], inv_h = 1.0 / hd, ln_h = log(hd), scale = 1.0;
+#pragma unroll
+        for (int l = 0; l <= P; ++l) {
+            if (l < w) {
+                double ur = l ? 0.0 : ln_h * acc[NV - 2];
+                double ui = l ? 0.0 : ln_h * acc[NV - 1];
+                local_re[d * w + l] += acc[2 * l] * scale + ur;
+                local_im[d * w + l] += acc[2 * l + 1] * scale + ui;
+            }
+            scale *= inv_h;
+        }
+    }
+}
+
 int bits_for(i64 v) {
     int b = 1;
     while (b < 32 && ((i64)1 << b) <= v) ++b;
     return b;
 }
 
-int key_bits_for(int span) { return bits_for((i64)n_keys(span)); }
+int key_bits_for(int span) { return bits_for((i64)n_keys(span) + G_ROWS - 1); }
 
 int fill_levels(const int64_t* levels, int64_t n_levels, int64_t n_nodes, GLevels& L) {
     if (n_levels < 1 || n_levels > G_MAX_LEVELS) return TD3_EINVAL;
@@ -557,45 +766,35 @@ int fill_levels(const int64_t* levels, int64_t n_levels, int64_t n_nodes, GLevel
     return TD3_OK;
 }
 
-template <int P, bool SMEM_A>
+template <int P>
 int launch_grouped(const int* tile_run, const int* run_start, const unsigned* keys,
                    const unsigned* vals, i64 n_nodes, const GLevels& L, const double* center,
-                   const double* half, const float2* hat, int order, const float* ops, int span,
-                   const double* coeff, double* lre, double* lim, i64* status, cudaStream_t s) {
+                   const double* half, const float2* hat, int order,
+                   const float* ops, int span, const double* coeff, double* lre, double* lim,
+                   i64* status, cudaStream_t s) {
+    const i64 n_tiles = (n_nodes + G_ROWS - 1) / G_ROWS;
+    const int kb = key_bits_for(span);
+    int dev = 0, n_sm = 0;
+    TD3_TRY(cudaGetDevice(&dev));
+    TD3_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
+    auto grouped = k_m2l_grouped<P>;
+    TD3_TRY(cudaFuncSetAttribute(grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM));
+    const i64 grid = n_tiles < n_sm ? n_tiles : n_sm;
+    grouped<<<(unsigned)grid, G_BLOCK, G_SMEM, s>>>(tile_run, run_start, keys, vals, (int)n_tiles,
+                                                    n_nodes, L, half, hat, order, ops, kb,
+                                                    n_keys(span), lre, lim, status);
+    TD3_CHECK_LAUNCH();
     GCoef<P> C;
     int w = order + 1;
     for (int k = 0; k <= P; ++k)
         for (int l = 0; l <= P; ++l)
-            C.c[k * (P + 1) + l] = (k < w && l < w) ? (float)coeff[k * w + l] : 0.0f;
-    // at most two CTAs per SM (each holds G_TMEM_COLS of the 512 tensor-memory columns):
-    // at least 80 KB of shared memory per CTA
-    constexpr int smem = GShape<P>::bytes(SMEM_A) > 80 * 1024 ? GShape<P>::bytes(SMEM_A) : 80 * 1024;
-    auto kernel = k_m2l_grouped<P, SMEM_A>;
-    TD3_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    i64 n_tiles = (n_nodes + G_THREADS - 1) / G_THREADS;
-    kernel<<<(unsigned)n_tiles, G_THREADS, smem, s>>>(
-        tile_run, run_start, keys, vals, n_nodes, L, center, half, hat, order, ops,
-        key_bits_for(span), n_keys(span), C, lre, lim, status);
+            C.c[k * (P + 1) + l] = (k < w && l < w) ? coeff[k * w + l] : 0.0;
+    constexpr int off_smem = G_ROWS * (2 * (P + 1) + 3) * 8 + 2 * G_ROWS * 4;
+    k_m2l_offtable<P><<<(unsigned)n_tiles, G_ROWS, off_smem, s>>>(
+        tile_run, run_start, keys, vals, n_nodes, L, center, half, hat, order, kb, n_keys(span), C,
+        lre, lim);
     TD3_CHECK_LAUNCH();
     return TD3_OK;
-}
-
-template <bool SMEM_A>
-int dispatch_grouped(const int* tile_run, const int* run_start, const unsigned* keys,
-                     const unsigned* vals, i64 n_nodes, const GLevels& L, const double* center,
-                     const double* half, const float2* hat, int order, const float* ops, int span,
-                     const double* coeff, double* lre, double* lim, i64* status, cudaStream_t s) {
-    if (order <= 4)
-        return launch_grouped<4, SMEM_A>(tile_run, run_start, keys, vals, n_nodes, L, center, half,
-                                         hat, order, ops, span, coeff, lre, lim, status, s);
-    if (order <= 8)
-        return launch_grouped<8, SMEM_A>(tile_run, run_start, keys, vals, n_nodes, L, center, half,
-                                         hat, order, ops, span, coeff, lre, lim, status, s);
-    if (order <= 12)
-        return launch_grouped<12, SMEM_A>(tile_run, run_start, keys, vals, n_nodes, L, center, half,
-                                          hat, order, ops, span, coeff, lre, lim, status, s);
-    return launch_grouped<14, SMEM_A>(tile_run, run_start, keys, vals, n_nodes, L, center, half,
-                                      hat, order, ops, span, coeff, lre, lim, status, s);
 }
 
 }  // namespace
@@ -635,7 +834,7 @@ extern "C" int td3_m2l_groups(const int64_t* pairs, int64_t n_pairs, const doubl
     TD3_TRY_RC(fill_levels(levels, n_levels, n_nodes, L));
     i64 e = 2 * n_pairs;
     if (e >= 0x7fffffffLL) return TD3_EINVAL;
-    i64 n_tiles = (n_nodes + G_THREADS - 1) / G_THREADS;
+    i64 n_tiles = (n_nodes + G_ROWS - 1) / G_ROWS;
     int kb = key_bits_for(span);
     int bits = bits_for(n_tiles - 1 > 0 ? n_tiles - 1 : 1) + kb;
     if (bits > 32) return TD3_EINVAL;
@@ -678,8 +877,8 @@ extern "C" int td3_fmm_m2l_grouped(const int32_t* tile_run, const int32_t* run_s
                                    const uint32_t* keys, const uint32_t* values, int64_t n_nodes,
                                    const int64_t* levels, int64_t n_levels,
                                    const double* node_center, const double* node_half,
-                                   const float* hat, int order, const float* ops, int span,
-                                   const double* coeff, int smem_operands, double* local_re,
+                                   const float* hat, int order, const float* ops,
+                                   int span, const double* coeff, double* local_re,
                                    double* local_im, int64_t* status, void* stream) {
     if (n_nodes < 1 || n_nodes >= ((i64)1 << 25) || order < 0 ||
         order > TD3_M2L_GROUPED_MAX_ORDER || span < 1 || span > G_MAX_SPAN || !status)
@@ -688,11 +887,19 @@ extern "C" int td3_fmm_m2l_grouped(const int32_t* tile_run, const int32_t* run_s
     TD3_TRY_RC(fill_levels(levels, n_levels, n_nodes, L));
     cudaStream_t s = td3_stream(stream);
     const float2* h = reinterpret_cast<const float2*>(hat);
-    if (smem_operands)
-        return dispatch_grouped<true>(tile_run, run_start, keys, values, n_nodes, L, node_center,
-                                      node_half, h, order, ops, span, coeff, local_re, local_im,
-                                      status, s);
-    return dispatch_grouped<false>(tile_run, run_start, keys, values, n_nodes, L, node_center,
-                                   node_half, h, order, ops, span, coeff, local_re, local_im,
-                                   status, s);
+    if (order <= 4)
+        return launch_grouped<4>(tile_run, run_start, keys, values, n_nodes, L, node_center,
+                                 node_half, h, order, ops, span, coeff, local_re, local_im,
+                                 status, s);
+    if (order <= 8)
+        return launch_grouped<8>(tile_run, run_start, keys, values, n_nodes, L, node_center,
+                                 node_half, h, order, ops, span, coeff, local_re, local_im,
+                                 status, s);
+    if (order <= 12)
+        return launch_grouped<12>(tile_run, run_start, keys, values, n_nodes, L, node_center,
+                                  node_half, h, order, ops, span, coeff, local_re, local_im,
+                                  status, s);
+    return launch_grouped<14>(tile_run, run_start, keys, values, n_nodes, L, node_center,
+                              node_half, h, order, ops, span, coeff, local_re, local_im,
+                              status, s);
 }

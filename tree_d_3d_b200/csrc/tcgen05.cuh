@@ -203,6 +203,36 @@ __device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
                  : "memory");
 }
 
+// 16 zero bytes into shared memory through the same path as cp_async16 (the source
+// size is zero: nothing is read from `src_global`, which must still be a valid address).
+__device__ __forceinline__ void cp_async16_zero(void* dst_smem, const void* src_global) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst_smem)),
+                 "l"(src_global), "r"(0)
+                 : "memory");
+}
+
+// Closes this thread's current group of cp.async copies.
+__device__ __forceinline__ void cp_async_commit() {
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Waits until at most N of this thread's cp.async groups are still in flight.
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// One arrival on `bar` (release: this thread's earlier writes are seen by a thread that
+// waits for the phase).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Barrier `id` (1..15) among the first `threads` threads of the block (whole warps).
+__device__ __forceinline__ void named_sync(int id, int threads) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(threads) : "memory");
+}
+
 // Asynchronous copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from
 // this GPU's global memory into this CTA's shared memory, its bytes counted on `bar`.
 // No multicast: the copy lands in the issuing CTA only.

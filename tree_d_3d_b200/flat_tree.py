@@ -195,8 +195,6 @@ MOMENTS_ONE_LAUNCH = False
 #: the mixed-precision M2L of ``fmm`` (mutual lists, log kernel, orders up to 14) as
 #: tensor-core products grouped by translation (td3_m2l_groups, td3_fmm_m2l_grouped)
 M2L_GROUPED = True
-#: keep the grouped products' A operand in shared memory instead of tensor memory
-M2L_GROUPED_SMEM = False
 
 
 def _group_span(theta: float) -> int:
@@ -721,9 +719,8 @@ class FlatQuadtree:
                   groups["vals"].data_ptr(), self.node_count, levels.ctypes.data,
                   len(levels) - 1, self.node_center.data_ptr(), self.node_half.data_ptr(),
                   hat.data_ptr(), self.order, self._m2l_operators(span).data_ptr(), span,
-                  coeff.ctypes.data, 1 if M2L_GROUPED_SMEM else 0, local_re.data_ptr(),
-                  local_im.data_ptr(), self._tensor_status().data_ptr(),
-                  _lib.stream(self.device))
+                  coeff.ctypes.data, local_re.data_ptr(), local_im.data_ptr(),
+                  self._tensor_status().data_ptr(), _lib.stream(self.device))
 
     def _m2l_matrix(self) -> torch.Tensor:
         key = ("m2l_coefficients", self.order, self.symmetric)
