@@ -39,6 +39,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_PARTICLES = 1_000_000
+#: nominal FP32 FMA rate of a B200 at its max SM clock, TFLOP/s (148 SM x 128 lanes x 2)
+FP32_PEAK = 148 * 128 * 2 * 1.965e9 / 1e12
 ORDER = 12
 THETA = 0.5
 LEAF = 8
@@ -300,8 +302,8 @@ def count_our_launches(fn, torch):
 
 def time_m2l_mixed(tree, torch, reps, form="grouped"):
     """One mixed M2L form alone (CUDA events on its stream), average ms per launch:
-    "grouped" the tensor-core products grouped by translation (the step's form), "lanes"
-    the FP32 CUDA-core form (a lane per translation), "tile" the per-translation
+    "lanes" the FP32 CUDA-core form (a lane per translation, the step's form), "grouped"
+    the tensor-core products grouped by translation, "tile" the per-translation
     tensor-core form."""
     from tree_d_3d_b200 import _lib
     from tree_d_3d_b200.flat_tree import _m2l_coefficients
@@ -314,7 +316,7 @@ def time_m2l_mixed(tree, torch, reps, form="grouped"):
     stream = _lib.stream(tree.device)
     status = tree._tensor_status()
     if form == "grouped":
-        groups = lists["groups"]
+        groups = lists.get("groups") or tree._m2l_groups(lists["m2l"], THETA)
 
         def launch():
             tree._m2l_grouped(groups, hat, lre, lim)
@@ -469,12 +471,12 @@ def run_ours(args):
     err_fp64, _ = field_error(pos, q, "fp64", torch)
     for prec in ("mixed", "fp64"):
         coulomb[prec]["rel_err_field"], _ = field_error(pos, q, prec, torch, kernel="coulomb")
-    # the step's M2L form (tensor-core products grouped by translation); the FP32 CUDA-core
-    # form and the per-translation tensor-core form are timed beside it
-    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, form="grouped")
-    m2l_lanes_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="lanes")
+    # the step's M2L form (FP32 on the CUDA cores, a lane per translation); the tensor-core
+    # forms (products grouped by translation; per translation) are timed beside it
+    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, form="lanes")
+    m2l_grouped_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="grouped")
     m2l_tile_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="tile")
-    groups = tree._lists(THETA)["groups"]
+    groups = tree._m2l_groups(tree._lists(THETA)["m2l"], THETA)
     n_runs = int(groups["tile_run"][-1].item())
     width = ORDER + 1
     flops = 2 * n_m2l * 8 * width * width  # directed translations x 8 (p + 1)^2
@@ -484,21 +486,29 @@ def run_ours(args):
     # per run: D[128 x 64] += A_hi [128 x 32] B^T and D[128 x 32] += A_lo B_hi^T
     issued = n_runs * 2 * 128 * 32 * (64 + 32)
     roofline = {
-        "kernel": "k_m2l_grouped<12> (3xTF32 tcgen05 M2L grouped by translation, forward)",
-        "bound": "tensor",
+        "kernel": "k_m2l_mixed<12> (FP32 M2L, a lane per translation, forward)",
+        "bound": "fp32",
         "achieved": achieved,
-        "peak": tf32,
+        "peak": FP32_PEAK,
         "unit": "TFLOP/s",
-        "frac": achieved / tf32,
-        "peak_source": f"dense TF32 = half the BF16 tensor rate, {peak_note}",
+        "frac": achieved / FP32_PEAK,
+        "peak_source": ("nominal FP32 FMA rate at the max SM clock (148 SM x 128 lanes x 2 x "
+                        "1965 MHz); MEASURED_PEAKS.json has no FP32 CUDA-core figure"),
         "algorithmic": "8 (p + 1)^2 flop per directed translation (the reference's count)",
-        "issued_tensor_tflops": issued / (m2l_ms * 1e-3) / 1e12,
-        "issued_frac": issued / (m2l_ms * 1e-3) / 1e12 / tf32,
-        "runs_per_launch": n_runs,
-        "traffic": None,
+        # dram read + write of one ncu capture of this kernel at 300k particles (86.4 MB
+        # for 3.745M translations), scaled by the translations of this launch
+        "traffic": 86.4e6 * (2 * n_m2l) / 3.745e6,
+        "traffic_unit": "bytes per launch (scaled from a 300k-particle ncu capture)",
         "ms_per_launch": m2l_ms,
         "flop_per_launch": flops,
-        "fp32_lanes_form_ms_per_launch": m2l_lanes_ms,
+        "grouped_tensor_form": {
+            "kernel": "k_m2l_grouped<12> (3xTF32 tcgen05 products grouped by translation)",
+            "ms_per_launch": m2l_grouped_ms,
+            "runs_per_launch": n_runs,
+            "issued_tensor_tflops": issued / (m2l_grouped_ms * 1e-3) / 1e12,
+            "issued_frac": issued / (m2l_grouped_ms * 1e-3) / 1e12 / tf32,
+            "peak_source": f"dense TF32 = half the BF16 tensor rate, {peak_note}",
+        },
         "tile_form_ms_per_launch": m2l_tile_ms,
     }
     clock = clocks.summary()

@@ -40,6 +40,14 @@ def _node_at(levels: np.ndarray, qp: np.ndarray) -> np.ndarray:
     return np.where(size % 4 == 0, node, qp)
 
 
+@pytest.fixture(autouse=True)
+def _grouped_form(monkeypatch):
+    """The mixed fmm takes the grouped products in this module."""
+    from tree_d_3d_b200 import flat_tree
+
+    monkeypatch.setattr(flat_tree, "M2L_GROUPED", True)
+
+
 def _trees(n, order, seed, symmetric=False):
     from tree_d_3d_b200 import FlatQuadtree, Quad, synthetic
 

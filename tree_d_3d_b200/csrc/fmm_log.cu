@@ -236,7 +236,8 @@ struct CoefTable {
 };
 
 // M2L in FP32 on the CUDA cores, one lane per translation (CSR entry), the entries of
-// a warp's run of rows taken 32 at a time across row boundaries (m2l_rows.cuh).
+// a warp's run of rows taken 32 at a time across row boundaries, each round's sums taken
+// by columns (m2l_rows.cuh, column_round).
 // With w = 1/t, ws = h_src w and wd = h_dst w (|ws|, |wd| < 1 for separated cells):
 //   a'_k = hat_k ws^k,  s_l = sum_k coeff[k, l] a'_k,
 //   bhat_0 = a_0 ln|t| - s_0,  bhat_l = -(-1)^l s_l wd^l  (b_l = bhat_l / h_dst^l),
@@ -254,14 +255,16 @@ k_m2l_mixed(const i64* __restrict__ row_start, const int* __restrict__ entry_row
     td3_chain_wait();
     td3_chain_release();
     constexpr int W = P + 1, V = 2 * W + 2;
-    __shared__ float carry[M2L_WARPS][V];
+    __shared__ __align__(16) float stage[M2L_WARPS][32 * V];
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int w = order + 1;
     double inv_unit2 = 1.0 / (unit * unit), ln_unit = log(unit);
     i64 e0, e1;
     td3m2l::warp_entries(row_start, n_dst, (i64)blockIdx.x * M2L_WARPS + wib,
                          (i64)gridDim.x * M2L_WARPS, e0, e1);
-    int carry_d = -1;
+    float col[(V + 31) / 32], comp[(V + 31) / 32];
+#pragma unroll
+    for (int c = 0; c < (V + 31) / 32; ++c) col[c] = comp[c] = 0.0f;
     for (i64 base = e0; base < e1; base += 32) {
         i64 e = base + lane;
         bool live = e < e1;
@@ -322,8 +325,8 @@ k_m2l_mixed(const i64* __restrict__ row_start, const int* __restrict__ entry_row
             v[2 * W] = ar[0];
             v[2 * W + 1] = ai[0];
         }
-        td3m2l::finish_round<W>(v, d, live, lane, base + 32, e1, entry_row, w, dst_half, ln_unit,
-                                local_re, local_im, carry[wib], carry_d);
+        td3m2l::column_round<W>(v, d, live, lane, base + 32, e1, entry_row, w, dst_half, ln_unit,
+                                local_re, local_im, stage[wib], col, comp);
     }
 }
 

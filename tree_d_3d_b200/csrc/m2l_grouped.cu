@@ -54,30 +54,35 @@ namespace {
 
 constexpr int G_ROWS = 128;            // destinations per tile; producer threads
 constexpr int G_BLOCK = G_ROWS + 32;   // + the MMA-issuing warp
-constexpr int G_STAGES = 4;            // A stages (tensor memory) and B stages (shared memory)
+constexpr int G_ASTAGES = 2;           // A stages in tensor memory (hi 32 + lo 32 columns each)
+constexpr int G_BSTAGES = 4;           // B stages in shared memory
+constexpr int G_BAHEAD = 2;            // a run's B is fetched when the products of run - 2 go
 constexpr int G_LAG = 3;               // a run's rows are stored 3 runs after their fetch
 constexpr int G_RSTAGES = G_LAG + 1;   // row stages in shared memory
 constexpr int G_GROUP = 4;             // runs of one tile summed in one accumulator
-constexpr int G_DBUF = 4;              // accumulators of 64 tensor-memory columns
+constexpr int G_DBUF = 2;              // accumulators of 64 tensor-memory columns
 constexpr int G_FIFO = 8;              // groups waiting for their readout (at most 6)
+constexpr int G_KRING = 8;             // keys of the runs noted, for the operator copies
+constexpr unsigned G_NO_RUN = 0xffffffffu;
 constexpr int G_B_BYTES = 8192;        // one key: 64 rows (B_hi, B_lo) x 32 columns of TF32
 constexpr int G_RSTRIDE = 144;         // bytes per row in a row stage (odd multiple of 16)
 constexpr int G_RSTAGE_BYTES = G_ROWS * G_RSTRIDE;
 constexpr int G_LBO = 128;             // bytes between core matrices along K
 constexpr int G_SBO = 1024;            // bytes between groups of 8 rows (K = 32)
-constexpr int G_D_COL = 0;             // accumulators: tensor-memory columns [0, 256)
-constexpr int G_A_COL = G_DBUF * 64;   // A stages (hi 32 + lo 32 columns): [256, 512)
-constexpr int G_TMEM_COLS = 512;
+constexpr int G_D_COL = 0;             // accumulators: tensor-memory columns [0, 128)
+constexpr int G_A_COL = G_DBUF * 64;   // A stages: [128, 256)
+constexpr int G_TMEM_COLS = 256;       // two CTAs per SM
 constexpr int G_OFF_B = 0;
-constexpr int G_OFF_ROWS = G_OFF_B + G_STAGES * G_B_BYTES;
+constexpr int G_OFF_ROWS = G_OFF_B + G_BSTAGES * G_B_BYTES;
 constexpr int G_OFF_ROWSRC = G_OFF_ROWS + G_RSTAGES * G_RSTAGE_BYTES;  // int[2][128]
-constexpr int G_OFF_INFO = G_OFF_ROWSRC + 2 * G_ROWS * 4;               // int[G_STAGES]
-constexpr int G_OFF_FIFO = (G_OFF_INFO + G_STAGES * 4 + 15) & ~15;      // int4[G_FIFO]
-constexpr int G_OFF_BARS = G_OFF_FIFO + G_FIFO * 16;  // full, bfull, empty, dfull, dempty, drain
-constexpr int G_SMEM_USED = G_OFF_BARS + (3 * G_STAGES + 2 * G_DBUF + 1) * 8 + 16;
-// at least 116 KB: one CTA per SM (it holds all 512 tensor-memory columns)
-constexpr int G_SMEM = G_SMEM_USED > 116 * 1024 ? G_SMEM_USED : 116 * 1024;
-static_assert(G_SMEM <= 227 * 1024, "shared memory of one CTA");
+constexpr int G_OFF_INFO = G_OFF_ROWSRC + 2 * G_ROWS * 4;               // int[G_ASTAGES]
+constexpr int G_OFF_KEYS = G_OFF_INFO + G_ASTAGES * 4;                  // unsigned[G_KRING]
+constexpr int G_OFF_FIFO = (G_OFF_KEYS + G_KRING * 4 + 15) & ~15;       // int4[G_FIFO]
+// barriers: full, aempty (G_ASTAGES); bfull, bempty (G_BSTAGES); dfull, dempty; drain
+constexpr int G_OFF_BARS = G_OFF_FIFO + G_FIFO * 16;
+constexpr int G_N_BARS = 2 * G_ASTAGES + 2 * G_BSTAGES + 2 * G_DBUF + 1;
+constexpr int G_SMEM = G_OFF_BARS + G_N_BARS * 8 + 16;
+static_assert(2 * (G_SMEM + 1024) <= 228 * 1024, "two CTAs per SM");
 constexpr int G_FIRST = 1, G_LAST = 2, G_END = 16;  // stage info: bits 2-3 the accumulator
 constexpr int G_MAX_LEVELS = 64;
 constexpr int G_MAX_SPAN = 40;
@@ -281,19 +286,20 @@ __device__ __forceinline__ bool producers_sync_or(bool pred) {
     return r != 0;
 }
 
-// The table's products, one persistent CTA per SM over an even share of the runs (cut
-// at tile boundaries), warp-specialised:
+// The table's products, a persistent grid of two CTAs per SM over even shares of the
+// runs (cut at tile boundaries), warp-specialised:
 //   warps 0-3, thread m = row m of every tile (tensor-memory lane m): per run, the
 //     translations note their rows in a row table; thread m fetches its row's source
 //     (the FP32 scaled moments) by cp.async into its own slot of a row stage and, G_LAG
-//     runs later, splits it into TF32 hi + lo and stores both into the run's A stage in
-//     tensor memory (zeros for a row the run leaves out), then arrives on the stage's
-//     `full` barrier; thread 0 fetches the key's B (8 KB) into shared memory with a bulk
-//     copy one run after the run's rows are noted;
+//     runs later, splits it into TF32 hi + lo (Veltkamp's split on the FP32 pipe: hi
+//     keeps 11 significant bits, lo = x - hi exactly) and stores both into the run's A
+//     stage in tensor memory (zeros for a row the run leaves out), then arrives on the
+//     stage's `full` barrier;
 //   warp 4, one thread: per run, waits `full` and `bfull`, issues D = A_hi [B_hi; B_lo]^T
 //     (N = 64) and D[:, 0:32] += A_lo B_hi^T (N = 32), K = 32 as four steps of 8, A from
-//     tensor memory and B from shared memory, and commits them to the stage's `empty`
-//     barrier; D accumulates G_GROUP runs of one tile (a fresh D at the group's first run)
+//     tensor memory and B from shared memory, and commits them to the A and B stages'
+//     `empty` barriers; it fetches each key's B (8 KB, one bulk copy) G_BAHEAD runs
+//     ahead; D accumulates G_GROUP runs of one tile (a fresh D at the group's first run)
 //     in one of G_DBUF accumulators, committed to `dfull`;
 //   warps 0-3 again: two runs after a group's last run was handed over, its accumulator
 //     (FP32 columns 0:32 + 32:64) is added to the row's FP64 sums and released (`dempty`);
@@ -302,7 +308,7 @@ __device__ __forceinline__ bool producers_sync_or(bool pred) {
 // out raises the CTA's abort flag and the status word, and the CTA drains its copies and
 // products before it releases its tensor memory.
 template <int P>
-__global__ void __launch_bounds__(G_BLOCK, 1)
+__global__ void __launch_bounds__(G_BLOCK, 2)
 k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_start,
               const unsigned* __restrict__ keys, const unsigned* __restrict__ vals, int n_tiles,
               i64 n_nodes, GLevels L, const double* __restrict__ half,
@@ -315,11 +321,13 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
     unsigned char* rows = smem + G_OFF_ROWS;
     int* row_src = reinterpret_cast<int*>(smem + G_OFF_ROWSRC);
     int* info = reinterpret_cast<int*>(smem + G_OFF_INFO);
+    unsigned* kring = reinterpret_cast<unsigned*>(smem + G_OFF_KEYS);
     int4* fifo = reinterpret_cast<int4*>(smem + G_OFF_FIFO);
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + G_OFF_BARS);
-    uint64_t* bfull = full + G_STAGES;
-    uint64_t* empty = bfull + G_STAGES;
-    uint64_t* dfull = empty + G_STAGES;
+    uint64_t* aempty = full + G_ASTAGES;
+    uint64_t* bfull = aempty + G_ASTAGES;
+    uint64_t* bempty = bfull + G_BSTAGES;
+    uint64_t* dfull = bempty + G_BSTAGES;
     uint64_t* dempty = dfull + G_DBUF;
     uint64_t* drain = dempty + G_DBUF;
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
@@ -335,10 +343,13 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
     const int r0 = tile_run[t0], r1 = tile_run[t1];
 
     if (tid == 0) {
-        for (int s = 0; s < G_STAGES; ++s) {
+        for (int s = 0; s < G_ASTAGES; ++s) {
             td3tc::mbar_init(&full[s], G_ROWS);  // the rows' threads, after their stores
-            td3tc::mbar_init(&bfull[s], 1);      // the B copy's bytes
-            td3tc::mbar_init(&empty[s], 1);      // the products that read the stage
+            td3tc::mbar_init(&aempty[s], 1);     // the products that read the A stage
+        }
+        for (int s = 0; s < G_BSTAGES; ++s) {
+            td3tc::mbar_init(&bfull[s], 1);   // the B copy's bytes
+            td3tc::mbar_init(&bempty[s], 1);  // the products that read the B stage
         }
         for (int b = 0; b < G_DBUF; ++b) {
             td3tc::mbar_init(&dfull[b], 1);
@@ -371,15 +382,16 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
         unsigned v0 = j < r1 && tid < s1 - s0 ? vals[s0 + tid] : 0u;
         unsigned v1 = j + 1 < r1 && tid < s2 - s1 ? vals[s1 + tid] : 0u;
 
-        double acc[32];
+        // FP64 sums of the columns an order up to P uses: bhat_l (re, im) in 2l, 2l + 1,
+        // then a_0 (D columns G_A0_ROW, G_A0_ROW + 1)
+        constexpr int NV = 2 * (P + 1) + 2;
+        double acc[NV];
 #pragma unroll
-        for (int k = 0; k < 32; ++k) acc[k] = 0.0;
-        // runs noted (rows fetched), runs whose B was fetched, runs consumed (A stored)
-        int qn = 0, qb = 0, qc = 0;
+        for (int k = 0; k < NV; ++k) acc[k] = 0.0;
+        int qn = 0, qc = 0;  // runs noted (rows fetched), runs consumed (A stored)
         int grp = 0, in_grp = 0, head = 0, tail = 0;
         unsigned live_bits = 0;  // bit i: this row takes part in run qn - 1 - i
-        unsigned pend_info = 0;  // thread 0: byte i, the stage info of run qn - 1 - i
-        unsigned last_key = 0;   // thread 0: the key of run qn - 1
+        unsigned pend_info = 0;  // byte i: the stage info of run qn - 1 - i
         bool ok = true;
 
         // the accumulator of group rec.y into the FP64 sums; after a tile's last group,
@@ -390,12 +402,15 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
             done = __all_sync(0xffffffffu, done);
             if (done) {
                 td3tc::fence_after_sync();
-                float d0[32], d1[32];
-                td3tc::tmem_load32(tmem + lane_base + G_D_COL + buf * 64, d0);
-                td3tc::tmem_load32(tmem + lane_base + G_D_COL + buf * 64 + 32, d1);
+                // the two column halves (hi and lo products) each added in FP64
 #pragma unroll
-                for (int k = 0; k < 32; ++k)
-                    if (k < 2 * (P + 1) || k >= G_A0_ROW) acc[k] += (double)(d0[k] + d1[k]);
+                for (int half_d = 0; half_d < 2; ++half_d) {
+                    float dv[32];
+                    td3tc::tmem_load32(tmem + lane_base + G_D_COL + buf * 64 + 32 * half_d, dv);
+#pragma unroll
+                    for (int k = 0; k < NV; ++k)
+                        acc[k] += (double)dv[k < NV - 2 ? k : G_A0_ROW + k - (NV - 2)];
+                }
                 td3tc::fence_before_sync();
             }
             td3tc::mbar_arrive(&dempty[buf]);
@@ -404,64 +419,75 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                 const i64 qp = (i64)rec.z * G_ROWS + tid;
                 bool any = false;
 #pragma unroll
-                for (int k = 0; k < 32; ++k) any |= acc[k] != 0.0;
+                for (int k = 0; k < NV; ++k) any |= acc[k] != 0.0;
                 if (any && qp < n_nodes) {
                     const i64 d = node_at(L, qp);
-                    double hd = half[d], inv_h = 1.0 / hd, ln_h = log(hd), scale = 1.0;
+                    double* lr = local_re + d * w;
+                    double* li = local_im + d * w;
+                    // the sums scaled in place: b_l = bhat_l / h^l (+ a_0 ln h for l = 0)
+                    double hd = half[d], inv_h = 1.0 / hd, scale = 1.0;
+                    acc[0] += log(hd) * acc[NV - 2];
+                    acc[1] += log(hd) * acc[NV - 1];
 #pragma unroll
                     for (int l = 0; l <= P; ++l) {
-                        if (l < w) {
-                            double ur = l ? 0.0 : ln_h * acc[G_A0_ROW];
-                            double ui = l ? 0.0 : ln_h * acc[G_A0_ROW + 1];
-                            local_re[d * w + l] += acc[2 * l] * scale + ur;
-                            local_im[d * w + l] += acc[2 * l + 1] * scale + ui;
-                        }
+                        acc[2 * l] *= scale;
+                        acc[2 * l + 1] *= scale;
                         scale *= inv_h;
+                    }
+                    // four coefficients at a time: their old values loaded together
+#pragma unroll
+                    for (int l0 = 0; l0 <= P; l0 += 4) {
+                        double o_r[4], o_i[4];
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            o_r[u] = l0 + u < w ? lr[l0 + u] : 0.0;
+                            o_i[u] = l0 + u < w ? li[l0 + u] : 0.0;
+                        }
+#pragma unroll
+                        for (int u = 0; u < 4; ++u) {
+                            if (l0 + u < w && l0 + u <= P) {
+                                lr[l0 + u] = o_r[u] + acc[2 * (l0 + u)];
+                                li[l0 + u] = o_i[u] + acc[2 * (l0 + u) + 1];
+                            }
+                        }
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < 32; ++k) acc[k] = 0.0;
+                for (int k = 0; k < NV; ++k) acc[k] = 0.0;
             }
         };
-        // thread 0: the operator of run qb into its stage (once the products of the
-        // stage's last use are done)
-        auto fetch_b = [&](unsigned key) {
-            const int s = qb % G_STAGES;
-            if (qb >= G_STAGES)
-                ok = td3tc::mbar_wait(&empty[s], (uint32_t)(qb / G_STAGES - 1) & 1u, G_WAIT) && ok;
-            if (ok) {
-                td3tc::mbar_arrive_expect_tx(&bfull[s], G_B_BYTES);
-                td3tc::bulk_g2s(bstage + s * G_B_BYTES, ops + (size_t)key * (G_B_BYTES / 4),
-                                G_B_BYTES, &bfull[s]);
-            }
-            ++qb;
-        };
-        // run qc's A stage: this thread's row (landed G_LAG cp.async groups ago) split into
-        // TF32 hi + lo, stored into tensor memory once the stage's last products are done
+        // run qc's A stage: this thread's row (G_LAG cp.async groups ago, or all of them
+        // in the drain) split into TF32 hi + lo, stored into tensor memory once the
+        // products that last read the stage are done
         auto consume = [&](bool drain_all) {
-            const int s = qc % G_STAGES, back = qn - 1 - qc;
+            const int s = qc % G_ASTAGES, back = qn - 1 - qc;
             const bool live = (live_bits >> back) & 1u;
             const unsigned inf = (pend_info >> (8 * back)) & 0xffu;
             if (drain_all) td3tc::cp_async_wait<0>();
             else td3tc::cp_async_wait<G_LAG>();
-            float hi[32], lo[32];
             const float4* row = reinterpret_cast<const float4*>(my_row + (qc % G_RSTAGES) * G_RSTAGE_BYTES);
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                float4 x4 = (live && c < chunks) ? row[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-                float x[4] = {x4.x, x4.y, x4.z, x4.w};
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    hi[4 * c + u] = td3tc::to_tf32(x[u]);
-                    lo[4 * c + u] = td3tc::to_tf32(x[u] - hi[4 * c + u]);
-                }
-            }
-            if (qc >= G_STAGES)
-                ok = td3tc::mbar_wait(&empty[s], (uint32_t)(qc / G_STAGES - 1) & 1u, G_WAIT) && ok;
+            if (qc >= G_ASTAGES)
+                ok = td3tc::mbar_wait(&aempty[s], (uint32_t)(qc / G_ASTAGES - 1) & 1u, G_WAIT) && ok;
             td3tc::fence_after_sync();
             const uint32_t a = tmem + lane_base + G_A_COL + 64 * s;
-            td3tc::tmem_store32(a, hi);
-            td3tc::tmem_store32(a + 32, lo);
+            // hi, then lo (the row read twice from shared memory: fewer live registers)
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                float v[32];
+#pragma unroll
+                for (int c = 0; c < 8; ++c) {
+                    float4 x4 = (live && c < chunks) ? row[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    float x[4] = {x4.x, x4.y, x4.z, x4.w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        // Veltkamp: t = (2^13 + 1) x, hi = t - (t - x) has 11 significant bits
+                        float t = __fmul_rn(x[u], 8193.0f);
+                        float h = __fsub_rn(t, __fsub_rn(t, x[u]));
+                        v[4 * c + u] = part ? __fsub_rn(x[u], h) : h;
+                    }
+                }
+                td3tc::tmem_store32(a + 32 * part, v);
+            }
             td3tc::tmem_wait_st();
             td3tc::fence_before_sync();
             if (tid == 0) info[s] = (int)inf;
@@ -482,7 +508,7 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
             const unsigned key = k0 & key_mask;
             if (key < offtable_key) {
                 const int tile = (int)(k0 >> key_bits);
-                // note the run's rows; its flags; the group's readout record
+                // note the run's rows, its flags and key, the group's readout record
                 if (tid < s1 - s0) row_src[(qn & 1) * G_ROWS + (v0 & 127u)] = (int)(v0 >> 7) + 1;
                 const bool first = in_grp == 0;
                 const bool last_of_tile =
@@ -490,7 +516,10 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                 const bool last = last_of_tile || in_grp + 1 == G_GROUP;
                 const unsigned inf =
                     (first ? G_FIRST : 0u) | (last ? G_LAST : 0u) | ((unsigned)(grp % G_DBUF) << 2);
-                if (tid == 0 && last) fifo[tail % G_FIFO] = make_int4(qn, grp, tile, last_of_tile ? 1 : 0);
+                if (tid == 0) {
+                    kring[qn % G_KRING] = key;
+                    if (last) fifo[tail % G_FIFO] = make_int4(qn, grp, tile, last_of_tile ? 1 : 0);
+                }
                 if (producers_sync_or(!ok)) {  // one decision for the four warps
                     ok = false;
                     break;
@@ -514,9 +543,6 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                     ++in_grp;
                 }
                 ++qn;
-                // the operator of the previous run
-                if (tid == 0 && qn >= 2) fetch_b(last_key);
-                if (tid == 0) last_key = key;
                 // the A stage of run qn - 1 - G_LAG
                 if (qn > G_LAG) consume(false);
                 due_readouts();
@@ -532,16 +558,17 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
             v1 = j + 2 < r1 && tid < s2 - s1 ? vals[s1 + tid] : 0u;
         }
         if (!producers_sync_or(!ok)) {
-            // the drain: the last operator, the last runs' A stages, the end marker,
-            // the last groups
-            if (tid == 0 && qb < qn) fetch_b(last_key);
+            // the drain: no operator past the last run, the last runs' A stages, the end
+            // marker, the last groups
+            if (tid == 0)
+                for (int r = qn; r < qn + G_BAHEAD; ++r) kring[r % G_KRING] = G_NO_RUN;
             while (qc < qn) {
                 consume(true);
                 due_readouts();
             }
-            const int s = qn % G_STAGES;
-            if (qn >= G_STAGES)
-                ok = td3tc::mbar_wait(&empty[s], (uint32_t)(qn / G_STAGES - 1) & 1u, G_WAIT) && ok;
+            const int s = qn % G_ASTAGES;
+            if (qn >= G_ASTAGES)
+                ok = td3tc::mbar_wait(&aempty[s], (uint32_t)(qn / G_ASTAGES - 1) & 1u, G_WAIT) && ok;
             if (tid == 0) info[s] = G_END;
             td3tc::mbar_arrive(&full[s]);
             while (head < tail) {
@@ -555,26 +582,37 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
         if (!ok) {
             *abort_flag = 1;
             td3_report(status, 1);
-            // the operator copies still in flight (the last use of each slot)
-            if (tid == 0)
-                for (int r = qb - G_STAGES < 0 ? 0 : qb - G_STAGES; r < qb; ++r)
-                    td3tc::mbar_wait(&bfull[r % G_STAGES], (uint32_t)(r / G_STAGES) & 1u, G_WAIT);
         }
     } else if (tid == G_ROWS) {
         // ------------------------------------------------ the MMA issuer
         constexpr uint32_t id64 = td3tc::idesc_tf32(G_ROWS, 64);
         constexpr uint32_t id32 = td3tc::idesc_tf32(G_ROWS, 32);
-        int q = 0, g = 0;
+        int q = 0, g = 0, fetched = 0;
         bool ok = true;
         for (;;) {
-            const int s = q % G_STAGES;
-            if (!wait_or_abort(&full[s], (uint32_t)(q / G_STAGES) & 1u, abort_flag)) {
+            const int s = q % G_ASTAGES, bs = q % G_BSTAGES;
+            if (!wait_or_abort(&full[s], (uint32_t)(q / G_ASTAGES) & 1u, abort_flag)) {
                 ok = false;
                 break;
             }
             const int inf = *reinterpret_cast<volatile int*>(&info[s]);
             if (inf & G_END) break;
-            if (!wait_or_abort(&bfull[s], (uint32_t)(q / G_STAGES) & 1u, abort_flag)) {
+            // the operators of runs up to q + G_BAHEAD (their keys are noted by now)
+            while (ok && fetched <= q + G_BAHEAD) {
+                const unsigned key = *reinterpret_cast<volatile unsigned*>(&kring[fetched % G_KRING]);
+                if (key == G_NO_RUN) break;
+                const int fs = fetched % G_BSTAGES;
+                if (fetched >= G_BSTAGES &&
+                    !wait_or_abort(&bempty[fs], (uint32_t)(fetched / G_BSTAGES - 1) & 1u, abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                td3tc::mbar_arrive_expect_tx(&bfull[fs], G_B_BYTES);
+                td3tc::bulk_g2s(bstage + fs * G_B_BYTES, ops + (size_t)key * (G_B_BYTES / 4),
+                                G_B_BYTES, &bfull[fs]);
+                ++fetched;
+            }
+            if (!ok || !wait_or_abort(&bfull[bs], (uint32_t)(q / G_BSTAGES) & 1u, abort_flag)) {
                 ok = false;
                 break;
             }
@@ -585,7 +623,7 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                 break;
             }
             td3tc::fence_after_sync();
-            const uint32_t bb = td3tc::smem_addr(bstage + s * G_B_BYTES);
+            const uint32_t bb = td3tc::smem_addr(bstage + bs * G_B_BYTES);
             const uint32_t d = tmem + G_D_COL + buf * 64;
             const uint32_t a = tmem + G_A_COL + 64 * s;
 #pragma unroll
@@ -598,7 +636,8 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
                 uint64_t db = td3tc::smem_desc(bb + 2 * G_LBO * ks, G_LBO, G_SBO);
                 td3tc::mma_tf32_ts(d, a + 32 + 8 * ks, db, id32, 1u);
             }
-            td3tc::mma_commit(&empty[s]);
+            td3tc::mma_commit(&aempty[s]);
+            td3tc::mma_commit(&bempty[bs]);
             if (inf & G_LAST) {
                 td3tc::mma_commit(&dfull[buf]);
                 ++g;
@@ -611,6 +650,9 @@ k_m2l_grouped(const int* __restrict__ tile_run, const int* __restrict__ run_star
         if (!ok) {
             *abort_flag = 1;
             td3_report(status, 1);
+            // the operator copies still in flight (the last use of each stage)
+            for (int f = fetched - G_BSTAGES < 0 ? 0 : fetched - G_BSTAGES; f < fetched; ++f)
+                td3tc::mbar_wait(&bfull[f % G_BSTAGES], (uint32_t)(f / G_BSTAGES) & 1u, G_WAIT);
         }
     }
     td3tc::fence_before_sync();
@@ -779,7 +821,7 @@ int launch_grouped(const int* tile_run, const int* run_start, const unsigned* ke
     TD3_TRY(cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev));
     auto grouped = k_m2l_grouped<P>;
     TD3_TRY(cudaFuncSetAttribute(grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, G_SMEM));
-    const i64 grid = n_tiles < n_sm ? n_tiles : n_sm;
+    const i64 grid = n_tiles < 2 * n_sm ? n_tiles : 2 * n_sm;  // two CTAs per SM
     grouped<<<(unsigned)grid, G_BLOCK, G_SMEM, s>>>(tile_run, run_start, keys, vals, (int)n_tiles,
                                                     n_nodes, L, half, hat, order, ops, kb,
                                                     n_keys(span), lre, lim, status);

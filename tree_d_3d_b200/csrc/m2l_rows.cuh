@@ -101,4 +101,71 @@ __device__ __forceinline__ void finish_round(float (&v)[2 * W + 2], int d, bool 
     __syncwarp();
 }
 
+// The column form of a round's sums: the round's contributions (v, lane order = entry
+// order) are staged in shared memory (`stage`, 32 x (2W + 2) floats of this warp), then
+// lane k sums column k (and k + 32, ...) over the round's entries in order, carrying the
+// destination that continues into the next round in `col` (compensated sums: `comp` holds
+// each one's running error), and at each destination's last entry the sums go to its
+// FP64 locals (b_l = bhat_l / h^l, plus ln(unit) times the source charge sums for l = 0):
+// a coalesced write per destination, and no shuffle per value.  Each destination belongs
+// to one warp: deterministic sums.
+template <int W>
+__device__ __forceinline__ void column_round(const float (&v)[2 * W + 2], int d, bool live,
+                                             int lane, i64 next_e, i64 e1,
+                                             const int* __restrict__ entry_row, int w,
+                                             const double* __restrict__ dst_half, double ln_unit,
+                                             double* __restrict__ local_re,
+                                             double* __restrict__ local_im, float* stage,
+                                             float (&col)[(2 * W + 2 + 31) / 32],
+                                             float (&comp)[(2 * W + 2 + 31) / 32]) {
+    constexpr int V = 2 * W + 2, NC = (V + 31) / 32;
+    static_assert(V % 4 == 0, "rows of whole float4s");
+#pragma unroll
+    for (int c = 0; c < V / 4; ++c)
+        reinterpret_cast<float4*>(stage + lane * V)[c] =
+            make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+    // lane i ends its destination's entries unless entry i + 1 (or the next round's first)
+    // has the same destination
+    const int d_next = __shfl_down_sync(0xffffffffu, d, 1);
+    const bool cont = next_e < e1 && entry_row[next_e] == __shfl_sync(0xffffffffu, d, 31);
+    const unsigned ends = __ballot_sync(0xffffffffu, live && (lane == 31 ? !cont : d_next != d));
+    const unsigned lives = __ballot_sync(0xffffffffu, live);
+    __syncwarp();
+    for (int i = 0; i < 32 && ((lives >> i) & 1u); ++i) {
+        // compensated (Kahan) sums: the error of a destination's sum stays at a few
+        // roundings whatever its length
+#pragma unroll
+        for (int c = 0; c < NC; ++c) {
+            if (lane + 32 * c < V) {
+                const float y = stage[i * V + lane + 32 * c] - comp[c];
+                const float t = col[c] + y;
+                comp[c] = (t - col[c]) - y;
+                col[c] = t;
+            }
+        }
+        if ((ends >> i) & 1u) {
+            const int di = __shfl_sync(0xffffffffu, d, i);
+            // the source charge sums (columns 2W, 2W + 1) to lanes 0 and 1
+            const float a0 = __shfl_sync(0xffffffffu, col[(2 * W) / 32] - comp[(2 * W) / 32],
+                                         ((2 * W) & 31) + (lane & 1));
+            const double inv_h = 1.0 / dst_half[di];
+#pragma unroll
+            for (int c = 0; c < NC; ++c) {
+                const int k = lane + 32 * c, l = k >> 1;
+                if (k < 2 * W && l < w) {
+                    double scale = 1.0;
+                    for (int t = 0; t < l; ++t) scale *= inv_h;
+                    double add = ((double)col[c] - (double)comp[c]) * scale;
+                    if (k < 2) add += ln_unit * (double)a0;
+                    double* out = (k & 1) ? local_im : local_re;
+                    out[(i64)di * w + l] += add;
+                }
+                col[c] = 0.0f;
+                comp[c] = 0.0f;
+            }
+        }
+    }
+    __syncwarp();
+}
+
 }  // namespace td3m2l

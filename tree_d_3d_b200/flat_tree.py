@@ -194,7 +194,9 @@ MOMENTS_ONE_LAUNCH = False
 
 #: the mixed-precision M2L of ``fmm`` (mutual lists, log kernel, orders up to 14) as
 #: tensor-core products grouped by translation (td3_m2l_groups, td3_fmm_m2l_grouped)
-M2L_GROUPED = True
+#: instead of the FP32 CUDA-core form (a lane per translation).  Off: 1.71 ms per launch
+#: at 1M, p = 12, against 0.91 ms for the CUDA-core form.
+M2L_GROUPED = False
 
 
 def _group_span(theta: float) -> int:
