@@ -71,6 +71,10 @@ def _args():
                    help="the kernel of the --trace-only steps (the headline is the log kernel)")
     p.add_argument("--precision", choices=("mixed", "fp64"), default="mixed",
                    help="the precision of the --trace-only steps")
+    p.add_argument("--m2l", choices=("lanes", "grouped"), default="lanes",
+                   help="the mixed log M2L form of the --trace-only steps: a lane per "
+                        "translation on the CUDA cores (the step's) or tensor-core products "
+                        "grouped by translation")
     return p.parse_args()
 
 
@@ -401,7 +405,10 @@ def run_ours(args):
 
     kernel, precision = ("log", "mixed")
     if args.trace_only:
+        from tree_d_3d_b200 import flat_tree
+
         kernel, precision = args.kernel, args.precision
+        flat_tree.M2L_GROUPED = args.m2l == "grouped"
     for _ in range(args.warmup):
         gpu_step(pos, q, w, e, precision, kernel=kernel)
     torch.cuda.synchronize()
