@@ -118,3 +118,34 @@ def test_downward_in_one_launch_equals_the_level_by_level_pass(order, monkeypatc
     levels = [_np(t)[leaves] for t in tree._log_locals(lists)]
     for a, b in zip(one, levels):
         assert relative(a, b) < 1e-13
+
+
+@pytest.mark.parametrize("mutual", [True, False])
+def test_pair_csr_rows_equal_the_oracle_at_full_lists(oracle, mutual):
+    """td3_pair_csr (counting placement, rows ordered by input position) against the
+    reference's pair_csr on the lists of a 300k-particle tree: the same rows, partners
+    in the same order, every entry's row."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, synthetic
+    from oracle.flat_tree_oracle import lib, _p
+
+    pos, q = synthetic.mixture8(300_000, seed=17)
+    tree = FlatQuadtree(torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda"),
+                        Quad(0, 0, 1), kernel="log", order=4)
+    lists = tree._lists(0.5)
+    for name in ("m2l", "p2p"):
+        pairs = lists[name]
+        rows, partners, entry = tree._rows(pairs, mutual, entry_rows=True)
+        n = tree.node_count
+        pn = np.ascontiguousarray(_np(pairs), dtype=np.int64)
+        want_rows = np.zeros(n + 1, dtype=np.int64)
+        want_partners = np.empty(max((2 if mutual else 1) * len(pn), 1), dtype=np.int64)
+        cursor = np.empty(n, dtype=np.int64)
+        lib().pair_csr(_p(pn), len(pn), 1 if mutual else 0, _p(want_rows), n, _p(want_partners),
+                       _p(cursor))
+        got_rows = _np(rows)
+        np.testing.assert_array_equal(got_rows, want_rows)
+        total = int(got_rows[-1])
+        np.testing.assert_array_equal(_np(partners)[:total], want_partners[:total])
+        row_of = np.repeat(np.arange(n), np.diff(want_rows))
+        np.testing.assert_array_equal(_np(entry)[:total], row_of)
+        assert np.all(_np(entry)[total:] == n)
