@@ -155,10 +155,15 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
     int n_coef = (order + 1) * (order + 2) / 2;
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int p = lane & (CART_GROUP - 1), q = lane >> 3;
-    // per warp: A~ [g][partner], m~ [a][partner], T~ [b]
+    // per warp: A~ [g][partner], m~ [a][partner], T~ [b]; per block: the moments' scale
+    // (-1)^|a| / (a_x! a_y!)
     double* At = cart_smem + (size_t)wib * (2 * CART_GROUP + 1) * n_coef;
     double* Mt = At + CART_GROUP * n_coef;
     double* T = Mt + CART_GROUP * n_coef;
+    double* mscale = cart_smem + (size_t)CM2L_WARPS * (2 * CART_GROUP + 1) * n_coef;
+    for (int a = threadIdx.x; a < n_coef; a += blockDim.x)
+        mscale[a] = ((C.bx[a] + C.by[a]) & 1) ? -C.inv_fact2[a] : C.inv_fact2[a];
+    __syncthreads();
     for (i64 dst = (i64)blockIdx.x * CM2L_WARPS + wib; dst < n_dst;
          dst += (i64)gridDim.x * CM2L_WARPS) {
         i64 e0 = row_start[dst], e1 = row_start[dst + 1];
@@ -198,11 +203,19 @@ k_m2l_cart_lanes(const i64* __restrict__ row_start, const i64* __restrict__ part
                         prev1[k] = cur[k];
                     }
                 }
-            } else if (lane < 2 * CART_GROUP) {
-                const double* m = moments + src * n_coef;
-                for (int a = 0; a < n_coef; ++a) {
-                    double v = live ? m[a] * C.inv_fact2[a] : 0.0;
-                    Mt[a * CART_GROUP + p] = ((C.bx[a] + C.by[a]) & 1) ? -v : v;
+            }
+            // the partners' scaled moments, every lane loading consecutive coefficients of
+            // one partner at a time (coalesced, the loads of a partner in flight together)
+            constexpr int NC = (P + 1) * (P + 2) / 2;
+#pragma unroll 2
+            for (int pp = 0; pp < CART_GROUP; ++pp) {
+                const i64 s2 = __shfl_sync(0xffffffffu, src, pp);
+                const bool l2 = __shfl_sync(0xffffffffu, live, pp);
+                const double* m = moments + s2 * n_coef;
+#pragma unroll
+                for (int a0 = 0; a0 < NC; a0 += 32) {
+                    const int a = a0 + lane;
+                    if (a < n_coef) Mt[a * CART_GROUP + pp] = l2 ? m[a] * mscale[a] : 0.0;
                 }
             }
             __syncwarp();
@@ -258,6 +271,18 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
     float* At = cart_smem_f + (size_t)wib * (2 * CART_GROUP + 1) * n_coef;
     float* Mt = At + CART_GROUP * n_coef;
     float* T = Mt + CART_GROUP * n_coef;
+    // per block: the moments' scale (-1)^|a| / (a_x! a_y!) and degree |a|; per warp: the
+    // partners' unit powers h^-n
+    double* mscale = reinterpret_cast<double*>(
+        cart_smem_f + (size_t)CM2L_WARPS * (2 * CART_GROUP + 1) * n_coef +
+        ((CM2L_WARPS * (2 * CART_GROUP + 1) * n_coef) & 1));
+    double* hpow = mscale + n_coef + (size_t)wib * CART_GROUP * (P + 1);
+    int* mdeg = reinterpret_cast<int*>(mscale + n_coef + CM2L_WARPS * CART_GROUP * (P + 1));
+    for (int a = threadIdx.x; a < n_coef; a += blockDim.x) {
+        mscale[a] = ((C.bx[a] + C.by[a]) & 1) ? -C.inv_fact2[a] : C.inv_fact2[a];
+        mdeg[a] = C.bx[a] + C.by[a];
+    }
+    __syncthreads();
     for (i64 dst = (i64)blockIdx.x * CM2L_WARPS + wib; dst < n_dst;
          dst += (i64)gridDim.x * CM2L_WARPS) {
         i64 e0 = row_start[dst], e1 = row_start[dst + 1];
@@ -305,13 +330,26 @@ k_m2l_cart_mixed(const i64* __restrict__ row_start, const i64* __restrict__ part
                     }
                 }
             } else if (lane < 2 * CART_GROUP) {
-                const double* m = moments + src * n_coef;
+                // partner p's powers h^-n, n <= order
                 double inv_h = 1.0 / hs, pw = 1.0;
-                for (int n = 0, a = 0; n <= order; ++n, pw *= inv_h) {
-                    for (int y = 0; y <= n; ++y, ++a) {
-                        double v = live ? m[a] * C.inv_fact2[a] * pw : 0.0;
-                        Mt[a * CART_GROUP + p] = (float)((n & 1) ? -v : v);
-                    }
+                for (int n = 0; n <= order; ++n, pw *= inv_h) hpow[p * (P + 1) + n] = pw;
+            }
+            __syncwarp();
+            // the partners' moments in units of their h, every lane loading consecutive
+            // coefficients of one partner at a time (coalesced, the loads of a partner in
+            // flight together)
+            constexpr int NC = (P + 1) * (P + 2) / 2;
+#pragma unroll 2
+            for (int pp = 0; pp < CART_GROUP; ++pp) {
+                const i64 s2 = __shfl_sync(0xffffffffu, src, pp);
+                const bool l2 = __shfl_sync(0xffffffffu, live, pp);
+                const double* m = moments + s2 * n_coef;
+#pragma unroll
+                for (int a0 = 0; a0 < NC; a0 += 32) {
+                    const int a = a0 + lane;
+                    if (a < n_coef)
+                        Mt[a * CART_GROUP + pp] =
+                            l2 ? (float)(m[a] * mscale[a] * hpow[pp * (P + 1) + mdeg[a]]) : 0.0f;
                 }
             }
             // ratio^(1 + nb) for this lane's chunks (their degrees only grow)
@@ -423,7 +461,7 @@ extern "C" int td3_cart_m2l(const int64_t* row_start, const int64_t* partners, i
                 C.inv_fact2[i] = 1.0 / (f[n - y] * f[y]);
             }
         cart_chunks(order, C);
-        size_t lane_smem = sizeof(double) * (2 * CART_GROUP + 1) * n_coef * CM2L_WARPS;
+        size_t lane_smem = sizeof(double) * ((2 * CART_GROUP + 1) * n_coef * CM2L_WARPS + n_coef);
         i64 nb = (n_dst + CM2L_WARPS - 1) / CM2L_WARPS;
         unsigned grid = (unsigned)(nb < 148 * 64 ? nb : 148 * 64);
         auto run = [&](auto kernel) -> int {
@@ -488,7 +526,10 @@ extern "C" int td3_cart_m2l_mixed(const int64_t* row_start, const int64_t* partn
     cudaStream_t s = td3_stream(stream);
     int n_coef = (order + 1) * (order + 2) / 2;
     CartScale C = cart_scale(order);
-    size_t smem = sizeof(float) * (2 * CART_GROUP + 1) * n_coef * CM2L_WARPS;
+    // per-warp areas (floats, padded to 8 bytes), the scale table, the unit powers, degrees
+    size_t smem = sizeof(float) * ((2 * CART_GROUP + 1) * n_coef * CM2L_WARPS + 1) +
+                  sizeof(double) * (n_coef + CM2L_WARPS * CART_GROUP * (CART_LANE_MAX + 1)) +
+                  sizeof(int) * n_coef;
     i64 nb = (n_dst + CM2L_WARPS - 1) / CM2L_WARPS;
     unsigned grid = (unsigned)(nb < 148 * 64 ? nb : 148 * 64);
     auto run = [&](auto kernel) -> int {
