@@ -128,11 +128,12 @@ __global__ void k_l2l_log_level(i64 lo, i64 hi, int order, const double* __restr
                                 double* __restrict__ local_im) {
     td3_chain_wait();
     td3_chain_release();
-    int w = order + 1;
-    i64 t = (i64)blockIdx.x * blockDim.x + threadIdx.x;
-    i64 ch = lo + t / w;
+    const unsigned w = (unsigned)order + 1u;
+    // (child, coefficient) from a 32-bit thread index (a level's (hi - lo) w < 2^32)
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x, tc = t / w;
+    i64 ch = lo + (i64)tc;
     if (ch >= hi || end[ch] == start[ch]) return;
-    int m = (int)(t % w);
+    int m = (int)(t - tc * w);
     i64 node = parent[ch];
     double s_re = center[2 * ch] - center[2 * node];
     double s_im = center[2 * ch + 1] - center[2 * node + 1];
@@ -451,6 +452,7 @@ extern "C" int td3_fmm_downward(const int64_t* levels, int64_t n_levels, const d
         i64 lo = levels[level], hi = levels[level + 1];
         if (hi <= lo) continue;
         i64 threads = (hi - lo) * w;
+        if (threads > 0xffffffffLL) return TD3_EINVAL;
         TD3_TRY(td3_launch_chained(k_l2l_log_level, td3_blocks(threads, 256), 256, 0, s, lo, hi,
                                    order, node_center, node_parent, node_start, node_end,
                                    binomial, binomial_size, local_re, local_im));
