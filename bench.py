@@ -7,8 +7,7 @@ A step takes the 1M particles of the workload (8-Gaussian mixture, +-1 charges o
 zero; log kernel, order 12, theta 0.5, leaf 8, unsoftened), builds a fresh tree
 (build, moments, traversal, interaction lists) and evaluates the FMM potential and
 field at every particle in mixed precision (FP32 near field with compensated sums,
-M2L as 3xTF32 tensor-core products grouped by translation on size-scaled expansions,
-FP64 M2M / L2L / L2P), then runs the hand-written
+FP32 M2L on size-scaled expansions, FP64 M2M / L2L / L2P), then runs the hand-written
 backward of L = sum w phi + sum e . E (fixed seeded w, e) to dL/dq and dL/dx.
 ``value`` is whole-job particles/s with the inputs resident in HBM; the same step in
 the plain FP64 form is timed beside it (``fp64``), and the mixed field error against
