@@ -1,6 +1,6 @@
 """The stable radix sort (td3_radix_sort_pairs) against NumPy's stable argsort.
 
-Sizes straddle the 4096-item tile (empty, single, ragged tails, many tiles); keys cover
+Sizes straddle the 2048-item tile and twice it (empty, single, ragged tails, many tiles); keys cover
 heavy duplication, a single repeated key, and sorts on fewer bits than the keys hold
 (the high bits must then be ignored, equal low bits kept in input order).
 """
@@ -50,5 +50,18 @@ def test_radix_sort_is_stable_and_matches_numpy(n, kind):
     ko, vo = _sort(keys, bits)
     low = keys & np.uint64((1 << bits) - 1) if bits < 32 else keys
     order = np.argsort(low, kind="stable")
+    assert np.array_equal(vo, order)
+    assert np.array_equal(ko, keys[order].astype(np.int64))
+
+
+@pytest.mark.parametrize("bits", [1, 5, 8, 9, 11, 12, 16, 20, 22, 23, 27, 31])
+def test_radix_sort_digit_widths(bits):
+    """Key widths that end on a full and on a partial digit: stable against NumPy on
+    keys whose high bits must be ignored."""
+    rng = np.random.default_rng(bits)
+    n = 250_007
+    keys = rng.integers(0, 2**32, n, dtype=np.uint64)
+    ko, vo = _sort(keys, bits)
+    order = np.argsort(keys & np.uint64((1 << bits) - 1), kind="stable")
     assert np.array_equal(vo, order)
     assert np.array_equal(ko, keys[order].astype(np.int64))
