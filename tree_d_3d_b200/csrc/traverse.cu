@@ -100,7 +100,6 @@ __device__ __forceinline__ int classify_dual(i64 a, i64 b, const NodeRec* __rest
 constexpr int GEN_ITEMS = 8;
 constexpr int GEN_TILE = TRAV_THREADS * GEN_ITEMS;
 constexpr int GEN_BATCH = 8;
-constexpr int GEN_SCAN_THREADS = 1024;
 
 struct TravState {
     i64 nf[2];          // frontier size of even / odd generations
@@ -109,6 +108,7 @@ struct TravState {
     i64 base_m2l, base_p2p;
     i64 overflow;       // a list or the next frontier outgrew its buffer
     i64 need_m2l, need_p2p, need_frontier;
+    unsigned long long arrived;  // classify blocks done in the current generation
 };
 
 template <bool DUAL>
@@ -158,15 +158,17 @@ __global__ void k_gen_init(TravState* st, FPair* frontier) {
     st->emit_nf = 0;
     st->n_m2l = st->n_p2p = st->base_m2l = st->base_p2p = 0;
     st->overflow = st->need_m2l = st->need_p2p = st->need_frontier = 0;
+    st->arrived = 0;
     frontier[0] = FPair{0, 0};
 }
 
 template <bool DUAL>
 __global__ void __launch_bounds__(TRAV_THREADS)
-k_gen_classify(const FPair* __restrict__ frontier, const TravState* st, int parity,
+k_gen_classify(const FPair* __restrict__ frontier, TravState* st, int parity,
                const NodeRec* __restrict__ t, const NodeRec* __restrict__ s, double theta,
-               signed char* __restrict__ action,
-               td3_i64x2* __restrict__ tile_sum) {
+               signed char* __restrict__ action, td3_i64x2* __restrict__ tile_sum,
+               i64 m2l_capacity, i64 p2p_capacity, i64 frontier_capacity) {
+    __shared__ bool last;
     td3_chain_wait();
     td3_chain_release();
     i64 nf = st->nf[parity];
@@ -186,25 +188,29 @@ k_gen_classify(const FPair* __restrict__ frontier, const TravState* st, int pari
         block_exclusive_x2(sum, &total);
         if (threadIdx.x == 0) tile_sum[tile] = total;
     }
-}
-
-__global__ void __launch_bounds__(GEN_SCAN_THREADS)
-k_gen_scan(TravState* st, int parity, td3_i64x2* __restrict__ tile_sum, i64 m2l_capacity,
-           i64 p2p_capacity, i64 frontier_capacity) {
-    td3_chain_wait();
-    td3_chain_release();
-    i64 nf = st->nf[parity];
-    i64 tiles = (nf + GEN_TILE - 1) / GEN_TILE;
+    // The last block to finish scans the tile sums (no block waits: the others leave).
+    if (threadIdx.x == 0) {
+        __threadfence();  // this block's tile sums before its arrival
+        last = atomicAdd(&st->arrived, 1ull) == (unsigned long long)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
     td3_i64x2 carry(0);
-    for (i64 c = 0; c < tiles; c += GEN_SCAN_THREADS) {
+    for (i64 c = 0; c < tiles; c += blockDim.x) {
         i64 tile = c + threadIdx.x;
-        td3_i64x2 v = tile < tiles ? tile_sum[tile] : td3_i64x2(0);
+        td3_i64x2 v(0);
+        if (tile < tiles) {
+            v.a = __ldcg(reinterpret_cast<const long long*>(&tile_sum[tile].a));
+            v.b = __ldcg(reinterpret_cast<const long long*>(&tile_sum[tile].b));
+        }
         td3_i64x2 total;
         td3_i64x2 ex = block_exclusive_x2(v, &total);
         if (tile < tiles) tile_sum[tile] = carry + ex;
         carry += total;
     }
     if (threadIdx.x == 0) {
+        st->arrived = 0;
         i64 add_m2l = carry.a & 0xffffffffLL, add_p2p = carry.a >> 32, nn = carry.b;
         st->base_m2l = st->n_m2l;
         st->base_p2p = st->n_p2p;
@@ -341,10 +347,8 @@ int run_generations(const NodeRec* t, const NodeRec* s, double theta, Pair* m2l,
         for (int k = 0; k < GEN_BATCH; ++k, ++gen) {
             int parity = gen & 1;
             TD3_TRY(td3_launch_chained(k_gen_classify<DUAL>, grid, TRAV_THREADS, 0, stream,
-                                       (const FPair*)b.frontier[parity], (const TravState*)b.state,
-                                       parity, t, s, theta, b.action, b.tile_sum));
-            TD3_TRY(td3_launch_chained(k_gen_scan, 1, GEN_SCAN_THREADS, 0, stream, b.state, parity,
-                                       b.tile_sum, m2l_capacity, p2p_capacity,
+                                       (const FPair*)b.frontier[parity], b.state, parity, t, s,
+                                       theta, b.action, b.tile_sum, m2l_capacity, p2p_capacity,
                                        frontier_capacity));
             TD3_TRY(td3_launch_chained(k_gen_emit<DUAL>, grid, TRAV_THREADS, 0, stream,
                                        (const FPair*)b.frontier[parity], (const TravState*)b.state,
