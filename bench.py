@@ -71,10 +71,10 @@ def _args():
                    help="the kernel of the --trace-only steps (the headline is the log kernel)")
     p.add_argument("--precision", choices=("mixed", "fp64"), default="mixed",
                    help="the precision of the --trace-only steps")
-    p.add_argument("--m2l", choices=("lanes", "grouped"), default="lanes",
-                   help="the mixed log M2L form of the --trace-only steps: a lane per "
-                        "translation on the CUDA cores (the step's) or tensor-core products "
-                        "grouped by translation")
+    p.add_argument("--m2l", choices=("rows", "lanes", "grouped"), default="rows",
+                   help="the mixed log M2L form of the --trace-only steps on the CUDA cores: "
+                        "8 lanes per destination row (the step's) or a lane per translation; "
+                        "or tensor-core products grouped by translation")
     return p.parse_args()
 
 
@@ -306,7 +306,8 @@ def count_our_launches(fn, torch):
 
 def time_m2l_mixed(tree, torch, reps, form="grouped"):
     """One mixed M2L form alone (CUDA events on its stream), average ms per launch:
-    "lanes" the FP32 CUDA-core form (a lane per translation, the step's form), "grouped"
+    "rows" the FP32 CUDA-core form with 8 lanes per destination row (the step's form),
+    "lanes" the FP32 CUDA-core form with a lane per translation, "grouped"
     the tensor-core products grouped by translation, "tile" the per-translation
     tensor-core form."""
     from tree_d_3d_b200 import _lib
@@ -324,6 +325,16 @@ def time_m2l_mixed(tree, torch, reps, form="grouped"):
 
         def launch():
             tree._m2l_grouped(groups, hat, lre, lim)
+    elif form == "rows":
+        coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
+        records = tree._source_records((tree.moment_re, tree.moment_im))
+        args = (lists["m2l_rows"].data_ptr(), lists["m2l_partners"].data_ptr(), count,
+                tree.node_center.data_ptr(), tree.node_half.data_ptr(), records.data_ptr(),
+                tree.order, coeff.ctypes.data, tree._unit, lre.data_ptr(), lim.data_ptr(),
+                stream)
+
+        def launch():
+            _lib.call("td3_fmm_m2l_mixed_rows", *args)
     else:
         coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
         args = (lists["m2l_rows"].data_ptr(), lists["m2l_entry_row"].data_ptr(),
@@ -409,6 +420,7 @@ def run_ours(args):
 
         kernel, precision = args.kernel, args.precision
         flat_tree.M2L_GROUPED = args.m2l == "grouped"
+        flat_tree.M2L_ROWS = args.m2l == "rows"
     for _ in range(args.warmup):
         gpu_step(pos, q, w, e, precision, kernel=kernel)
     torch.cuda.synchronize()
@@ -518,7 +530,8 @@ def run_ours(args):
         coulomb[prec]["rel_err_field"], _ = field_error(pos, q, prec, torch, kernel="coulomb")
     # the step's M2L form (FP32 on the CUDA cores, a lane per translation); the tensor-core
     # forms (products grouped by translation; per translation) are timed beside it
-    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, form="lanes")
+    m2l_ms, n_m2l = time_m2l_mixed(tree, torch, reps=5, form="rows")
+    m2l_lanes_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="lanes")
     m2l_grouped_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="grouped")
     m2l_tile_ms, _ = time_m2l_mixed(tree, torch, reps=5, form="tile")
     groups = tree._m2l_groups(tree._lists(THETA)["m2l"], THETA)
@@ -531,7 +544,7 @@ def run_ours(args):
     # per run: D[128 x 64] += A_hi [128 x 32] B^T and D[128 x 32] += A_lo B_hi^T
     issued = n_runs * 2 * 128 * 32 * (64 + 32)
     roofline = {
-        "kernel": "k_m2l_mixed<12> (FP32 M2L, a lane per translation, forward)",
+        "kernel": "k_m2l_mixed_rows<12> (FP32 M2L, 8 lanes per destination row, forward)",
         "bound": "fp32",
         "achieved": achieved,
         "peak": FP32_PEAK,
@@ -555,6 +568,7 @@ def run_ours(args):
             "peak_source": f"dense TF32 = half the BF16 tensor rate, {peak_note}",
         },
         "tile_form_ms_per_launch": m2l_tile_ms,
+        "lane_form_ms_per_launch": m2l_lanes_ms,
     }
     clock = clocks.summary()
     if dist:

@@ -322,6 +322,27 @@ int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
                       double unit, int tensor_cores, double* local_re, double* local_im,
                       int64_t* status, void* stream);
 
+/* The same mixed-precision log M2L (same formula, arguments and accuracy as
+ * td3_fmm_m2l_mixed with tensor_cores = 0) with a group of 8 lanes per destination row:
+ * each lane keeps its partial sums of the row in FP32 registers, the group's 8 partial
+ * rows are summed pairwise at the row's end and added to local_re / local_im (FP64);
+ * rows above 96 entries are taken by a whole warp (32 partial rows).  Every destination
+ * is summed by one group in a fixed order (deterministic).  The sources come as packed
+ * records (td3_pack_m2l_sources: td3_m2l_record_floats(order) floats per node, 16-byte
+ * aligned: the centre as two doubles, hat_k = a_k / h^k as FP32 pairs, h / unit; 128
+ * bytes at order 12, one cache line per gathered partner) written from the source tree's
+ * FP64 moments, centres and half-widths.  Orders <= 20; coeff HOST.  Replaces
+ * fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/fmm_m2l_host_pyccel.py:16-105) in
+ * FP32 for fmm / fmm_at (src/tree_d_3d/flat_tree.py:1505-1539, :1151-1316). */
+int td3_m2l_record_floats(int order);
+int td3_pack_m2l_sources(int64_t count, int order, const double* moment_re,
+                         const double* moment_im, const double* node_center,
+                         const double* node_half, double unit, float* records, void* stream);
+int td3_fmm_m2l_mixed_rows(const int64_t* row_start, const int64_t* partners, int64_t n_dst,
+                           const double* dst_center, const double* dst_half,
+                           const float* records, int order, const double* coeff, double unit,
+                           double* local_re, double* local_im, void* stream);
+
 /* The mixed-precision log M2L of the mutual lists of one tree as dense tensor-core
  * products grouped by translation (tcgen05.mma, 3xTF32 with FP32 accumulation), orders
  * up to TD3_M2L_GROUPED_MAX_ORDER.  A translation between cells whose depths differ by

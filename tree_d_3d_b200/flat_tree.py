@@ -198,6 +198,11 @@ MOMENTS_ONE_LAUNCH = False
 #: at 1M, p = 12, against 0.91 ms for the CUDA-core form.
 M2L_GROUPED = False
 
+#: the mixed-precision CUDA-core M2L with a group of 8 lanes per destination row
+#: (td3_fmm_m2l_mixed_rows: partial sums in registers, packed 128-byte source records)
+#: instead of a lane per entry across row boundaries (td3_fmm_m2l_mixed).
+M2L_ROWS = True
+
 
 def _group_span(theta: float) -> int:
     """Offsets (in units of the smaller half-width) covered by the grouped M2L's
@@ -846,6 +851,19 @@ class FlatQuadtree:
                   _lib.stream(self.device))
         return hat
 
+    def _source_records(self, moments):
+        """Packed source cells of the row-group M2L (td3_pack_m2l_sources): centre (FP64),
+        hat_k = a_k / h^k (FP32 pairs) and h / unit, td3_m2l_record_floats(order) floats
+        per node."""
+        mre, mim = moments
+        width = _lib.lib().td3_m2l_record_floats(self.order)
+        records = torch.empty((self.node_count, width), dtype=torch.float32,
+                              device=self.device)
+        _lib.call("td3_pack_m2l_sources", self.node_count, self.order, mre.data_ptr(),
+                  mim.data_ptr(), self.node_center.data_ptr(), self.node_half.data_ptr(),
+                  self._unit, records.data_ptr(), _lib.stream(self.device))
+        return records
+
     def _tensor_status(self) -> torch.Tensor:
         """The device word the tensor-core M2L raises when a wait for the tensor cores
         runs out (checked by _check_tensor_cores)."""
@@ -877,6 +895,13 @@ class FlatQuadtree:
             rows, partners = lists["m2l_rows"], lists["m2l_partners"]
             coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
             tensor = 1 if M2L_TENSOR_CORES and self.order <= 15 else 0
+            if M2L_ROWS and not tensor:
+                records = self._source_records(moments)
+                _lib.call("td3_fmm_m2l_mixed_rows", rows.data_ptr(), partners.data_ptr(),
+                          dst.node_count, dst.node_center.data_ptr(), dst.node_half.data_ptr(),
+                          records.data_ptr(), self.order, coeff.ctypes.data, self._unit,
+                          local_re.data_ptr(), local_im.data_ptr(), stream)
+                return
             _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), lists["m2l_entry_row"].data_ptr(),
                       partners.data_ptr(), dst.node_count,
                       dst.node_center.data_ptr(), dst.node_half.data_ptr(),
