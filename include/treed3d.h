@@ -491,6 +491,29 @@ int td3_fmm_evaluate(int kernel, const double* sorted_pos, const double* sorted_
                      int mixed, double unit, double* phi, double* field, int64_t* status,
                      void* stream);
 
+/* The mixed-precision form of td3_fmm_evaluate (same arguments, outputs, status and
+ * accuracy contract as mixed = 1) in three launches: the local expansions at every
+ * particle in FP64, one thread per slot (slot_leaf: the leaf of every particle slot,
+ * td3_slot_leaves), then the pair sums added to them, one warp per plan segment, then
+ * the partial sums of leaves with several segments.  Pair arithmetic without FP64:
+ * positions relative to the target leaf's centre in units of the power of two u with
+ * unit <= u < 2 unit, held as FP32 hi + lo pairs, a pair's difference
+ * (hi_i - hi_j) + (lo_i - lo_j); compensated sums as td3_fmm_evaluate.  slot_leaf is
+ * required.  Replaces fmm_evaluate_host (src/tree_d_3d/kernels/fmm_evaluate_host/
+ * fmm_evaluate_host_pyccel.py:14-100) and cart_evaluate_host (kernels/cart_evaluate_host/
+ * cart_evaluate_host_pyccel.py:16-110) in FP32. */
+int td3_slot_leaves(int64_t n_nodes, const int64_t* node_child, const int64_t* node_start,
+                    const int64_t* node_end, int32_t* slot_leaf, void* stream);
+int td3_fmm_evaluate_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+                           const int64_t* perm, int64_t n, const double* node_center,
+                           const int64_t* node_start, const int64_t* node_end, int order,
+                           const double* local_a, const double* local_b,
+                           const int32_t* slot_leaf, const int64_t* p2p_partners,
+                           const int* seg_leaf, const int64_t* seg_range, const int64_t* seg_out,
+                           int64_t n_seg, double* partial, double softening, int with_potential,
+                           double unit, double* phi, double* field, int64_t* status,
+                           void* stream);
+
 /* fmm_at: L2P at the m targets (sorted_targets (2, m) in target-tree order, target_perm
  * their input indices, sorted_exclude their excluded source index) plus exact sums over
  * the partner source leaves of each target leaf (the one-way P2P rows cut by
@@ -552,6 +575,22 @@ int td3_fmm_adjoint(int kernel, const double* sorted_pos, const double* sorted_c
                     double* partial, const double* sorted_weight, const double* sorted_dipole,
                     const double* efield, double softening, int mixed, double unit,
                     double* qbar, double* xbar, void* stream);
+
+/* The mixed-precision form of td3_fmm_adjoint (mixed = 1 implied) laid out as
+ * td3_fmm_evaluate_mixed: the far parts of qbar and xbar at every particle in FP64, one
+ * thread per slot (slot_leaf required), then the near parts added pair by pair without
+ * FP64 arithmetic (qbar and xbar are linear in the near sums), then the partial sums of
+ * multi-segment leaves.  No reference counterpart. */
+int td3_fmm_adjoint_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+                          const int64_t* perm, int64_t n, const double* node_center,
+                          const int64_t* node_start, const int64_t* node_end, int order,
+                          const double* fwd_a, const double* fwd_b, const double* adj_a,
+                          const double* adj_b, const int32_t* slot_leaf,
+                          const int64_t* p2p_partners, const int* seg_leaf,
+                          const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
+                          double* partial, const double* sorted_weight,
+                          const double* sorted_dipole, const double* efield, double softening,
+                          double unit, double* qbar, double* xbar, void* stream);
 
 /* ------------------------------------------------------------------ grounded strip */
 

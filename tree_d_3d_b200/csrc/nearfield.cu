@@ -19,6 +19,12 @@ constexpr int NF_WARPS = 4;
 constexpr int LOCAL_COMPLEX = 0;
 constexpr int LOCAL_CART = 1;
 
+// Blocks of a finish launch: a warp per 32 segments, at most 148 x 16 blocks.
+static inline unsigned td3_finish_blocks(i64 n_seg) {
+    const i64 warps = (n_seg + 31) / 32, blocks = (warps + NF_WARPS - 1) / NF_WARPS;
+    return (unsigned)(blocks < 1 ? 1 : blocks > 148 * 16 ? 148 * 16 : blocks);
+}
+
 __device__ __forceinline__ int pow2_at_least(int v) {
     int p = 1;
     while (p < v) p <<= 1;
@@ -458,21 +464,16 @@ __device__ __forceinline__ i64 leaf_segments(const int* __restrict__ seg_leaf, i
     }
 }
 
-// Leaves whose row took several segments: partial sums in segment order, plus L2P.
-template <bool POT, int LOCAL>
-__global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_leaf,
-                              const i64* __restrict__ seg_out, const double* __restrict__ local_a,
-                              const double* __restrict__ local_b, int order, int width,
-                              const double* __restrict__ partial, double* __restrict__ phi,
-                              double* __restrict__ field) {
-    td3_chain_wait();
-    td3_chain_release();
-    i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (seg >= n_seg) return;
-    i64 p0 = seg_out[seg];
-    // the first segment of a multi-segment leaf finishes it
-    if (p0 < 0 || (seg > 0 && seg_leaf[seg - 1] == seg_leaf[seg])) return;
+// One multi-segment leaf (its first segment `seg`): every target's partial sums over the
+// segments, then L2P (or, ADD, added to what k_far_field wrote).
+template <bool POT, int LOCAL, bool ADD>
+__device__ __forceinline__ void finish_leaf(Targets T, i64 n_seg, const int* __restrict__ seg_leaf,
+                                            const i64* __restrict__ seg_out,
+                                            const double* __restrict__ local_a,
+                                            const double* __restrict__ local_b, int order,
+                                            int width, const double* __restrict__ partial,
+                                            double* __restrict__ phi, double* __restrict__ field,
+                                            i64 seg, int lane) {
     i64 leaf = seg_leaf[seg];
     i64 s0 = T.start[leaf];
     int count = (int)(T.end[leaf] - s0);
@@ -492,7 +493,12 @@ __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_
             ex += __shfl_xor_sync(0xffffffffu, ex, off);
             ey += __shfl_xor_sync(0xffffffffu, ey, off);
         }
-        if (lane == (it & 31)) {
+        if (ADD && lane == (it & 31)) {
+            const i64 i = T.perm[s0 + it];
+            if (POT) phi[i] += pot;
+            field[i] += ex;
+            field[T.m + i] += ey;
+        } else if (lane == (it & 31)) {
             i64 k = s0 + it;
             double xi = T.pos[k], yi = T.pos[T.m + k];
             double lp, lx, ly;
@@ -502,6 +508,36 @@ __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_
             phi[i] = POT ? lp + pot : 0.0;
             field[i] = lx + ex;
             field[T.m + i] = ly + ey;
+        }
+    }
+}
+
+// Leaves whose row took several segments: partial sums in segment order, plus L2P (or,
+// ADD, added to the far field k_far_field wrote).  Launched over a fraction of the
+// segments' warps (td3_finish_blocks): most leaves have one segment.
+template <bool POT, int LOCAL, bool ADD = false>
+__global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_leaf,
+                              const i64* __restrict__ seg_out, const double* __restrict__ local_a,
+                              const double* __restrict__ local_b, int order, int width,
+                              const double* __restrict__ partial, double* __restrict__ phi,
+                              double* __restrict__ field) {
+    td3_chain_wait();
+    td3_chain_release();
+    const int lane = threadIdx.x & 31;
+    // the first segment of a multi-segment leaf finishes it; each warp scans 32 segments
+    // at a time for them
+    const i64 warps = (i64)gridDim.x * NF_WARPS;
+    for (i64 base = ((i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5)) * 32; base < n_seg;
+         base += warps * 32) {
+        const i64 mine = base + lane;
+        unsigned firsts = __ballot_sync(
+            0xffffffffu, mine < n_seg && seg_out[mine] >= 0 &&
+                             (mine == 0 || seg_leaf[mine - 1] != seg_leaf[mine]));
+        while (firsts) {
+            const i64 seg = base + __ffs(firsts) - 1;
+            firsts &= firsts - 1;
+            finish_leaf<POT, LOCAL, ADD>(T, n_seg, seg_leaf, seg_out, local_a, local_b, order,
+                                         width, partial, phi, field, seg, lane);
         }
     }
 }
@@ -598,6 +634,16 @@ __device__ __forceinline__ void adjoint_combine(const double* acc, const LocalJe
     A.qbar[i] = psi;
     A.xbar[i] = -w * A.efield[i] + q * gx - (mxx * ex + mxy * ey);
     A.xbar[n + i] = -w * A.efield[n + i] + q * gy - (mxy * ex + myy * ey);
+}
+
+// The near part of qbar and xbar of slot k (input index i), added to the far part that
+// k_far_adjoint wrote (qbar and xbar are linear in the near sums acc).
+__device__ __forceinline__ void adjoint_add(const double* acc, i64 k, i64 i, i64 n,
+                                            const Sources& S, const Adjoint& A) {
+    const double q = S.charge[k], ex = A.dipole[k], ey = A.dipole[n + k];
+    A.qbar[i] += acc[0];
+    A.xbar[i] += q * acc[1] - (acc[3] * ex + acc[4] * ey);
+    A.xbar[n + i] += q * acc[2] - (acc[4] * ex + acc[5] * ey);
 }
 
 template <int LOCAL>
@@ -749,20 +795,17 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
     }
 }
 
-template <int LOCAL>
-__global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg,
-                                      const int* __restrict__ seg_leaf,
-                                      const i64* __restrict__ seg_out, const double* __restrict__ fa,
-                                      const double* __restrict__ fb, const double* __restrict__ ba,
-                                      const double* __restrict__ bb, int order, int width,
-                                      const double* __restrict__ partial) {
-    td3_chain_wait();
-    td3_chain_release();
-    i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
-    int lane = threadIdx.x & 31;
-    if (seg >= n_seg) return;
-    i64 p0 = seg_out[seg];
-    if (p0 < 0 || (seg > 0 && seg_leaf[seg - 1] == seg_leaf[seg])) return;
+// One multi-segment leaf of the adjoint pass (its first segment `seg`), as finish_leaf.
+template <int LOCAL, bool ADD>
+__device__ __forceinline__ void finish_adjoint_leaf(Targets T, Sources S, Adjoint A, i64 n_seg,
+                                                    const int* __restrict__ seg_leaf,
+                                                    const i64* __restrict__ seg_out,
+                                                    const double* __restrict__ fa,
+                                                    const double* __restrict__ fb,
+                                                    const double* __restrict__ ba,
+                                                    const double* __restrict__ bb, int order,
+                                                    int width, const double* __restrict__ partial,
+                                                    i64 seg, int lane) {
     i64 leaf = seg_leaf[seg];
     i64 s0 = T.start[leaf];
     int count = (int)(T.end[leaf] - s0);
@@ -776,11 +819,334 @@ __global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg
         for (int c = 0; c < 6; ++c)
             for (int off = 16; off > 0; off >>= 1)
                 acc[c] += __shfl_xor_sync(0xffffffffu, acc[c], off);
-        if (lane == (it & 31)) {
+        if (ADD && lane == (it & 31)) {
+            adjoint_add(acc, s0 + it, T.perm[s0 + it], S.n, S, A);
+        } else if (lane == (it & 31)) {
             i64 k = s0 + it;
             adjoint_finish<LOCAL>(acc, k, T.perm[k], S.n, S.pos[k] - T.center[2 * leaf],
                                   S.pos[S.n + k] - T.center[2 * leaf + 1], leaf, order, width,
                                   fa, fb, ba, bb, S, A);
+        }
+    }
+}
+
+template <int LOCAL, bool ADD = false>
+__global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg,
+                                      const int* __restrict__ seg_leaf,
+                                      const i64* __restrict__ seg_out, const double* __restrict__ fa,
+                                      const double* __restrict__ fb, const double* __restrict__ ba,
+                                      const double* __restrict__ bb, int order, int width,
+                                      const double* __restrict__ partial) {
+    td3_chain_wait();
+    td3_chain_release();
+    const int lane = threadIdx.x & 31;
+    const i64 warps = (i64)gridDim.x * NF_WARPS;
+    for (i64 base = ((i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5)) * 32; base < n_seg;
+         base += warps * 32) {
+        const i64 mine = base + lane;
+        unsigned firsts = __ballot_sync(
+            0xffffffffu, mine < n_seg && seg_out[mine] >= 0 &&
+                             (mine == 0 || seg_leaf[mine - 1] != seg_leaf[mine]));
+        while (firsts) {
+            const i64 seg = base + __ffs(firsts) - 1;
+            firsts &= firsts - 1;
+            finish_adjoint_leaf<LOCAL, ADD>(T, S, A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb,
+                                            order, width, partial, seg, lane);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ mixed form at the sources
+// The mixed-precision near field at the sources in three launches: the far field of every
+// particle in FP64, one thread per slot (k_far_field / k_far_adjoint: every lane busy,
+// where a segment's warp would run it on one lane per target), then the pair sums,
+// added to it (k_near_mixed / k_near_adjoint_mixed), then the partial sums of the leaves
+// that took several segments (k_near_finish / k_near_adjoint_finish with ADD).
+//
+// Pair arithmetic: positions relative to the target leaf's centre, in units of the
+// power-of-two length u (pair_unit), as FP32 hi + lo pairs (x = hi + lo to 2^-48
+// relative); a pair's difference is (hi_i - hi_j) + (lo_i - lo_j), exact in its hi part
+// for close pairs, so no FP64 operation is left in the pair loop.  Lanes are (target,
+// slice) with floor(32 / targets) slices (no power-of-two rounding); the slices of a
+// target are added by a fixed-order tree.
+
+// Slot -> leaf: the leaf holding every particle slot (thread per node).
+__global__ void k_slot_leaves(i64 n_nodes, const i64* __restrict__ child,
+                              const i64* __restrict__ start, const i64* __restrict__ end,
+                              int* __restrict__ slot_leaf) {
+    td3_chain_wait();
+    td3_chain_release();
+    const i64 node = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (node >= n_nodes || child[node] >= 0) return;
+    for (i64 k = start[node]; k < end[node]; ++k) slot_leaf[k] = (int)node;
+}
+
+template <int LOCAL, bool POT>
+__global__ void k_far_field(Targets T, const int* __restrict__ slot_leaf,
+                            const double* __restrict__ la, const double* __restrict__ lb,
+                            int order, int width, double* __restrict__ phi,
+                            double* __restrict__ field) {
+    td3_chain_wait();
+    td3_chain_release();
+    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= T.m) return;
+    const i64 leaf = slot_leaf[k];
+    double lp, lx, ly;
+    eval_local<LOCAL>(la, lb, leaf, order, width, T.pos[k] - T.center[2 * leaf],
+                      T.pos[T.m + k] - T.center[2 * leaf + 1], lp, lx, ly);
+    const i64 i = T.perm[k];
+    phi[i] = POT ? lp : 0.0;
+    field[i] = lx;
+    field[T.m + i] = ly;
+}
+
+template <int LOCAL>
+__global__ void k_far_adjoint(Targets T, Sources S, Adjoint A, const int* __restrict__ slot_leaf,
+                              const double* __restrict__ fa, const double* __restrict__ fb,
+                              const double* __restrict__ ba, const double* __restrict__ bb,
+                              int order, int width) {
+    td3_chain_wait();
+    td3_chain_release();
+    const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= T.m) return;
+    const double zero[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    const i64 leaf = slot_leaf[k];
+    adjoint_finish<LOCAL>(zero, k, T.perm[k], S.n, T.pos[k] - T.center[2 * leaf],
+                          T.pos[T.m + k] - T.center[2 * leaf + 1], leaf, order, width, fa, fb,
+                          ba, bb, S, A);
+}
+
+// x in units of u relative to c, as an FP32 hi + lo pair.
+__device__ __forceinline__ float2 split_rel(double x, double c, double inv_u) {
+    const double v = (x - c) * inv_u;
+    const float hi = (float)v;
+    return make_float2(hi, (float)(v - (double)hi));
+}
+
+// Lanes (target, slice): targets t of the leaf in chunks of tsz, floor(32 / tsz) slices.
+struct LaneMap {
+    int tsz, slices, ti, slice;
+    __device__ LaneMap(int count, int lane) {
+        tsz = count < 32 ? count : 32;
+        slices = 32 / tsz;
+        ti = lane % tsz;
+        slice = lane / tsz;
+    }
+    // v summed over the slices of each target into the slice-0 lane (fixed-order tree)
+    template <int N>
+    __device__ void sum_slices(double (&v)[N]) const {
+        for (int off = 1; off < slices; off <<= 1) {
+            const bool take = slice % (2 * off) == 0 && slice + off < slices;
+#pragma unroll
+            for (int c = 0; c < N; ++c) {
+                const double o = __shfl_down_sync(0xffffffffu, v[c], off * tsz);
+                if (take) v[c] += o;
+            }
+        }
+    }
+};
+
+constexpr int NM_CAP = 128;  // staged sources per warp window (mixed forward)
+
+struct MixedWindow {
+    float4 pos[NM_CAP];  // (x hi, x lo, y hi, y lo) relative to the target leaf's centre
+    double q[NM_CAP];
+    float qf[NM_CAP];
+    int tag[NM_CAP];  // slot j (self-exclusion)
+};
+
+template <int KERNEL, bool POT>
+__global__ void __launch_bounds__(32 * NF_WARPS, 8)
+k_near_mixed(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
+             const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
+             const i64* __restrict__ partners, double eps2, double* __restrict__ partial,
+             double* __restrict__ phi, double* __restrict__ field, i64* status) {
+    td3_chain_wait();
+    td3_chain_release();
+    __shared__ MixedWindow windows[NF_WARPS];
+    const int lane = threadIdx.x & 31;
+    MixedWindow& win = windows[threadIdx.x >> 5];
+    const i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    if (seg >= n_seg) return;
+    const i64 leaf = seg_leaf[seg];
+    const longlong2 er = seg_range[seg];
+    const i64 outp = seg_out[seg];
+    const i64 s0 = T.start[leaf];
+    const int count = (int)(T.end[leaf] - s0);
+    const LaneMap L(count, lane);
+    const double u = pair_unit(S.unit), inv_u = 1.0 / u;
+    const double cx = T.center[2 * leaf], cy = T.center[2 * leaf + 1];
+    const float eps2f = (float)(eps2 * inv_u * inv_u);
+    const i64 n = S.n;
+    auto stage = [&](int p, i64 j) {
+        const float2 x = split_rel(S.pos[j], cx, inv_u), y = split_rel(S.pos[n + j], cy, inv_u);
+        win.pos[p] = make_float4(x.x, x.y, y.x, y.y);
+        const double q = S.charge[j];
+        win.q[p] = q;
+        win.qf[p] = (float)q;
+        win.tag[p] = (int)j;
+    };
+    for (int base = 0; base < count; base += L.tsz) {
+        const int it = base + L.ti;
+        const bool valid = L.slice < L.slices && it < count;
+        const i64 k = s0 + (valid ? it : 0);
+        const float2 X = split_rel(S.pos[k], cx, inv_u), Y = split_rel(S.pos[n + k], cy, inv_u);
+        const bool qi_nonzero = S.charge[k] != 0.0;
+        const int self = (int)k;
+        KahanF kp, kx, ky;
+        double qsum = 0.0;
+        bool bad = false;
+        for_source_windows<NM_CAP>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
+            if (!valid) return;
+            const int step = L.slices;
+            for (int p0 = L.slice; p0 < wn; p0 += NF_BLOCK * step) {
+                float bp = 0.0f, bx = 0.0f, by = 0.0f;
+                const int p1 = p0 + NF_BLOCK * step < wn ? p0 + NF_BLOCK * step : wn;
+                for (int p = p0; p < p1; p += step) {
+                    if (win.tag[p] == self) continue;
+                    const float4 src = win.pos[p];
+                    const float dx = (X.x - src.x) + (X.y - src.y);
+                    const float dy = (Y.x - src.z) + (Y.y - src.w);
+                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, eps2f));
+                    if (r2 == 0.0f) {  // coincident, unsoftened
+                        bad |= qi_nonzero && win.q[p] != 0.0;
+                        continue;
+                    }
+                    const float qj = win.qf[p];
+                    if (KERNEL == TD3_KERNEL_LOG) {
+                        if (POT) {
+                            bp = fmaf(-qj, __logf(r2), bp);
+                            qsum += win.q[p];
+                        }
+                        const float f = __fdividef(2.0f * qj, r2);
+                        bx = fmaf(f, dx, bx);
+                        by = fmaf(f, dy, by);
+                    } else {
+                        const float ir = rsqrtf(r2), qr = qj * ir, qr3 = qr * ir * ir;
+                        bp += qr;
+                        bx = fmaf(qr3, dx, bx);
+                        by = fmaf(qr3, dy, by);
+                    }
+                }
+                if (POT || KERNEL != TD3_KERNEL_LOG) kp.add(bp);
+                kx.add(bx);
+                ky.add(by);
+            }
+        });
+        // back from units of u: log -ln u^2 sum q, 1/u; Coulomb 1/u, 1/u^2
+        double v[3];
+        if (KERNEL == TD3_KERNEL_LOG) {
+            v[0] = kp.value() - 2.0 * log(u) * qsum;
+            v[1] = kx.value() * inv_u;
+            v[2] = ky.value() * inv_u;
+        } else {
+            v[0] = kp.value() * inv_u;
+            v[1] = kx.value() * inv_u * inv_u;
+            v[2] = ky.value() * inv_u * inv_u;
+        }
+        L.sum_slices(v);
+        const unsigned badmask = __ballot_sync(0xffffffffu, bad && valid);
+        if (valid && L.slice == 0) {
+            if (outp < 0) {
+                const i64 i = T.perm[k];
+                if (POT) phi[i] += v[0];
+                field[i] += v[1];
+                field[T.m + i] += v[2];
+            } else {
+                const i64 p = outp + it;
+                partial[3 * p] = v[0];
+                partial[3 * p + 1] = v[1];
+                partial[3 * p + 2] = v[2];
+            }
+        }
+        if (badmask && lane == __ffs(badmask) - 1) td3_report(status, T.perm[k] + 1);
+    }
+}
+
+constexpr int NM_CAP_ADJ = 128;  // staged sources per warp window (mixed adjoint)
+
+struct MixedAdjointWindow {
+    float4 pos[NM_CAP_ADJ];  // as MixedWindow
+    float4 qwe[NM_CAP_ADJ];  // (q, w, e_x / u, e_y / u)
+    double w[NM_CAP_ADJ];    // the monopole in FP64 (its ln u^2 sum)
+    int tag[NM_CAP_ADJ];
+};
+
+template <int KERNEL>
+__global__ void __launch_bounds__(32 * NF_WARPS, 8)
+k_near_adjoint_mixed(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
+                     const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
+                     const i64* __restrict__ partners, double eps2, double* __restrict__ partial) {
+    td3_chain_wait();
+    td3_chain_release();
+    __shared__ MixedAdjointWindow windows[NF_WARPS];
+    const int lane = threadIdx.x & 31;
+    MixedAdjointWindow& win = windows[threadIdx.x >> 5];
+    const i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    if (seg >= n_seg) return;
+    const i64 leaf = seg_leaf[seg];
+    const longlong2 er = seg_range[seg];
+    const i64 outp = seg_out[seg];
+    const i64 s0 = T.start[leaf];
+    const int count = (int)(T.end[leaf] - s0);
+    const LaneMap L(count, lane);
+    const i64 n = S.n;
+    const double u = pair_unit(S.unit), inv_u = 1.0 / u;
+    const double cx = T.center[2 * leaf], cy = T.center[2 * leaf + 1];
+    const float eps2f = (float)(eps2 * inv_u * inv_u);
+    auto stage = [&](int p, i64 j) {
+        const float2 x = split_rel(S.pos[j], cx, inv_u), y = split_rel(S.pos[n + j], cy, inv_u);
+        win.pos[p] = make_float4(x.x, x.y, y.x, y.y);
+        const double w = A.weight[j];
+        win.qwe[p] = make_float4((float)S.charge[j], (float)w, (float)(A.dipole[j] * inv_u),
+                                 (float)(A.dipole[n + j] * inv_u));
+        win.w[p] = w;
+        win.tag[p] = (int)j;
+    };
+    for (int base = 0; base < count; base += L.tsz) {
+        const int it = base + L.ti;
+        const bool valid = L.slice < L.slices && it < count;
+        const i64 k = s0 + (valid ? it : 0);
+        const float2 X = split_rel(S.pos[k], cx, inv_u), Y = split_rel(S.pos[n + k], cy, inv_u);
+        const int self = (int)k;
+        KahanF kacc[6];
+        double wsum = 0.0;
+        for_source_windows<NM_CAP_ADJ>(S, partners, er.x, er.y, lane, stage, [&](int wn) {
+            if (!valid) return;
+            const int step = L.slices;
+            for (int p0 = L.slice; p0 < wn; p0 += NF_BLOCK * step) {
+                float blk[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+                const int p1 = p0 + NF_BLOCK * step < wn ? p0 + NF_BLOCK * step : wn;
+                for (int p = p0; p < p1; p += step) {
+                    if (win.tag[p] == self) continue;
+                    const float4 src = win.pos[p];
+                    const float dx = (X.x - src.x) + (X.y - src.y);
+                    const float dy = (Y.x - src.z) + (Y.y - src.w);
+                    if (eps2f == 0.0f && dx == 0.0f && dy == 0.0f) continue;  // coincident
+                    const float4 c = win.qwe[p];
+                    if (KERNEL == TD3_KERNEL_LOG) wsum += win.w[p];
+                    adjoint_pair_mixed<KERNEL>(dx, dy, eps2f, c.x, c.y, c.z, c.w, blk);
+                }
+#pragma unroll
+                for (int c = 0; c < 6; ++c) kacc[c].add(blk[c]);
+            }
+        });
+        // back from units of u: the log kernel's sums scale as (1, 1/u, 1/u^2) plus
+        // -ln u^2 sum w for Psi, the Coulomb kernel's as (1/u, 1/u^2, 1/u^3)
+        const double sc = KERNEL == TD3_KERNEL_LOG ? 1.0 : inv_u;
+        double acc[6];
+        acc[0] = kacc[0].value() * sc;
+        if (KERNEL == TD3_KERNEL_LOG) acc[0] -= 2.0 * log(u) * wsum;
+        for (int c = 1; c < 3; ++c) acc[c] = kacc[c].value() * (sc * inv_u);
+        for (int c = 3; c < 6; ++c) acc[c] = kacc[c].value() * (sc * inv_u * inv_u);
+        L.sum_slices(acc);
+        if (valid && L.slice == 0) {
+            if (outp < 0) {
+                adjoint_add(acc, k, T.perm[k], n, S, A);
+            } else {
+                const i64 p = outp + it;
+                for (int c = 0; c < 6; ++c) partial[6 * p + c] = acc[c];
+            }
         }
     }
 }
@@ -811,7 +1177,7 @@ int launch_near(const NearArgs& a, cudaStream_t s) {
                                s, a.T, a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out,
                                a.partners, a.la, a.lb, a.order, a.width, a.eps2, a.partial, a.phi,
                                a.field, a.status));
-    TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL>, blocks, 32 * NF_WARPS, 0, s, a.T,
+    TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL>, td3_finish_blocks(a.n_seg), 32 * NF_WARPS, 0, s, a.T,
                                a.n_seg, a.seg_leaf, a.seg_out, a.la, a.lb, a.order, a.width,
                                a.partial, a.phi, a.field));
     TD3_CHECK_LAUNCH();
@@ -913,7 +1279,7 @@ int launch_adjoint(const Targets& T, const Sources& S, const Adjoint& A, i64 n_s
     TD3_TRY(td3_launch_chained(k_near_adjoint<KERNEL, LOCAL, MIXED>, blocks, 32 * NF_WARPS, 0, s,
                                T, S, A, n_seg, seg_leaf, sr, seg_out, partners, fa, fb, ba, bb,
                                order, width, eps2, partial));
-    TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL>, blocks, 32 * NF_WARPS, 0, s, T, S,
+    TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL>, td3_finish_blocks(n_seg), 32 * NF_WARPS, 0, s, T, S,
                                A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb, order, width,
                                partial));
     return TD3_OK;
@@ -986,4 +1352,117 @@ extern "C" int td3_fmm_targets(int kernel, const double* sorted_targets,
     cudaStream_t s = td3_stream(stream);
     if (lg) return dispatch_near<true, LOCAL_COMPLEX>(kernel, with_potential, mixed, a, s);
     return dispatch_near<true, LOCAL_CART>(kernel, with_potential, mixed, a, s);
+}
+
+extern "C" int td3_slot_leaves(int64_t n_nodes, const int64_t* node_child,
+                               const int64_t* node_start, const int64_t* node_end,
+                               int32_t* slot_leaf, void* stream) {
+    if (n_nodes < 1 || n_nodes > 0x7fffffffLL) return TD3_EINVAL;
+    TD3_TRY(td3_launch_chained(k_slot_leaves, td3_blocks(n_nodes, 256), 256, 0,
+                               td3_stream(stream), n_nodes, node_child, node_start, node_end,
+                               slot_leaf));
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+namespace {
+
+template <int KERNEL, bool POT, int LOCAL>
+int launch_near_mixed(const NearArgs& a, const int* slot_leaf, cudaStream_t s) {
+    TD3_TRY(td3_launch_chained(k_far_field<LOCAL, POT>, td3_blocks(a.T.m, 256), 256, 0, s, a.T,
+                               slot_leaf, a.la, a.lb, a.order, a.width, a.phi, a.field));
+    if (a.n_seg > 0) {
+        const unsigned blocks = td3_blocks(a.n_seg, NF_WARPS);
+        TD3_TRY(td3_launch_chained(k_near_mixed<KERNEL, POT>, blocks, 32 * NF_WARPS, 0, s, a.T,
+                                   a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out, a.partners,
+                                   a.eps2, a.partial, a.phi, a.field, a.status));
+        TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL, true>, td3_finish_blocks(a.n_seg), 32 * NF_WARPS, 0, s,
+                                   a.T, a.n_seg, a.seg_leaf, a.seg_out, a.la, a.lb, a.order,
+                                   a.width, a.partial, a.phi, a.field));
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+template <int KERNEL, int LOCAL>
+int launch_adjoint_mixed(const Targets& T, const Sources& S, const Adjoint& A,
+                         const int* slot_leaf, i64 n_seg, const int* seg_leaf,
+                         const longlong2* sr, const i64* seg_out, const i64* partners,
+                         const double* fa, const double* fb, const double* ba, const double* bb,
+                         int order, int width, double eps2, double* partial, cudaStream_t s) {
+    TD3_TRY(td3_launch_chained(k_far_adjoint<LOCAL>, td3_blocks(T.m, 256), 256, 0, s, T, S, A,
+                               slot_leaf, fa, fb, ba, bb, order, width));
+    if (n_seg > 0) {
+        const unsigned blocks = td3_blocks(n_seg, NF_WARPS);
+        TD3_TRY(td3_launch_chained(k_near_adjoint_mixed<KERNEL>, blocks, 32 * NF_WARPS, 0, s, T,
+                                   S, A, n_seg, seg_leaf, sr, seg_out, partners, eps2, partial));
+        TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL, true>, td3_finish_blocks(n_seg), 32 * NF_WARPS, 0,
+                                   s, T, S, A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb, order,
+                                   width, partial));
+    }
+    TD3_CHECK_LAUNCH();
+    return TD3_OK;
+}
+
+}  // namespace
+
+extern "C" int td3_fmm_evaluate_mixed(int kernel, const double* sorted_pos,
+                                      const double* sorted_charge, const int64_t* perm, int64_t n,
+                                      const double* node_center, const int64_t* node_start,
+                                      const int64_t* node_end, int order, const double* local_a,
+                                      const double* local_b, const int32_t* slot_leaf,
+                                      const int64_t* p2p_partners, const int* seg_leaf,
+                                      const int64_t* seg_range, const int64_t* seg_out,
+                                      int64_t n_seg, double* partial, double softening,
+                                      int with_potential, double unit, double* phi,
+                                      double* field, int64_t* status, void* stream) {
+    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (!(unit > 0.0 && unit < INFINITY) || !slot_leaf) return TD3_EINVAL;
+    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
+    if (n == 0) return TD3_OK;
+    const bool lg = kernel == TD3_KERNEL_LOG;
+    NearArgs a{Targets{sorted_pos, nullptr, perm, node_center, node_start, node_end, n},
+               Sources{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit},
+               n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
+               p2p_partners, local_a, local_b, order,
+               lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,
+               phi, field, status};
+    cudaStream_t s = td3_stream(stream);
+    constexpr int LG = TD3_KERNEL_LOG, CL = TD3_KERNEL_COULOMB;
+    if (lg)
+        return with_potential ? launch_near_mixed<LG, true, LOCAL_COMPLEX>(a, slot_leaf, s)
+                              : launch_near_mixed<LG, false, LOCAL_COMPLEX>(a, slot_leaf, s);
+    return with_potential ? launch_near_mixed<CL, true, LOCAL_CART>(a, slot_leaf, s)
+                          : launch_near_mixed<CL, false, LOCAL_CART>(a, slot_leaf, s);
+}
+
+extern "C" int td3_fmm_adjoint_mixed(int kernel, const double* sorted_pos,
+                                     const double* sorted_charge, const int64_t* perm, int64_t n,
+                                     const double* node_center, const int64_t* node_start,
+                                     const int64_t* node_end, int order, const double* fwd_a,
+                                     const double* fwd_b, const double* adj_a,
+                                     const double* adj_b, const int32_t* slot_leaf,
+                                     const int64_t* p2p_partners, const int* seg_leaf,
+                                     const int64_t* seg_range, const int64_t* seg_out,
+                                     int64_t n_seg, double* partial, const double* sorted_weight,
+                                     const double* sorted_dipole, const double* efield,
+                                     double softening, double unit, double* qbar, double* xbar,
+                                     void* stream) {
+    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (!(unit > 0.0 && unit < INFINITY) || !slot_leaf) return TD3_EINVAL;
+    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
+    if (n == 0) return TD3_OK;
+    Targets T{sorted_pos, nullptr, perm, node_center, node_start, node_end, n};
+    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit};
+    Adjoint A{sorted_weight, sorted_dipole, efield, qbar, xbar};
+    const double eps2 = softening * softening;
+    cudaStream_t s = td3_stream(stream);
+    const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
+    if (kernel == TD3_KERNEL_LOG)
+        return launch_adjoint_mixed<TD3_KERNEL_LOG, LOCAL_COMPLEX>(
+            T, S, A, slot_leaf, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a,
+            adj_b, order, order + 1, eps2, partial, s);
+    return launch_adjoint_mixed<TD3_KERNEL_COULOMB, LOCAL_CART>(
+        T, S, A, slot_leaf, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b,
+        order, (order + 1) * (order + 2) / 2, eps2, partial, s);
 }

@@ -176,6 +176,11 @@ def _m2l_coefficients(order: int, symmetric: bool) -> np.ndarray:
 #: partners per near-field work segment (one warp each)
 NEAR_SEGMENT = 256
 
+#: the mixed-precision near field at the sources in three launches (td3_fmm_evaluate_mixed,
+#: td3_fmm_adjoint_mixed: far field per particle, FP32 hi + lo pair arithmetic) instead of
+#: the one-launch form of td3_fmm_evaluate / td3_fmm_adjoint with mixed = 1.
+NEAR_SPLIT = True
+
 #: mixed-precision M2L matrix products on the tensor cores (tcgen05, 3xTF32; orders up
 #: to 15) instead of FP32 CUDA-core arithmetic.  Off by default: the tensor-core form is
 #: correct but, waiting on each 128-row tile, still slower than the CUDA-core form.
@@ -816,11 +821,34 @@ class FlatQuadtree:
                   binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
                   _lib.stream(self.device))
 
+    def _slot_leaves(self) -> torch.Tensor:
+        """The leaf of every particle slot (td3_slot_leaves), kept with the tree."""
+        if getattr(self, "_slot_leaf", None) is None:
+            n = self.pos.shape[1]
+            self._slot_leaf = torch.empty(max(n, 1), dtype=torch.int32, device=self.device)
+            _lib.call("td3_slot_leaves", self.node_count, self.node_child.data_ptr(),
+                      self.node_start.data_ptr(), self.node_end.data_ptr(),
+                      self._slot_leaf.data_ptr(), _lib.stream(self.device))
+        return self._slot_leaf
+
     def _evaluate_near(self, lists, kernel, local_a, local_b, softening, potential, phi, field,
                        status):
-        """L2P + P2P at the sources (td3_fmm_evaluate) over the near-field plan."""
+        """L2P + P2P at the sources (td3_fmm_evaluate) over the near-field plan; the
+        mixed form as td3_fmm_evaluate_mixed (NEAR_SPLIT)."""
         plan = lists["plan"]
         n = self.pos.shape[1]
+        if self._mixed and NEAR_SPLIT:
+            _lib.call(
+                "td3_fmm_evaluate_mixed", kernel, self._sorted_pos.data_ptr(),
+                self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
+                self.node_center.data_ptr(), self.node_start.data_ptr(),
+                self.node_end.data_ptr(), self.order, local_a.data_ptr(), local_b.data_ptr(),
+                self._slot_leaves().data_ptr(), lists["p2p_partners"].data_ptr(),
+                plan["seg_leaf"].data_ptr(), plan["seg_range"].data_ptr(),
+                plan["seg_out"].data_ptr(), plan["n_seg"], plan["partial"].data_ptr(),
+                float(softening), 1 if potential else 0, self._unit, phi.data_ptr(),
+                field.data_ptr(), status.data_ptr(), _lib.stream(self.device))
+            return
         _lib.call(
             "td3_fmm_evaluate", kernel, self._sorted_pos.data_ptr(),
             self._sorted_charge.data_ptr(), self.perm.data_ptr(), n, self.node_center.data_ptr(),
@@ -887,10 +915,9 @@ class FlatQuadtree:
         stream = _lib.stream(self.device)
         mre, mim = moments
         if self.precision == "mixed" and self.order <= 20:
-            hat = self._scaled_moments(moments)
             groups = lists.get("groups") if dst is self else None
             if groups is not None:
-                self._m2l_grouped(groups, hat, local_re, local_im)
+                self._m2l_grouped(groups, self._scaled_moments(moments), local_re, local_im)
                 return
             rows, partners = lists["m2l_rows"], lists["m2l_partners"]
             coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
@@ -902,6 +929,7 @@ class FlatQuadtree:
                           records.data_ptr(), self.order, coeff.ctypes.data, self._unit,
                           local_re.data_ptr(), local_im.data_ptr(), stream)
                 return
+            hat = self._scaled_moments(moments)
             _lib.call("td3_fmm_m2l_mixed", rows.data_ptr(), lists["m2l_entry_row"].data_ptr(),
                       partners.data_ptr(), dst.node_count,
                       dst.node_center.data_ptr(), dst.node_half.data_ptr(),
@@ -967,6 +995,18 @@ class FlatQuadtree:
         partial = torch.empty(6 * max(plan["partial_len"], 1), dtype=torch.float64, device=dev)
         qbar = torch.zeros(n, dtype=torch.float64, device=dev)
         xbar = torch.zeros((2, n), dtype=torch.float64, device=dev)
+        if self._mixed and NEAR_SPLIT:
+            _lib.call("td3_fmm_adjoint_mixed", kernel, self._sorted_pos.data_ptr(),
+                      self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
+                      self.node_center.data_ptr(), self.node_start.data_ptr(),
+                      self.node_end.data_ptr(), self.order, fwd_a.data_ptr(), fwd_b.data_ptr(),
+                      adj_a.data_ptr(), adj_b.data_ptr(), self._slot_leaves().data_ptr(),
+                      lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
+                      plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
+                      partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), efield.data_ptr(),
+                      float(softening), self._unit, qbar.data_ptr(), xbar.data_ptr(), stream)
+            self._check_tensor_cores()
+            return qbar, xbar
         _lib.call("td3_fmm_adjoint", kernel, self._sorted_pos.data_ptr(),
                   self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
                   self.node_center.data_ptr(), self.node_start.data_ptr(), self.node_end.data_ptr(),
