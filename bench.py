@@ -553,9 +553,9 @@ def run_ours(args):
         "peak_source": ("nominal FP32 FMA rate at the max SM clock (148 SM x 128 lanes x 2 x "
                         "1965 MHz); MEASURED_PEAKS.json has no FP32 CUDA-core figure"),
         "algorithmic": "8 (p + 1)^2 flop per directed translation (the reference's count)",
-        # dram read + write of one ncu capture of this kernel at 300k particles (86.4 MB
+        # dram read + write of one ncu capture of this kernel at 300k particles (72.8 MB
         # for 3.745M translations), scaled by the translations of this launch
-        "traffic": 86.4e6 * (2 * n_m2l) / 3.745e6,
+        "traffic": 72.8e6 * (2 * n_m2l) / 3.745e6,
         "traffic_unit": "bytes per launch (scaled from a 300k-particle ncu capture)",
         "ms_per_launch": m2l_ms,
         "flop_per_launch": flops,
