@@ -501,7 +501,9 @@ int td3_fmm_evaluate(int kernel, const double* sorted_pos, const double* sorted_
  * (hi_i - hi_j) + (lo_i - lo_j); compensated sums as td3_fmm_evaluate.  slot_leaf is
  * required.  Replaces fmm_evaluate_host (src/tree_d_3d/kernels/fmm_evaluate_host/
  * fmm_evaluate_host_pyccel.py:14-100) and cart_evaluate_host (kernels/cart_evaluate_host/
- * cart_evaluate_host_pyccel.py:16-110) in FP32. */
+ * cart_evaluate_host_pyccel.py:16-110) in FP32.  slot_leaf[k] = -1 leaves slot k out of
+ * the far field (its outputs untouched), as the plan's emptied leaves leave it out of the
+ * pair sums: one rank's share of the leaves. */
 int td3_slot_leaves(int64_t n_nodes, const int64_t* node_child, const int64_t* node_start,
                     const int64_t* node_end, int32_t* slot_leaf, void* stream);
 int td3_fmm_evaluate_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,

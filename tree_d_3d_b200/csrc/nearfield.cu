@@ -891,6 +891,7 @@ __global__ void k_far_field(Targets T, const int* __restrict__ slot_leaf,
     const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= T.m) return;
     const i64 leaf = slot_leaf[k];
+    if (leaf < 0) return;  // a slot left out (another rank's leaf)
     double lp, lx, ly;
     eval_local<LOCAL>(la, lb, leaf, order, width, T.pos[k] - T.center[2 * leaf],
                       T.pos[T.m + k] - T.center[2 * leaf + 1], lp, lx, ly);
@@ -911,6 +912,7 @@ __global__ void k_far_adjoint(Targets T, Sources S, Adjoint A, const int* __rest
     if (k >= T.m) return;
     const double zero[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     const i64 leaf = slot_leaf[k];
+    if (leaf < 0) return;
     adjoint_finish<LOCAL>(zero, k, T.perm[k], S.n, T.pos[k] - T.center[2 * leaf],
                           T.pos[T.m + k] - T.center[2 * leaf + 1], leaf, order, width, fa, fb,
                           ba, bb, S, A);

@@ -843,7 +843,8 @@ class FlatQuadtree:
                 self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
                 self.node_center.data_ptr(), self.node_start.data_ptr(),
                 self.node_end.data_ptr(), self.order, local_a.data_ptr(), local_b.data_ptr(),
-                self._slot_leaves().data_ptr(), lists["p2p_partners"].data_ptr(),
+                lists.get("slot_leaf", self._slot_leaves()).data_ptr(),
+                lists["p2p_partners"].data_ptr(),
                 plan["seg_leaf"].data_ptr(), plan["seg_range"].data_ptr(),
                 plan["seg_out"].data_ptr(), plan["n_seg"], plan["partial"].data_ptr(),
                 float(softening), 1 if potential else 0, self._unit, phi.data_ptr(),
@@ -1217,6 +1218,11 @@ class FlatQuadtree:
             end = torch.where(inside, self.node_end, self.node_start).contiguous()
             part["p2p"] = lists["p2p"]
             part["p2p_partners"] = lists["p2p_partners"]
+            if self.precision == "mixed":
+                # the far field of this share's leaves only (-1: another rank's slot)
+                slot = self._slot_leaves()
+                keep = (slot >= leaves.start) & (slot < leaves.stop)
+                part["slot_leaf"] = torch.where(keep, slot, torch.full_like(slot, -1))
             part["plan"] = _nearfield_plan(lists["p2p_rows"], self, 2 * lists["p2p"].shape[0],
                                            end=end)
             part["pairs"], part["leaves"] = pairs, leaves
