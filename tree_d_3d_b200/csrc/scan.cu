@@ -190,14 +190,17 @@ k_sort_hist(const unsigned* __restrict__ keys, i64 n, int shift, unsigned mask, 
     __syncthreads();
     int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     i64 base = (i64)blockIdx.x * SORT_TILE + (i64)wib * WARP_ITEMS;
-#pragma unroll 4
+    // the warp's items loaded first, then counted with shared-memory atomics into the
+    // warp's own counts (lanes that meet on a digit are serialised by the hardware)
+    unsigned dig[SORT_ITEMS];
+#pragma unroll
     for (int r = 0; r < SORT_ITEMS; ++r) {
         i64 k = base + r * 32 + lane;
-        bool live = k < n;
-        unsigned d = live ? (keys[k] >> shift) & mask : RADIX;
-        unsigned peers = __match_any_sync(0xffffffffu, d);
-        if (live && (peers & lanes_below()) == 0) atomicAdd(&counts[wib][d], __popc(peers));
+        dig[r] = k < n ? (keys[k] >> shift) & mask : RADIX;
     }
+#pragma unroll
+    for (int r = 0; r < SORT_ITEMS; ++r)
+        if (dig[r] < RADIX) atomicAdd(&counts[wib][dig[r]], 1);
     __syncthreads();
     int d = threadIdx.x, sum = 0;
 #pragma unroll
