@@ -9,12 +9,12 @@
 // Work: a warp owns a run of whole destination rows (an even share of the entries).
 // Its four 8-lane groups take the rows in order, each row whole: lane i of a group
 // translates entries i, i + 8, ... of the row and adds the contributions into its own
-// FP32 registers (the output products fold into the sums, no staging per entry); at the
-// row's end the group's 8 partial rows pass through shared memory and lane i sums
-// columns i, i + 8, ... over them pairwise, then adds them to the FP64 locals.  Rows
-// longer than LONG_ROW entries are taken by the whole warp first (32 partial rows),
-// so no group holds a warp for long.  Every destination is summed by one group in a
-// fixed order: deterministic results.
+// FP32 sums, kept in shared memory (a warp's sums column-major with a 33-word stride: a
+// column's accesses hit 32 banks, freeing registers for more resident warps); at the
+// row's end lane i sums columns i, i + 8, ... over the group's 8 lanes pairwise and adds
+// them to the FP64 locals.  Rows longer than LONG_ROW entries are taken by the whole
+// warp first (32 partial rows), so no group holds a warp for long.  Every destination
+// is summed by one group in a fixed order: deterministic results.
 #include "common.cuh"
 
 namespace {
@@ -92,10 +92,10 @@ __device__ __forceinline__ void load_record(const float4* __restrict__ rec, i64 
 
 // One translation from the source whose record is `m` into this lane's sums `acc`
 // (columns 2l, 2l + 1: bhat_l in units of the destination size; 2W, 2W + 1: a_0).
-template <int P>
+template <int P, class Acc>
 __device__ __forceinline__ void translate(const float4 (&m)[rec_words<P>()], double cx, double cy,
                                           float fhd, double inv_unit, const RowCoef<P>& C,
-                                          float (&acc)[2 * P + 4]) {
+                                          Acc& acc) {
     constexpr int W = P + 1, F4 = rec_words<P>();
     const double2 c = *reinterpret_cast<const double2*>(&m[0]);
     float hr[W + 1], hi[W + 1];
@@ -153,16 +153,22 @@ __device__ __forceinline__ void translate(const float4 (&m)[rec_words<P>()], dou
     acc[2 * W + 1] += ai[0];
 }
 
-// Sum of column c over the n = 8 * G partial rows of `park` (rows of group g at
-// g * gstride + i * V), pairwise in a fixed order.
-template <int V, int G>
-__device__ __forceinline__ float column_sum(const float* park, int gstride, int c) {
+// A lane's partial sums in shared memory: column c of lane L at c * 33 + L (a warp's
+// accesses of one column hit 32 banks; a group's 8 lanes of a column are contiguous).
+struct SmemAcc {
+    float* base;  // the warp's array plus the lane
+    __device__ __forceinline__ float& operator[](int c) const { return base[c * 33]; }
+};
+
+// Sum of column c over the lanes [8 g0, 8 g0 + 8 G) of a warp's SmemAcc array, pairwise
+// in a fixed order.
+template <int G>
+__device__ __forceinline__ float smem_column_sum(const float* a, int c, int g0) {
     float gs[G];
 #pragma unroll
     for (int g = 0; g < G; ++g) {
-        const float* p = park + g * gstride + c;
-        gs[g] = ((p[0] + p[V]) + (p[2 * V] + p[3 * V])) +
-                ((p[4 * V] + p[5 * V]) + (p[6 * V] + p[7 * V]));
+        const float* p = a + c * 33 + 8 * (g0 + g);
+        gs[g] = ((p[0] + p[1]) + (p[2] + p[3])) + ((p[4] + p[5]) + (p[6] + p[7]));
     }
     if (G == 1) return gs[0];
     return (gs[0] + gs[G > 1 ? 1 : 0]) + (gs[G > 2 ? 2 : 0] + gs[G > 3 ? 3 : 0]);
@@ -176,15 +182,12 @@ k_m2l_mixed_rows(const i64* __restrict__ row_start, const i64* __restrict__ part
                  double* __restrict__ local_re, double* __restrict__ local_im) {
     td3_chain_wait();
     td3_chain_release();
-    constexpr int W = P + 1, V = 2 * W + 2, GSTRIDE = GL * V + 8;
-    static_assert(V % 4 == 0, "partial rows of whole float4s");
-    __shared__ __align__(16) float park[RW][4 * GSTRIDE];
+    constexpr int W = P + 1, V = 2 * W + 2;
+    __shared__ float accs[RW][V * 33];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, g = lane >> 3, gl = lane & 7;
-    float* wpark = park[wib];
+    float* wacc = accs[wib];
     const int w = order + 1;
     const double inv_unit = 1.0 / unit, ln_unit = log(unit);
-
-    // this warp's rows [da, db): the rows whose first entry lies in its even share
     const i64 gw = (i64)blockIdx.x * RW + wib, nw = (i64)gridDim.x * RW;
     const i64 total = row_start[n_dst], share = (total + nw - 1) / nw;
     auto first_row_at = [&](i64 e) {
@@ -199,11 +202,10 @@ k_m2l_mixed_rows(const i64* __restrict__ row_start, const i64* __restrict__ part
     const i64 da = first_row_at(gw * share);
     const i64 db = gw + 1 == nw ? n_dst : first_row_at((gw + 1) * share);
     if (da >= db) return;
-
-    float acc[V];
+    // this lane's partial sums (shared memory, 72 registers per thread instead of 96)
+    SmemAcc acc{wacc + lane};
 #pragma unroll
-    for (int j = 0; j < V; ++j) acc[j] = 0.0f;
-    float* mine = wpark + g * GSTRIDE + gl * V;
+    for (int c = 0; c < V; ++c) acc[c] = 0.0f;
 
     // 1. rows longer than LONG_ROW: the whole warp, 32 entries per round
     for (i64 base = da; base < db; base += 32) {
@@ -221,22 +223,19 @@ k_m2l_mixed_rows(const i64* __restrict__ row_start, const i64* __restrict__ part
                 load_record<P>(rec, partners[e], m);
                 translate<P>(m, cx, cy, fhd, inv_unit, C, acc);
             }
-#pragma unroll
-            for (int c = 0; c < V / 4; ++c) {
-                reinterpret_cast<float4*>(mine)[c] =
-                    make_float4(acc[4 * c], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
-                acc[4 * c] = acc[4 * c + 1] = acc[4 * c + 2] = acc[4 * c + 3] = 0.0f;
-            }
             __syncwarp();
             if (lane < 2 * W && (lane >> 1) < w) {
                 const int l = lane >> 1;
-                double s = 1.0;
+                double sc = 1.0;
                 const double inv_h = 1.0 / hd;
-                for (int i = 0; i < l; ++i) s *= inv_h;
-                double add = (double)column_sum<V, 4>(wpark, GSTRIDE, lane) * s;
-                if (lane < 2) add += ln_unit * (double)column_sum<V, 4>(wpark, GSTRIDE, 2 * W + lane);
+                for (int i = 0; i < l; ++i) sc *= inv_h;
+                double add = (double)smem_column_sum<4>(wacc, lane, 0) * sc;
+                if (lane < 2) add += ln_unit * (double)smem_column_sum<4>(wacc, 2 * W + lane, 0);
                 ((lane & 1) ? local_im : local_re)[d * w + l] += add;
             }
+            __syncwarp();
+#pragma unroll
+            for (int c = 0; c < V; ++c) acc[c] = 0.0f;
             __syncwarp();
         }
     }
@@ -270,35 +269,28 @@ k_m2l_mixed_rows(const i64* __restrict__ row_start, const i64* __restrict__ part
         const bool done = d >= 0 && cur >= end;
         const unsigned dm = __ballot_sync(FULL, done);
         if (!dm) continue;
-        if (done && had) {
-#pragma unroll
-            for (int c = 0; c < V / 4; ++c)
-                reinterpret_cast<float4*>(mine)[c] =
-                    make_float4(acc[4 * c], acc[4 * c + 1], acc[4 * c + 2], acc[4 * c + 3]);
-        }
         __syncwarp();
         if (done && had) {
             // lane gl adds columns gl + 8 j (coefficient l = gl / 2 + 4 j) to the locals
             const double inv_h = 1.0 / dst_half[d];
-            double s = 1.0, h4 = inv_h * inv_h;
+            double sc = 1.0, h4 = inv_h * inv_h;
             h4 *= h4;
-            for (int i = 0; i < (gl >> 1); ++i) s *= inv_h;
-            const float* gp = wpark + g * GSTRIDE;
+            for (int i = 0; i < (gl >> 1); ++i) sc *= inv_h;
 #pragma unroll
             for (int j = 0; j < (2 * W + 7) / 8; ++j) {
                 const int c = gl + 8 * j, l = c >> 1;
                 if (c < 2 * W && l < w) {
-                    double add = (double)column_sum<V, 1>(gp, GSTRIDE, c) * s;
-                    if (c < 2) add += ln_unit * (double)column_sum<V, 1>(gp, GSTRIDE, 2 * W + c);
+                    double add = (double)smem_column_sum<1>(wacc, c, g) * sc;
+                    if (c < 2) add += ln_unit * (double)smem_column_sum<1>(wacc, 2 * W + c, g);
                     ((c & 1) ? local_im : local_re)[d * w + l] += add;
                 }
-                s *= h4;
+                sc *= h4;
             }
         }
         __syncwarp();
         if (done) {
 #pragma unroll
-            for (int j = 0; j < V; ++j) acc[j] = 0.0f;
+            for (int c = 0; c < V; ++c) acc[c] = 0.0f;
         }
         // the finished groups take the next rows, in group order
         const unsigned gm = dm & 0x01010101u;
