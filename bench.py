@@ -197,17 +197,62 @@ def run_reference(args):
 
 # ----------------------------------------------------------------------------- GPU arm
 class ClockSampler:
-    """nvidia-smi samples of SM clocks and throttle reasons while the timed region runs."""
+    """SM clocks and throttle reasons sampled while the timed region runs: NVML read every
+    5 ms from a thread (reads only; no setting is touched), or nvidia-smi every 200 ms
+    where NVML is not importable."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.rows = []
+
+    def _nvml_handle(self, nvml):
+        """This process's CUDA device in NVML, found by its PCI address (CUDA and NVML
+        may number the GPUs differently), else by index."""
+        try:
+            import torch
+
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return nvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return nvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _nvml_loop(self, nvml, handle):
+        bits = [nvml.nvmlClocksEventReasonHwSlowdown, nvml.nvmlClocksEventReasonHwThermalSlowdown,
+                nvml.nvmlClocksEventReasonSwThermalSlowdown, nvml.nvmlClocksEventReasonSwPowerCap]
+        top = nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM)
+        while not self.stop.is_set():
+            try:
+                sm = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                why = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                self.rows.append((float(sm), float(top),
+                                  ["Active" if why & b else "Not Active" for b in bits]))
+            except Exception:  # a failed read drops one sample
+                pass
+            self.stop.wait(0.005)
 
     def __enter__(self):
+        import threading
+
+        try:
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            handle = self._nvml_handle(nvml)
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nvml, handle),
+                                           daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
@@ -218,30 +263,32 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
-        self.lines = []
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
+            return False
         if self.proc is not None:
             time.sleep(0.25)
             self.proc.terminate()
             out, _ = self.proc.communicate(timeout=5)
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            for ln in out.splitlines():
+                parts = [p.strip() for p in ln.split(",")]
+                try:
+                    self.rows.append((float(parts[0]), float(parts[1]), parts[3:]))
+                except (ValueError, IndexError):
+                    continue
         return False
 
     def summary(self):
-        rows = []
-        for ln in getattr(self, "lines", []):
-            parts = [p.strip() for p in ln.split(",")]
-            try:
-                rows.append((float(parts[0]), float(parts[1]), parts[3:]))
-            except (ValueError, IndexError):
-                continue
+        rows = self.rows
         if not rows:
             return None
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for _, _, flags in rows for i, f in enumerate(flags)
-                          if i < len(names) and f.lower() == "active"})
+        reasons = sorted({self.NAMES[i] for _, _, flags in rows for i, f in enumerate(flags)
+                          if i < len(self.NAMES) and f.lower() == "active"})
         sm = sorted(r[0] for r in rows)
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[1] for r in rows),
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows),
+                "source": "nvml every 5 ms" if self.thread is not None else "nvidia-smi every 200 ms"}
 
 
 def max_over_ranks(value: float, dist, device) -> float:

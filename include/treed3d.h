@@ -516,6 +516,24 @@ int td3_fmm_evaluate_mixed(int kernel, const double* sorted_pos, const double* s
                            double unit, double* phi, double* field, int64_t* status,
                            void* stream);
 
+/* td3_fmm_evaluate_mixed in its two parts, for callers that overlap them with other work:
+ * td3_fmm_near_mixed WRITES the near field alone into phi and field (the pair sums, then
+ * the leaves with several segments; every slot of a planned leaf; it reads no expansion,
+ * so it can run on another stream while the M2M, M2L and L2L run), and
+ * td3_fmm_far_mixed then ADDS the local expansions at the slots whose slot_leaf is not
+ * -1.  td3_fmm_evaluate_mixed is the two in a row on one stream (the same bits). */
+int td3_fmm_near_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+                       const int64_t* perm, int64_t n, const double* node_center,
+                       const int64_t* node_start, const int64_t* node_end,
+                       const int64_t* p2p_partners, const int* seg_leaf, const int64_t* seg_range,
+                       const int64_t* seg_out, int64_t n_seg, double* partial, double softening,
+                       int with_potential, double unit, double* phi, double* field,
+                       int64_t* status, void* stream);
+int td3_fmm_far_mixed(int kernel, const double* sorted_pos, const int64_t* perm, int64_t n,
+                      const double* node_center, int order, const double* local_a,
+                      const double* local_b, const int32_t* slot_leaf, int with_potential,
+                      double* phi, double* field, void* stream);
+
 /* fmm_at: L2P at the m targets (sorted_targets (2, m) in target-tree order, target_perm
  * their input indices, sorted_exclude their excluded source index) plus exact sums over
  * the partner source leaves of each target leaf (the one-way P2P rows cut by
@@ -593,6 +611,24 @@ int td3_fmm_adjoint_mixed(int kernel, const double* sorted_pos, const double* so
                           double* partial, const double* sorted_weight,
                           const double* sorted_dipole, const double* efield, double softening,
                           double unit, double* qbar, double* xbar, void* stream);
+
+/* td3_fmm_adjoint_mixed in its two parts, as td3_fmm_near_mixed / td3_fmm_far_mixed:
+ * td3_fmm_adjoint_near_mixed WRITES the near parts of qbar and xbar (it reads no
+ * expansion), td3_fmm_adjoint_far_mixed then ADDS the far parts. */
+int td3_fmm_adjoint_near_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+                               const int64_t* perm, int64_t n, const double* node_center,
+                               const int64_t* node_start, const int64_t* node_end,
+                               const int64_t* p2p_partners, const int* seg_leaf,
+                               const int64_t* seg_range, const int64_t* seg_out, int64_t n_seg,
+                               double* partial, const double* sorted_weight,
+                               const double* sorted_dipole, double softening, double unit,
+                               double* qbar, double* xbar, void* stream);
+int td3_fmm_adjoint_far_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+                              const int64_t* perm, int64_t n, const double* node_center, int order,
+                              const double* fwd_a, const double* fwd_b, const double* adj_a,
+                              const double* adj_b, const int32_t* slot_leaf,
+                              const double* sorted_weight, const double* sorted_dipole,
+                              const double* efield, double* qbar, double* xbar, void* stream);
 
 /* ------------------------------------------------------------------ grounded strip */
 

@@ -1,7 +1,8 @@
-"""The mixed-precision near field at the sources in three launches (td3_fmm_evaluate_mixed
-and td3_fmm_adjoint_mixed: FP64 far field per particle, FP32 hi + lo pair arithmetic,
-partial sums of multi-segment leaves) against the one-launch mixed form and FP64, for
-the field, the potential and the backward, both kernels, softened or not."""
+"""The mixed-precision near field at the sources in two parts (td3_fmm_near_mixed /
+td3_fmm_far_mixed and the adjoint pair: FP32 hi + lo pair arithmetic and the partial sums
+of multi-segment leaves, then the FP64 far field per particle), the near part on a second
+stream or on the caller's, against the one-launch mixed form and FP64, for the field, the
+potential and the backward, both kernels, softened or not."""
 
 from __future__ import annotations
 
@@ -14,11 +15,12 @@ from conftest import relative
 pytestmark = pytest.mark.gpu
 
 
-def _run(pos, q, kernel, eps, precision, split, w, e):
+def _run(pos, q, kernel, eps, precision, split, w, e, overlap=True):
     from tree_d_3d_b200 import Quad, flat_tree
     from tree_d_3d_b200.autograd import fmm_field
 
     flat_tree.NEAR_SPLIT = split
+    flat_tree.NEAR_OVERLAP = overlap
     P = torch.tensor(pos, device="cuda", requires_grad=True)
     Q = torch.tensor(q, device="cuda", requires_grad=True)
     phi, field = fmm_field(P, Q, Quad(0, 0, 1), kernel=kernel, order=12, softening=eps,
@@ -35,16 +37,20 @@ def test_split_near_field_matches_one_launch_form_and_fp64(kernel, eps, segment,
     # segment 8: most leaves take several segments (the partial-sum path)
     monkeypatch.setattr(flat_tree, "NEAR_SEGMENT", segment)
     monkeypatch.setattr(flat_tree, "NEAR_SPLIT", True)
+    monkeypatch.setattr(flat_tree, "NEAR_OVERLAP", True)
     pos, q = synthetic.mixture8(60_000, seed=70)
     rng = np.random.default_rng(71)
     w = torch.tensor(rng.normal(size=pos.shape[1]), device="cuda")
     e = torch.tensor(rng.normal(size=pos.shape), device="cuda")
     split = _run(pos, q, kernel, eps, "mixed", True, w, e)
     again = _run(pos, q, kernel, eps, "mixed", True, w, e)
+    serial = _run(pos, q, kernel, eps, "mixed", True, w, e, overlap=False)
     one = _run(pos, q, kernel, eps, "mixed", False, w, e)
     fp64 = _run(pos, q, kernel, eps, "fp64", True, w, e)
-    for a, b, c, d in zip(split, again, one, fp64):
+    for a, b, s1, c, d in zip(split, again, serial, one, fp64):
         assert np.array_equal(a, b)  # fixed summation order
+        # the near part on its own stream gives the bits of the one-stream call
+        assert np.array_equal(a, s1)
         assert relative(a, c) < 1e-6
         assert relative(a, d) < 1e-6
 

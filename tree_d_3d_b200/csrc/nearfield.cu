@@ -465,7 +465,7 @@ __device__ __forceinline__ i64 leaf_segments(const int* __restrict__ seg_leaf, i
 }
 
 // One multi-segment leaf (its first segment `seg`): every target's partial sums over the
-// segments, then L2P (or, ADD, added to what k_far_field wrote).
+// segments, then L2P (or, ADD, written alone for k_far_field to complete).
 template <bool POT, int LOCAL, bool ADD>
 __device__ __forceinline__ void finish_leaf(Targets T, i64 n_seg, const int* __restrict__ seg_leaf,
                                             const i64* __restrict__ seg_out,
@@ -495,9 +495,9 @@ __device__ __forceinline__ void finish_leaf(Targets T, i64 n_seg, const int* __r
         }
         if (ADD && lane == (it & 31)) {
             const i64 i = T.perm[s0 + it];
-            if (POT) phi[i] += pot;
-            field[i] += ex;
-            field[T.m + i] += ey;
+            phi[i] = POT ? pot : 0.0;
+            field[i] = ex;
+            field[T.m + i] = ey;
         } else if (lane == (it & 31)) {
             i64 k = s0 + it;
             double xi = T.pos[k], yi = T.pos[T.m + k];
@@ -513,7 +513,7 @@ __device__ __forceinline__ void finish_leaf(Targets T, i64 n_seg, const int* __r
 }
 
 // Leaves whose row took several segments: partial sums in segment order, plus L2P (or,
-// ADD, added to the far field k_far_field wrote).  Launched over a fraction of the
+// ADD, the near sums alone, which k_far_field completes).  Launched over a fraction of the
 // segments' warps (td3_finish_blocks): most leaves have one segment.
 template <bool POT, int LOCAL, bool ADD = false>
 __global__ void k_near_finish(Targets T, i64 n_seg, const int* __restrict__ seg_leaf,
@@ -636,14 +636,24 @@ __device__ __forceinline__ void adjoint_combine(const double* acc, const LocalJe
     A.xbar[n + i] = -w * A.efield[n + i] + q * gy - (mxy * ex + myy * ey);
 }
 
-// The near part of qbar and xbar of slot k (input index i), added to the far part that
-// k_far_adjoint wrote (qbar and xbar are linear in the near sums acc).
+// The near part of qbar and xbar of slot k (input index i), written alone; k_far_adjoint
+// adds the far part (qbar and xbar are linear in the near sums acc).
 __device__ __forceinline__ void adjoint_add(const double* acc, i64 k, i64 i, i64 n,
                                             const Sources& S, const Adjoint& A) {
     const double q = S.charge[k], ex = A.dipole[k], ey = A.dipole[n + k];
-    A.qbar[i] += acc[0];
-    A.xbar[i] += q * acc[1] - (acc[3] * ex + acc[4] * ey);
-    A.xbar[n + i] += q * acc[2] - (acc[4] * ex + acc[5] * ey);
+    A.qbar[i] = acc[0];
+    A.xbar[i] = q * acc[1] - (acc[3] * ex + acc[4] * ey);
+    A.xbar[n + i] = q * acc[2] - (acc[4] * ex + acc[5] * ey);
+}
+
+// The far part of qbar and xbar of slot k (input index i) added to the near part: f the
+// forward local expansion's jet (its Hessian), b the adjoint one's (Psi, grad Psi).
+__device__ __forceinline__ void adjoint_far_add(const LocalJet& f, const LocalJet& b, i64 k, i64 i,
+                                                i64 n, const Sources& S, const Adjoint& A) {
+    const double q = S.charge[k], w = A.weight[k], ex = A.dipole[k], ey = A.dipole[n + k];
+    A.qbar[i] += b.v;
+    A.xbar[i] += -w * A.efield[i] + q * b.gx - (f.hxx * ex + f.hxy * ey);
+    A.xbar[n + i] += -w * A.efield[n + i] + q * b.gy - (f.hxy * ex + f.hyy * ey);
 }
 
 template <int LOCAL>
@@ -857,11 +867,13 @@ __global__ void k_near_adjoint_finish(Targets T, Sources S, Adjoint A, i64 n_seg
 }
 
 // ------------------------------------------------------------------ mixed form at the sources
-// The mixed-precision near field at the sources in three launches: the far field of every
-// particle in FP64, one thread per slot (k_far_field / k_far_adjoint: every lane busy,
-// where a segment's warp would run it on one lane per target), then the pair sums,
-// added to it (k_near_mixed / k_near_adjoint_mixed), then the partial sums of the leaves
-// that took several segments (k_near_finish / k_near_adjoint_finish with ADD).
+// The mixed-precision near field at the sources in two parts: the near part writes the
+// pair sums (k_near_mixed / k_near_adjoint_mixed, then the partial sums of the leaves
+// that took several segments, k_near_finish / k_near_adjoint_finish with ADD); the far
+// part adds the local expansions of every particle in FP64, one thread per slot
+// (k_far_field / k_far_adjoint: every lane busy, where a segment's warp would run it on
+// one lane per target).  The near part needs no expansion, so a caller can run it on
+// another stream while the M2M, M2L and L2L run.
 //
 // Pair arithmetic: positions relative to the target leaf's centre, in units of the
 // power-of-two length u (pair_unit), as FP32 hi + lo pairs (x = hi + lo to 2^-48
@@ -896,9 +908,9 @@ __global__ void k_far_field(Targets T, const int* __restrict__ slot_leaf,
     eval_local<LOCAL>(la, lb, leaf, order, width, T.pos[k] - T.center[2 * leaf],
                       T.pos[T.m + k] - T.center[2 * leaf + 1], lp, lx, ly);
     const i64 i = T.perm[k];
-    phi[i] = POT ? lp : 0.0;
-    field[i] = lx;
-    field[T.m + i] = ly;
+    if (POT) phi[i] += lp;
+    field[i] += lx;
+    field[T.m + i] += ly;
 }
 
 template <int LOCAL>
@@ -910,12 +922,12 @@ __global__ void k_far_adjoint(Targets T, Sources S, Adjoint A, const int* __rest
     td3_chain_release();
     const i64 k = (i64)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= T.m) return;
-    const double zero[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     const i64 leaf = slot_leaf[k];
     if (leaf < 0) return;
-    adjoint_finish<LOCAL>(zero, k, T.perm[k], S.n, T.pos[k] - T.center[2 * leaf],
-                          T.pos[T.m + k] - T.center[2 * leaf + 1], leaf, order, width, fa, fb,
-                          ba, bb, S, A);
+    const double ux = T.pos[k] - T.center[2 * leaf], uy = T.pos[T.m + k] - T.center[2 * leaf + 1];
+    const LocalJet f = local_jet<LOCAL>(fa, fb, leaf, order, width, ux, uy);  // Hessian
+    const LocalJet b = local_jet<LOCAL>(ba, bb, leaf, order, width, ux, uy);  // Psi
+    adjoint_far_add(f, b, k, T.perm[k], S.n, S, A);
 }
 
 // x in units of u relative to c, as an FP32 hi + lo pair.
@@ -1051,9 +1063,9 @@ k_near_mixed(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
         if (valid && L.slice == 0) {
             if (outp < 0) {
                 const i64 i = T.perm[k];
-                if (POT) phi[i] += v[0];
-                field[i] += v[1];
-                field[T.m + i] += v[2];
+                phi[i] = POT ? v[0] : 0.0;
+                field[i] = v[1];
+                field[T.m + i] = v[2];
             } else {
                 const i64 p = outp + it;
                 partial[3 * p] = v[0];
@@ -1369,19 +1381,24 @@ extern "C" int td3_slot_leaves(int64_t n_nodes, const int64_t* node_child,
 
 namespace {
 
+constexpr int PART_NEAR = 1, PART_FAR = 2;
+
+// The near part (pair sums written, then the multi-segment leaves) and / or the far part
+// (local expansions added) of the mixed near field at the sources.
 template <int KERNEL, bool POT, int LOCAL>
-int launch_near_mixed(const NearArgs& a, const int* slot_leaf, cudaStream_t s) {
-    TD3_TRY(td3_launch_chained(k_far_field<LOCAL, POT>, td3_blocks(a.T.m, 256), 256, 0, s, a.T,
-                               slot_leaf, a.la, a.lb, a.order, a.width, a.phi, a.field));
-    if (a.n_seg > 0) {
+int launch_near_mixed(const NearArgs& a, const int* slot_leaf, int parts, cudaStream_t s) {
+    if ((parts & PART_NEAR) && a.n_seg > 0) {
         const unsigned blocks = td3_blocks(a.n_seg, NF_WARPS);
         TD3_TRY(td3_launch_chained(k_near_mixed<KERNEL, POT>, blocks, 32 * NF_WARPS, 0, s, a.T,
                                    a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out, a.partners,
                                    a.eps2, a.partial, a.phi, a.field, a.status));
-        TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL, true>, td3_finish_blocks(a.n_seg), 32 * NF_WARPS, 0, s,
-                                   a.T, a.n_seg, a.seg_leaf, a.seg_out, a.la, a.lb, a.order,
-                                   a.width, a.partial, a.phi, a.field));
+        TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL, true>, td3_finish_blocks(a.n_seg),
+                                   32 * NF_WARPS, 0, s, a.T, a.n_seg, a.seg_leaf, a.seg_out, a.la,
+                                   a.lb, a.order, a.width, a.partial, a.phi, a.field));
     }
+    if (parts & PART_FAR)
+        TD3_TRY(td3_launch_chained(k_far_field<LOCAL, POT>, td3_blocks(a.T.m, 256), 256, 0, s,
+                                   a.T, slot_leaf, a.la, a.lb, a.order, a.width, a.phi, a.field));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
 }
@@ -1391,19 +1408,80 @@ int launch_adjoint_mixed(const Targets& T, const Sources& S, const Adjoint& A,
                          const int* slot_leaf, i64 n_seg, const int* seg_leaf,
                          const longlong2* sr, const i64* seg_out, const i64* partners,
                          const double* fa, const double* fb, const double* ba, const double* bb,
-                         int order, int width, double eps2, double* partial, cudaStream_t s) {
-    TD3_TRY(td3_launch_chained(k_far_adjoint<LOCAL>, td3_blocks(T.m, 256), 256, 0, s, T, S, A,
-                               slot_leaf, fa, fb, ba, bb, order, width));
-    if (n_seg > 0) {
+                         int order, int width, double eps2, double* partial, int parts,
+                         cudaStream_t s) {
+    if ((parts & PART_NEAR) && n_seg > 0) {
         const unsigned blocks = td3_blocks(n_seg, NF_WARPS);
         TD3_TRY(td3_launch_chained(k_near_adjoint_mixed<KERNEL>, blocks, 32 * NF_WARPS, 0, s, T,
                                    S, A, n_seg, seg_leaf, sr, seg_out, partners, eps2, partial));
-        TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL, true>, td3_finish_blocks(n_seg), 32 * NF_WARPS, 0,
-                                   s, T, S, A, n_seg, seg_leaf, seg_out, fa, fb, ba, bb, order,
-                                   width, partial));
+        TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL, true>, td3_finish_blocks(n_seg),
+                                   32 * NF_WARPS, 0, s, T, S, A, n_seg, seg_leaf, seg_out, fa, fb,
+                                   ba, bb, order, width, partial));
     }
+    if (parts & PART_FAR)
+        TD3_TRY(td3_launch_chained(k_far_adjoint<LOCAL>, td3_blocks(T.m, 256), 256, 0, s, T, S,
+                                   A, slot_leaf, fa, fb, ba, bb, order, width));
     TD3_CHECK_LAUNCH();
     return TD3_OK;
+}
+
+int near_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+               const int64_t* perm, int64_t n, const double* node_center,
+               const int64_t* node_start, const int64_t* node_end, int order,
+               const double* local_a, const double* local_b, const int32_t* slot_leaf,
+               const int64_t* p2p_partners, const int* seg_leaf, const int64_t* seg_range,
+               const int64_t* seg_out, int64_t n_seg, double* partial, double softening,
+               int with_potential, double unit, double* phi, double* field, int64_t* status,
+               int parts, void* stream) {
+    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (!(unit > 0.0 && unit < INFINITY)) return TD3_EINVAL;
+    if ((parts & PART_FAR) && !slot_leaf) return TD3_EINVAL;
+    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
+    if (n == 0) return TD3_OK;
+    const bool lg = kernel == TD3_KERNEL_LOG;
+    NearArgs a{Targets{sorted_pos, nullptr, perm, node_center, node_start, node_end, n},
+               Sources{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit},
+               n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
+               p2p_partners, local_a, local_b, order,
+               lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,
+               phi, field, status};
+    cudaStream_t s = td3_stream(stream);
+    constexpr int LG = TD3_KERNEL_LOG, CL = TD3_KERNEL_COULOMB;
+    if (lg)
+        return with_potential
+                   ? launch_near_mixed<LG, true, LOCAL_COMPLEX>(a, slot_leaf, parts, s)
+                   : launch_near_mixed<LG, false, LOCAL_COMPLEX>(a, slot_leaf, parts, s);
+    return with_potential ? launch_near_mixed<CL, true, LOCAL_CART>(a, slot_leaf, parts, s)
+                          : launch_near_mixed<CL, false, LOCAL_CART>(a, slot_leaf, parts, s);
+}
+
+int adjoint_mixed(int kernel, const double* sorted_pos, const double* sorted_charge,
+                  const int64_t* perm, int64_t n, const double* node_center,
+                  const int64_t* node_start, const int64_t* node_end, int order,
+                  const double* fwd_a, const double* fwd_b, const double* adj_a,
+                  const double* adj_b, const int32_t* slot_leaf, const int64_t* p2p_partners,
+                  const int* seg_leaf, const int64_t* seg_range, const int64_t* seg_out,
+                  int64_t n_seg, double* partial, const double* sorted_weight,
+                  const double* sorted_dipole, const double* efield, double softening,
+                  double unit, double* qbar, double* xbar, int parts, void* stream) {
+    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
+    if (!(unit > 0.0 && unit < INFINITY)) return TD3_EINVAL;
+    if ((parts & PART_FAR) && !slot_leaf) return TD3_EINVAL;
+    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
+    if (n == 0) return TD3_OK;
+    Targets T{sorted_pos, nullptr, perm, node_center, node_start, node_end, n};
+    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit};
+    Adjoint A{sorted_weight, sorted_dipole, efield, qbar, xbar};
+    const double eps2 = softening * softening;
+    cudaStream_t s = td3_stream(stream);
+    const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
+    if (kernel == TD3_KERNEL_LOG)
+        return launch_adjoint_mixed<TD3_KERNEL_LOG, LOCAL_COMPLEX>(
+            T, S, A, slot_leaf, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a,
+            adj_b, order, order + 1, eps2, partial, parts, s);
+    return launch_adjoint_mixed<TD3_KERNEL_COULOMB, LOCAL_CART>(
+        T, S, A, slot_leaf, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b,
+        order, (order + 1) * (order + 2) / 2, eps2, partial, parts, s);
 }
 
 }  // namespace
@@ -1418,24 +1496,34 @@ extern "C" int td3_fmm_evaluate_mixed(int kernel, const double* sorted_pos,
                                       int64_t n_seg, double* partial, double softening,
                                       int with_potential, double unit, double* phi,
                                       double* field, int64_t* status, void* stream) {
-    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
-    if (!(unit > 0.0 && unit < INFINITY) || !slot_leaf) return TD3_EINVAL;
-    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
-    if (n == 0) return TD3_OK;
-    const bool lg = kernel == TD3_KERNEL_LOG;
-    NearArgs a{Targets{sorted_pos, nullptr, perm, node_center, node_start, node_end, n},
-               Sources{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit},
-               n_seg, seg_leaf, reinterpret_cast<const longlong2*>(seg_range), seg_out,
-               p2p_partners, local_a, local_b, order,
-               lg ? order + 1 : (order + 1) * (order + 2) / 2, softening * softening, partial,
-               phi, field, status};
-    cudaStream_t s = td3_stream(stream);
-    constexpr int LG = TD3_KERNEL_LOG, CL = TD3_KERNEL_COULOMB;
-    if (lg)
-        return with_potential ? launch_near_mixed<LG, true, LOCAL_COMPLEX>(a, slot_leaf, s)
-                              : launch_near_mixed<LG, false, LOCAL_COMPLEX>(a, slot_leaf, s);
-    return with_potential ? launch_near_mixed<CL, true, LOCAL_CART>(a, slot_leaf, s)
-                          : launch_near_mixed<CL, false, LOCAL_CART>(a, slot_leaf, s);
+    return near_mixed(kernel, sorted_pos, sorted_charge, perm, n, node_center, node_start,
+                      node_end, order, local_a, local_b, slot_leaf, p2p_partners, seg_leaf,
+                      seg_range, seg_out, n_seg, partial, softening, with_potential, unit, phi,
+                      field, status, PART_NEAR | PART_FAR, stream);
+}
+
+extern "C" int td3_fmm_near_mixed(int kernel, const double* sorted_pos,
+                                  const double* sorted_charge, const int64_t* perm, int64_t n,
+                                  const double* node_center, const int64_t* node_start,
+                                  const int64_t* node_end, const int64_t* p2p_partners,
+                                  const int* seg_leaf, const int64_t* seg_range,
+                                  const int64_t* seg_out, int64_t n_seg, double* partial,
+                                  double softening, int with_potential, double unit, double* phi,
+                                  double* field, int64_t* status, void* stream) {
+    return near_mixed(kernel, sorted_pos, sorted_charge, perm, n, node_center, node_start,
+                      node_end, 0, nullptr, nullptr, nullptr, p2p_partners, seg_leaf, seg_range,
+                      seg_out, n_seg, partial, softening, with_potential, unit, phi, field,
+                      status, PART_NEAR, stream);
+}
+
+extern "C" int td3_fmm_far_mixed(int kernel, const double* sorted_pos, const int64_t* perm,
+                                 int64_t n, const double* node_center, int order,
+                                 const double* local_a, const double* local_b,
+                                 const int32_t* slot_leaf, int with_potential, double* phi,
+                                 double* field, void* stream) {
+    return near_mixed(kernel, sorted_pos, nullptr, perm, n, node_center, nullptr, nullptr, order,
+                      local_a, local_b, slot_leaf, nullptr, nullptr, nullptr, nullptr, 0,
+                      nullptr, 0.0, with_potential, 1.0, phi, field, nullptr, PART_FAR, stream);
 }
 
 extern "C" int td3_fmm_adjoint_mixed(int kernel, const double* sorted_pos,
@@ -1450,21 +1538,39 @@ extern "C" int td3_fmm_adjoint_mixed(int kernel, const double* sorted_pos,
                                      const double* sorted_dipole, const double* efield,
                                      double softening, double unit, double* qbar, double* xbar,
                                      void* stream) {
-    if (n < 0 || n_seg < 0 || order < 0 || order > TD3_MAX_ORDER) return TD3_EINVAL;
-    if (!(unit > 0.0 && unit < INFINITY) || !slot_leaf) return TD3_EINVAL;
-    if (kernel != TD3_KERNEL_COULOMB && kernel != TD3_KERNEL_LOG) return TD3_EINVAL;
-    if (n == 0) return TD3_OK;
-    Targets T{sorted_pos, nullptr, perm, node_center, node_start, node_end, n};
-    Sources S{sorted_pos, sorted_charge, perm, node_start, node_end, n, unit};
-    Adjoint A{sorted_weight, sorted_dipole, efield, qbar, xbar};
-    const double eps2 = softening * softening;
-    cudaStream_t s = td3_stream(stream);
-    const longlong2* sr = reinterpret_cast<const longlong2*>(seg_range);
-    if (kernel == TD3_KERNEL_LOG)
-        return launch_adjoint_mixed<TD3_KERNEL_LOG, LOCAL_COMPLEX>(
-            T, S, A, slot_leaf, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a,
-            adj_b, order, order + 1, eps2, partial, s);
-    return launch_adjoint_mixed<TD3_KERNEL_COULOMB, LOCAL_CART>(
-        T, S, A, slot_leaf, n_seg, seg_leaf, sr, seg_out, p2p_partners, fwd_a, fwd_b, adj_a, adj_b,
-        order, (order + 1) * (order + 2) / 2, eps2, partial, s);
+    return adjoint_mixed(kernel, sorted_pos, sorted_charge, perm, n, node_center, node_start,
+                         node_end, order, fwd_a, fwd_b, adj_a, adj_b, slot_leaf, p2p_partners,
+                         seg_leaf, seg_range, seg_out, n_seg, partial, sorted_weight,
+                         sorted_dipole, efield, softening, unit, qbar, xbar,
+                         PART_NEAR | PART_FAR, stream);
+}
+
+extern "C" int td3_fmm_adjoint_near_mixed(int kernel, const double* sorted_pos,
+                                          const double* sorted_charge, const int64_t* perm,
+                                          int64_t n, const double* node_center,
+                                          const int64_t* node_start, const int64_t* node_end,
+                                          const int64_t* p2p_partners, const int* seg_leaf,
+                                          const int64_t* seg_range, const int64_t* seg_out,
+                                          int64_t n_seg, double* partial,
+                                          const double* sorted_weight,
+                                          const double* sorted_dipole, double softening,
+                                          double unit, double* qbar, double* xbar, void* stream) {
+    return adjoint_mixed(kernel, sorted_pos, sorted_charge, perm, n, node_center, node_start,
+                         node_end, 0, nullptr, nullptr, nullptr, nullptr, nullptr, p2p_partners,
+                         seg_leaf, seg_range, seg_out, n_seg, partial, sorted_weight,
+                         sorted_dipole, nullptr, softening, unit, qbar, xbar, PART_NEAR, stream);
+}
+
+extern "C" int td3_fmm_adjoint_far_mixed(int kernel, const double* sorted_pos,
+                                         const double* sorted_charge, const int64_t* perm,
+                                         int64_t n, const double* node_center, int order,
+                                         const double* fwd_a, const double* fwd_b,
+                                         const double* adj_a, const double* adj_b,
+                                         const int32_t* slot_leaf, const double* sorted_weight,
+                                         const double* sorted_dipole, const double* efield,
+                                         double* qbar, double* xbar, void* stream) {
+    return adjoint_mixed(kernel, sorted_pos, sorted_charge, perm, n, node_center, nullptr,
+                         nullptr, order, fwd_a, fwd_b, adj_a, adj_b, slot_leaf, nullptr, nullptr,
+                         nullptr, nullptr, 0, nullptr, sorted_weight, sorted_dipole, efield, 0.0,
+                         1.0, qbar, xbar, PART_FAR, stream);
 }

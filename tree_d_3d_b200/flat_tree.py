@@ -181,6 +181,20 @@ NEAR_SEGMENT = 256
 #: the one-launch form of td3_fmm_evaluate / td3_fmm_adjoint with mixed = 1.
 NEAR_SPLIT = True
 
+#: with NEAR_SPLIT, the near part (pair sums) runs on a second stream while the M2L and the
+#: downward pass run on the caller's stream; the far part follows both.
+NEAR_OVERLAP = True
+
+_SIDE_STREAMS: dict = {}
+
+
+def _side_stream(device) -> "torch.cuda.Stream":
+    """The second stream of ``device`` the near field's pair sums run on."""
+    key = torch.device(device).index
+    if key not in _SIDE_STREAMS:
+        _SIDE_STREAMS[key] = torch.cuda.Stream(device=device)
+    return _SIDE_STREAMS[key]
+
 #: mixed-precision M2L matrix products on the tensor cores (tcgen05, 3xTF32; orders up
 #: to 15) instead of FP32 CUDA-core arithmetic.  Off by default: the tensor-core form is
 #: correct but, waiting on each 128-row tile, still slower than the CUDA-core form.
@@ -768,11 +782,24 @@ class FlatQuadtree:
             self._coulomb_fmm(theta, softening, phi, field, _status)
             return out((phi, field), self._numpy)
         lists = self._lists(theta)
-        local_re, local_im = self._log_locals(lists)
-        self._fwd_locals = ((theta, softening), local_re, local_im)
         status = status_word(dev) if _status is None else _status
-        self._evaluate_near(lists, _lib.KERNEL_LOG, local_re, local_im, softening, potential,
-                            phi, field, status)
+        if self._mixed and NEAR_SPLIT and NEAR_OVERLAP:
+            # the pair sums on the second stream while the M2L and L2L run here
+            done = self._near_part(lists, _lib.KERNEL_LOG, softening, potential, phi, field,
+                                   status)
+            local_re, local_im = self._log_locals(lists)
+            self._fwd_locals = ((theta, softening), local_re, local_im)
+            torch.cuda.current_stream(dev).wait_event(done)
+            _lib.call("td3_fmm_far_mixed", _lib.KERNEL_LOG, self._sorted_pos.data_ptr(),
+                      self.perm.data_ptr(), n, self.node_center.data_ptr(), self.order,
+                      local_re.data_ptr(), local_im.data_ptr(), self._slot_leaves().data_ptr(),
+                      1 if potential else 0, phi.data_ptr(), field.data_ptr(),
+                      _lib.stream(dev))
+        else:
+            local_re, local_im = self._log_locals(lists)
+            self._fwd_locals = ((theta, softening), local_re, local_im)
+            self._evaluate_near(lists, _lib.KERNEL_LOG, local_re, local_im, softening,
+                                potential, phi, field, status)
         if _status is None:
             _check(status)
             self._check_tensor_cores()
@@ -820,6 +847,26 @@ class FlatQuadtree:
                   self.node_start.data_ptr(), self.node_end.data_ptr(), order,
                   binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
                   _lib.stream(self.device))
+
+    def _near_part(self, lists, kernel, softening, potential, phi, field, status):
+        """td3_fmm_near_mixed on the second stream after the work enqueued so far on the
+        caller's stream; returns the event the far part waits for.  The tensors it reads
+        and writes stay alive until the caller's stream has waited for the event."""
+        dev = self.device
+        side = _side_stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        plan = lists["plan"]
+        _lib.call("td3_fmm_near_mixed", kernel, self._sorted_pos.data_ptr(),
+                  self._sorted_charge.data_ptr(), self.perm.data_ptr(), self.pos.shape[1],
+                  self.node_center.data_ptr(), self.node_start.data_ptr(),
+                  self.node_end.data_ptr(), lists["p2p_partners"].data_ptr(),
+                  plan["seg_leaf"].data_ptr(), plan["seg_range"].data_ptr(),
+                  plan["seg_out"].data_ptr(), plan["n_seg"], plan["partial"].data_ptr(),
+                  float(softening), 1 if potential else 0, self._unit, phi.data_ptr(),
+                  field.data_ptr(), status.data_ptr(), side.cuda_stream)
+        done = torch.cuda.Event()
+        done.record(side)
+        return done
 
     def _slot_leaves(self) -> torch.Tensor:
         """The leaf of every particle slot (td3_slot_leaves), kept with the tree."""
@@ -965,6 +1012,28 @@ class FlatQuadtree:
         kept = getattr(self, "_fwd_locals", None)
         if kept is not None and kept[0] != (theta, softening):
             kept = None
+        overlap = self._mixed and NEAR_SPLIT and NEAR_OVERLAP
+        if overlap:
+            # the near parts of qbar and xbar on the second stream while the adjoint
+            # moments, M2L and L2L run here
+            plan = lists["plan"]
+            partial = torch.empty(6 * max(plan["partial_len"], 1), dtype=torch.float64,
+                                  device=dev)
+            qbar = torch.empty(n, dtype=torch.float64, device=dev)
+            xbar = torch.empty((2, n), dtype=torch.float64, device=dev)
+            side = _side_stream(dev)
+            side.wait_stream(torch.cuda.current_stream(dev))
+            _lib.call("td3_fmm_adjoint_near_mixed",
+                      _lib.KERNEL_LOG if self.kernel == "log" else _lib.KERNEL_COULOMB,
+                      self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
+                      self.perm.data_ptr(), n, self.node_center.data_ptr(),
+                      self.node_start.data_ptr(), self.node_end.data_ptr(),
+                      lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
+                      plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
+                      partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), float(softening),
+                      self._unit, qbar.data_ptr(), xbar.data_ptr(), side.cuda_stream)
+            near_done = torch.cuda.Event()
+            near_done.record(side)
         if self.kernel == "log":
             w = self.order + 1
             fwd_a, fwd_b = (kept[1], kept[2]) if kept else self._log_locals(lists)
@@ -992,6 +1061,16 @@ class FlatQuadtree:
                                       softening, moments=moments)
             fwd_b, adj_b = fwd_a, adj_a
             kernel = _lib.KERNEL_COULOMB
+        if overlap:
+            torch.cuda.current_stream(dev).wait_event(near_done)
+            _lib.call("td3_fmm_adjoint_far_mixed", kernel, self._sorted_pos.data_ptr(),
+                      self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
+                      self.node_center.data_ptr(), self.order, fwd_a.data_ptr(),
+                      fwd_b.data_ptr(), adj_a.data_ptr(), adj_b.data_ptr(),
+                      self._slot_leaves().data_ptr(), sw.data_ptr(), sd.data_ptr(),
+                      efield.data_ptr(), qbar.data_ptr(), xbar.data_ptr(), stream)
+            self._check_tensor_cores()
+            return qbar, xbar
         plan = lists["plan"]
         partial = torch.empty(6 * max(plan["partial_len"], 1), dtype=torch.float64, device=dev)
         qbar = torch.zeros(n, dtype=torch.float64, device=dev)
