@@ -784,11 +784,17 @@ class FlatQuadtree:
         lists = self._lists(theta)
         status = status_word(dev) if _status is None else _status
         if self._mixed and NEAR_SPLIT and NEAR_OVERLAP:
-            # the pair sums on the second stream while the M2L and L2L run here
-            done = self._near_part(lists, _lib.KERNEL_LOG, softening, potential, phi, field,
-                                   status)
+            # the M2L and L2L enqueued here first, then the pair sums on the second stream
+            # (after the lists only): the M2L's blocks are dispatched first and the pair
+            # sums fill the SMs the per-level L2L launches leave idle
+            # (phi, field, status and the plan's buffer, which the second stream writes,
+            # exist before the event it waits for)
+            ready = torch.cuda.Event()
+            ready.record(torch.cuda.current_stream(dev))
             local_re, local_im = self._log_locals(lists)
             self._fwd_locals = ((theta, softening), local_re, local_im)
+            done = self._near_part(lists, _lib.KERNEL_LOG, softening, potential, phi, field,
+                                   status, after=ready)
             torch.cuda.current_stream(dev).wait_event(done)
             _lib.call("td3_fmm_far_mixed", _lib.KERNEL_LOG, self._sorted_pos.data_ptr(),
                       self.perm.data_ptr(), n, self.node_center.data_ptr(), self.order,
@@ -848,13 +854,13 @@ class FlatQuadtree:
                   binom.data_ptr(), binom.shape[0], local_re.data_ptr(), local_im.data_ptr(),
                   _lib.stream(self.device))
 
-    def _near_part(self, lists, kernel, softening, potential, phi, field, status):
-        """td3_fmm_near_mixed on the second stream after the work enqueued so far on the
+    def _near_part(self, lists, kernel, softening, potential, phi, field, status, after):
+        """td3_fmm_near_mixed on the second stream after the event ``after`` of the
         caller's stream; returns the event the far part waits for.  The tensors it reads
         and writes stay alive until the caller's stream has waited for the event."""
         dev = self.device
         side = _side_stream(dev)
-        side.wait_stream(torch.cuda.current_stream(dev))
+        side.wait_event(after)
         plan = lists["plan"]
         _lib.call("td3_fmm_near_mixed", kernel, self._sorted_pos.data_ptr(),
                   self._sorted_charge.data_ptr(), self.perm.data_ptr(), self.pos.shape[1],
@@ -1014,26 +1020,15 @@ class FlatQuadtree:
             kept = None
         overlap = self._mixed and NEAR_SPLIT and NEAR_OVERLAP
         if overlap:
-            # the near parts of qbar and xbar on the second stream while the adjoint
-            # moments, M2L and L2L run here
+            # what the second stream writes is allocated before the event it waits for,
+            # so it cannot take memory that work enqueued after the event still uses
             plan = lists["plan"]
             partial = torch.empty(6 * max(plan["partial_len"], 1), dtype=torch.float64,
                                   device=dev)
             qbar = torch.empty(n, dtype=torch.float64, device=dev)
             xbar = torch.empty((2, n), dtype=torch.float64, device=dev)
-            side = _side_stream(dev)
-            side.wait_stream(torch.cuda.current_stream(dev))
-            _lib.call("td3_fmm_adjoint_near_mixed",
-                      _lib.KERNEL_LOG if self.kernel == "log" else _lib.KERNEL_COULOMB,
-                      self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
-                      self.perm.data_ptr(), n, self.node_center.data_ptr(),
-                      self.node_start.data_ptr(), self.node_end.data_ptr(),
-                      lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
-                      plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
-                      partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), float(softening),
-                      self._unit, qbar.data_ptr(), xbar.data_ptr(), side.cuda_stream)
-            near_done = torch.cuda.Event()
-            near_done.record(side)
+            ready = torch.cuda.Event()
+            ready.record(torch.cuda.current_stream(dev))
         if self.kernel == "log":
             w = self.order + 1
             fwd_a, fwd_b = (kept[1], kept[2]) if kept else self._log_locals(lists)
@@ -1062,6 +1057,22 @@ class FlatQuadtree:
             fwd_b, adj_b = fwd_a, adj_a
             kernel = _lib.KERNEL_COULOMB
         if overlap:
+            # the adjoint moments, M2L and L2L enqueued first; the near parts of qbar and
+            # xbar on the second stream after the weights only, filling the SMs the
+            # per-level launches leave idle
+            side = _side_stream(dev)
+            side.wait_event(ready)
+            _lib.call("td3_fmm_adjoint_near_mixed",
+                      _lib.KERNEL_LOG if self.kernel == "log" else _lib.KERNEL_COULOMB,
+                      self._sorted_pos.data_ptr(), self._sorted_charge.data_ptr(),
+                      self.perm.data_ptr(), n, self.node_center.data_ptr(),
+                      self.node_start.data_ptr(), self.node_end.data_ptr(),
+                      lists["p2p_partners"].data_ptr(), plan["seg_leaf"].data_ptr(),
+                      plan["seg_range"].data_ptr(), plan["seg_out"].data_ptr(), plan["n_seg"],
+                      partial.data_ptr(), sw.data_ptr(), sd.data_ptr(), float(softening),
+                      self._unit, qbar.data_ptr(), xbar.data_ptr(), side.cuda_stream)
+            near_done = torch.cuda.Event()
+            near_done.record(side)
             torch.cuda.current_stream(dev).wait_event(near_done)
             _lib.call("td3_fmm_adjoint_far_mixed", kernel, self._sorted_pos.data_ptr(),
                       self._sorted_charge.data_ptr(), self.perm.data_ptr(), n,
