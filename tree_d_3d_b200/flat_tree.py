@@ -1370,13 +1370,28 @@ class FlatQuadtree:
         """ft:1360-1428: the Coulomb FMM with Cartesian expansions (the potential is
         always computed, as in the reference); ``status`` as fmm's ``_status``."""
         lists = self._lists(theta)
+        deferred = status is not None
+        status = status_word(self.device) if status is None else status
+        overlap = self._mixed and NEAR_SPLIT and NEAR_OVERLAP
+        if overlap:  # as fmm's log kernel: the pair sums beside the M2L and L2L
+            lists["m2l_rows"]
+            ready = torch.cuda.Event()
+            ready.record(torch.cuda.current_stream(self.device))
         local = self._cart_locals(lists["m2l_rows"], lists["m2l_partners"],
                                   lists["m2l"].shape[0], self, softening)
         self._fwd_locals = ((theta, softening), local, local)
-        deferred = status is not None
-        status = status_word(self.device) if status is None else status
-        self._evaluate_near(lists, _lib.KERNEL_COULOMB, local, local, softening, True, phi,
-                            field, status)
+        if overlap:
+            done = self._near_part(lists, _lib.KERNEL_COULOMB, softening, True, phi, field,
+                                   status, after=ready)
+            torch.cuda.current_stream(self.device).wait_event(done)
+            _lib.call("td3_fmm_far_mixed", _lib.KERNEL_COULOMB, self._sorted_pos.data_ptr(),
+                      self.perm.data_ptr(), self.pos.shape[1], self.node_center.data_ptr(),
+                      self.order, local.data_ptr(), local.data_ptr(),
+                      self._slot_leaves().data_ptr(), 1, phi.data_ptr(), field.data_ptr(),
+                      _lib.stream(self.device))
+        else:
+            self._evaluate_near(lists, _lib.KERNEL_COULOMB, local, local, softening, True,
+                                phi, field, status)
         if not deferred:
             _check(status)
         self.fmm_pairs = (int(lists["m2l"].shape[0]), int(lists["p2p"].shape[0]))
