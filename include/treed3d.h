@@ -331,12 +331,11 @@ int td3_fmm_m2l_mixed(const int64_t* row_start, const int32_t* entry_row,
  * records (td3_pack_m2l_sources: td3_m2l_record_floats(order) floats per node, 16-byte
  * aligned: the centre as two doubles, hat_k = a_k / h^k as FP32 pairs, h / unit; 128
  * bytes at order 12, one cache line per gathered partner) written from the source tree's
- * FP64 moments, centres and half-widths.  Orders <= 20; coeff HOST.  Fastest on rows of
- * a few tens of entries (fmm's mutual lists: 0.78 ms against 0.93 ms for
- * td3_fmm_m2l_mixed at 1M particles); on fmm_at's one-way target rows (a quarter of them
- * up to 5 entries) it measured 4.0 ms against 1.05 ms, so FlatQuadtree keeps
- * td3_fmm_m2l_mixed there.  Replaces fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/
- * fmm_m2l_host_pyccel.py:16-105) in FP32 for fmm (src/tree_d_3d/flat_tree.py:1505-1539). */
+ * FP64 moments, centres and half-widths.  A warp's rows are an even share of entries + 8
+ * per row (a row takes a group at least one round), so runs of empty or short rows, as
+ * in fmm_at's one-way target rows, spread over the warps.  Orders <= 20; coeff HOST.
+ * Replaces fmm_m2l_host (src/tree_d_3d/kernels/fmm_m2l_host/fmm_m2l_host_pyccel.py:16-105)
+ * in FP32 for fmm / fmm_at (src/tree_d_3d/flat_tree.py:1505-1539, :1151-1316). */
 int td3_m2l_record_floats(int order);
 int td3_pack_m2l_sources(int64_t count, int order, const double* moment_re,
                          const double* moment_im, const double* node_center,

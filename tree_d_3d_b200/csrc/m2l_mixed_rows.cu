@@ -6,7 +6,8 @@
 // FP64, its moments scaled by its size, hat_k = a_k / h^k, in FP32 pairs, and h / unit,
 // 8 (P + 4) bytes (128 bytes at P = 12: one cache line per gathered partner).
 //
-// Work: a warp owns a run of whole destination rows (an even share of the entries).
+// Work: a warp owns a run of whole destination rows (an even share of the entries, each
+// row counting 8 more).
 // Its four 8-lane groups take the rows in order, each row whole: lane i of a group
 // translates entries i, i + 8, ... of the row and adds the contributions into its own
 // FP32 sums, kept in shared memory (a warp's sums column-major with a 33-word stride: a
@@ -22,6 +23,7 @@ namespace {
 constexpr int RW = 4;          // warps per block
 constexpr int GL = 8;          // lanes per destination group
 constexpr int LONG_ROW = 96;   // rows longer than this are taken by the whole warp
+constexpr int ROW_COST = GL;   // entries a row counts for in the warps' shares
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int MAX_DEVICES = 64;
 
@@ -188,13 +190,16 @@ k_m2l_mixed_rows(const i64* __restrict__ row_start, const i64* __restrict__ part
     float* wacc = accs[wib];
     const int w = order + 1;
     const double inv_unit = 1.0 / unit, ln_unit = log(unit);
+    // this warp's rows [da, db): an even share of the cost entries + ROW_COST x rows (a
+    // row takes a group at least one round, however few its entries: a run of empty or
+    // short rows must not fall to one warp)
     const i64 gw = (i64)blockIdx.x * RW + wib, nw = (i64)gridDim.x * RW;
-    const i64 total = row_start[n_dst], share = (total + nw - 1) / nw;
+    const i64 total = row_start[n_dst] + ROW_COST * n_dst, share = (total + nw - 1) / nw;
     auto first_row_at = [&](i64 e) {
         i64 lo = 0, hi = n_dst;
         while (lo < hi) {
             i64 mid = (lo + hi) >> 1;
-            if (row_start[mid] < e) lo = mid + 1;
+            if (row_start[mid] + ROW_COST * mid < e) lo = mid + 1;
             else hi = mid;
         }
         return lo;

@@ -217,11 +217,9 @@ MOMENTS_ONE_LAUNCH = False
 #: at 1M, p = 12, against 0.91 ms for the CUDA-core form.
 M2L_GROUPED = False
 
-#: the mixed-precision CUDA-core M2L of fmm's mutual lists with a group of 8 lanes per
-#: destination row (td3_fmm_m2l_mixed_rows: partial sums in shared memory, packed
-#: 128-byte source records) instead of a lane per entry across row boundaries
-#: (td3_fmm_m2l_mixed, which fmm_at's one-way lists keep: 1.05 against 4.0 ms at 1M
-#: targets).
+#: the mixed-precision CUDA-core M2L with a group of 8 lanes per destination row
+#: (td3_fmm_m2l_mixed_rows: partial sums in shared memory, packed 128-byte source records)
+#: instead of a lane per entry across row boundaries (td3_fmm_m2l_mixed).
 M2L_ROWS = True
 
 
@@ -978,9 +976,7 @@ class FlatQuadtree:
             rows, partners = lists["m2l_rows"], lists["m2l_partners"]
             coeff = np.ascontiguousarray(_m2l_coefficients(self.order, self.symmetric))
             tensor = 1 if M2L_TENSOR_CORES and self.order <= 15 else 0
-            # the row-group form on the mutual lists of fmm; fmm_at's one-way target rows
-            # (shorter and uneven) keep the lane-per-entry form, which is 4x faster on them
-            if M2L_ROWS and not tensor and dst is self:
+            if M2L_ROWS and not tensor:
                 records = self._source_records(moments)
                 _lib.call("td3_fmm_m2l_mixed_rows", rows.data_ptr(), partners.data_ptr(),
                           dst.node_count, dst.node_center.data_ptr(), dst.node_half.data_ptr(),
