@@ -15,7 +15,10 @@
 
 namespace {
 
-constexpr int NF_WARPS = 4;
+constexpr int NF_WARPS = 4;   // warps per block of the finish kernels
+// Warps per block of the one-launch pair kernels (k_near, k_near_adjoint): one, so a
+// segment's warp frees its slot when it ends rather than with its block's slowest segment.
+constexpr int NW_NEAR = 1;
 constexpr int LOCAL_COMPLEX = 0;
 constexpr int LOCAL_CART = 1;
 
@@ -313,7 +316,7 @@ constexpr int NF_BLOCK = 16;
 // arithmetic with compensated sums (pair_mixed), else FP64.  The sources come through
 // shared memory (for_source_windows).
 template <int KERNEL, bool POT, bool OTHER, int LOCAL, bool MIXED>
-__global__ void __launch_bounds__(32 * NF_WARPS)
+__global__ void __launch_bounds__(32 * NW_NEAR, 28 / NW_NEAR)
 k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
        const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
        const i64* __restrict__ partners, const double* __restrict__ local_a,
@@ -322,10 +325,10 @@ k_near(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
        i64* status) {
     td3_chain_wait();
     td3_chain_release();
-    __shared__ NearWindow windows[NF_WARPS];
+    __shared__ NearWindow windows[NW_NEAR];
     int lane = threadIdx.x & 31;
     NearWindow& win = windows[threadIdx.x >> 5];
-    i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    i64 seg = (i64)blockIdx.x * NW_NEAR + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     i64 leaf = seg_leaf[seg];
     longlong2 er = seg_range[seg];
@@ -686,7 +689,7 @@ struct AdjointWindow<true> {
 };
 
 template <int KERNEL, int LOCAL, bool MIXED>
-__global__ void __launch_bounds__(32 * NF_WARPS, 6)
+__global__ void __launch_bounds__(32 * NW_NEAR, 24 / NW_NEAR)
 k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
                const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
                const i64* __restrict__ partners, const double* __restrict__ fa,
@@ -695,10 +698,10 @@ k_near_adjoint(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict
                double* __restrict__ partial) {
     td3_chain_wait();
     td3_chain_release();
-    __shared__ AdjointWindow<MIXED> windows[NF_WARPS];
+    __shared__ AdjointWindow<MIXED> windows[NW_NEAR];
     int lane = threadIdx.x & 31;
     AdjointWindow<MIXED>& win = windows[threadIdx.x >> 5];
-    i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    i64 seg = (i64)blockIdx.x * NW_NEAR + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     i64 leaf = seg_leaf[seg];
     longlong2 er = seg_range[seg];
@@ -961,6 +964,10 @@ struct LaneMap {
 };
 
 constexpr int NM_CAP = 128;  // staged sources per warp window (mixed forward)
+// Warps per block of the mixed pair kernels: one, so a segment's warp frees its slot when
+// it ends rather than with its block's slowest segment (segments differ in cost with
+// their leaf's particles and partners); 32 one-warp blocks of 64 registers per SM.
+constexpr int NM_WARPS = 1;
 
 struct MixedWindow {
     float4 pos[NM_CAP];  // (x hi, x lo, y hi, y lo) relative to the target leaf's centre
@@ -969,18 +976,18 @@ struct MixedWindow {
     int tag[NM_CAP];  // slot j (self-exclusion)
 };
 
-template <int KERNEL, bool POT>
-__global__ void __launch_bounds__(32 * NF_WARPS, 8)
+template <int KERNEL, bool POT, int NW>
+__global__ void __launch_bounds__(32 * NW, 32 / NW)
 k_near_mixed(Targets T, Sources S, i64 n_seg, const int* __restrict__ seg_leaf,
              const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
              const i64* __restrict__ partners, double eps2, double* __restrict__ partial,
              double* __restrict__ phi, double* __restrict__ field, i64* status) {
     td3_chain_wait();
     td3_chain_release();
-    __shared__ MixedWindow windows[NF_WARPS];
+    __shared__ MixedWindow windows[NW];
     const int lane = threadIdx.x & 31;
     MixedWindow& win = windows[threadIdx.x >> 5];
-    const i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    const i64 seg = (i64)blockIdx.x * NW + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     const i64 leaf = seg_leaf[seg];
     const longlong2 er = seg_range[seg];
@@ -1086,17 +1093,17 @@ struct MixedAdjointWindow {
     int tag[NM_CAP_ADJ];
 };
 
-template <int KERNEL>
-__global__ void __launch_bounds__(32 * NF_WARPS, 8)
+template <int KERNEL, int NW>
+__global__ void __launch_bounds__(32 * NW, 32 / NW)
 k_near_adjoint_mixed(Targets T, Sources S, Adjoint A, i64 n_seg, const int* __restrict__ seg_leaf,
                      const longlong2* __restrict__ seg_range, const i64* __restrict__ seg_out,
                      const i64* __restrict__ partners, double eps2, double* __restrict__ partial) {
     td3_chain_wait();
     td3_chain_release();
-    __shared__ MixedAdjointWindow windows[NF_WARPS];
+    __shared__ MixedAdjointWindow windows[NW];
     const int lane = threadIdx.x & 31;
     MixedAdjointWindow& win = windows[threadIdx.x >> 5];
-    const i64 seg = (i64)blockIdx.x * NF_WARPS + (threadIdx.x >> 5);
+    const i64 seg = (i64)blockIdx.x * NW + (threadIdx.x >> 5);
     if (seg >= n_seg) return;
     const i64 leaf = seg_leaf[seg];
     const longlong2 er = seg_range[seg];
@@ -1186,9 +1193,8 @@ struct NearArgs {
 template <int KERNEL, bool POT, bool OTHER, int LOCAL, bool MIXED>
 int launch_near(const NearArgs& a, cudaStream_t s) {
     if (a.n_seg == 0) return TD3_OK;
-    unsigned blocks = td3_blocks(a.n_seg, NF_WARPS);
-    TD3_TRY(td3_launch_chained(k_near<KERNEL, POT, OTHER, LOCAL, MIXED>, blocks, 32 * NF_WARPS, 0,
-                               s, a.T, a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out,
+    TD3_TRY(td3_launch_chained(k_near<KERNEL, POT, OTHER, LOCAL, MIXED>,
+                               td3_blocks(a.n_seg, NW_NEAR), 32 * NW_NEAR, 0, s, a.T, a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out,
                                a.partners, a.la, a.lb, a.order, a.width, a.eps2, a.partial, a.phi,
                                a.field, a.status));
     TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL>, td3_finish_blocks(a.n_seg), 32 * NF_WARPS, 0, s, a.T,
@@ -1289,8 +1295,8 @@ int launch_adjoint(const Targets& T, const Sources& S, const Adjoint& A, i64 n_s
                    const i64* partners, const double* fa, const double* fb, const double* ba,
                    const double* bb, int order, int width, double eps2, double* partial,
                    cudaStream_t s) {
-    unsigned blocks = td3_blocks(n_seg, NF_WARPS);
-    TD3_TRY(td3_launch_chained(k_near_adjoint<KERNEL, LOCAL, MIXED>, blocks, 32 * NF_WARPS, 0, s,
+    TD3_TRY(td3_launch_chained(k_near_adjoint<KERNEL, LOCAL, MIXED>, td3_blocks(n_seg, NW_NEAR),
+                               32 * NW_NEAR, 0, s,
                                T, S, A, n_seg, seg_leaf, sr, seg_out, partners, fa, fb, ba, bb,
                                order, width, eps2, partial));
     TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL>, td3_finish_blocks(n_seg), 32 * NF_WARPS, 0, s, T, S,
@@ -1388,9 +1394,9 @@ constexpr int PART_NEAR = 1, PART_FAR = 2;
 template <int KERNEL, bool POT, int LOCAL>
 int launch_near_mixed(const NearArgs& a, const int* slot_leaf, int parts, cudaStream_t s) {
     if ((parts & PART_NEAR) && a.n_seg > 0) {
-        const unsigned blocks = td3_blocks(a.n_seg, NF_WARPS);
-        TD3_TRY(td3_launch_chained(k_near_mixed<KERNEL, POT>, blocks, 32 * NF_WARPS, 0, s, a.T,
-                                   a.S, a.n_seg, a.seg_leaf, a.seg_range, a.seg_out, a.partners,
+        TD3_TRY(td3_launch_chained(k_near_mixed<KERNEL, POT, NM_WARPS>,
+                                   td3_blocks(a.n_seg, NM_WARPS), 32 * NM_WARPS, 0, s, a.T, a.S,
+                                   a.n_seg, a.seg_leaf, a.seg_range, a.seg_out, a.partners,
                                    a.eps2, a.partial, a.phi, a.field, a.status));
         TD3_TRY(td3_launch_chained(k_near_finish<POT, LOCAL, true>, td3_finish_blocks(a.n_seg),
                                    32 * NF_WARPS, 0, s, a.T, a.n_seg, a.seg_leaf, a.seg_out, a.la,
@@ -1411,9 +1417,9 @@ int launch_adjoint_mixed(const Targets& T, const Sources& S, const Adjoint& A,
                          int order, int width, double eps2, double* partial, int parts,
                          cudaStream_t s) {
     if ((parts & PART_NEAR) && n_seg > 0) {
-        const unsigned blocks = td3_blocks(n_seg, NF_WARPS);
-        TD3_TRY(td3_launch_chained(k_near_adjoint_mixed<KERNEL>, blocks, 32 * NF_WARPS, 0, s, T,
-                                   S, A, n_seg, seg_leaf, sr, seg_out, partners, eps2, partial));
+        TD3_TRY(td3_launch_chained(k_near_adjoint_mixed<KERNEL, NM_WARPS>,
+                                   td3_blocks(n_seg, NM_WARPS), 32 * NM_WARPS, 0, s, T, S, A,
+                                   n_seg, seg_leaf, sr, seg_out, partners, eps2, partial));
         TD3_TRY(td3_launch_chained(k_near_adjoint_finish<LOCAL, true>, td3_finish_blocks(n_seg),
                                    32 * NF_WARPS, 0, s, T, S, A, n_seg, seg_leaf, seg_out, fa, fb,
                                    ba, bb, order, width, partial));
