@@ -65,3 +65,58 @@ def test_row_group_m2l_records_and_rejections():
     assert rc == _lib.EINVAL
     rc = _lib.lib().td3_fmm_m2l_mixed_rows(0, 0, 1, 0, 0, 0, 21, 0, 1.0, 0, 0, 0)
     assert rc == _lib.EINVAL
+
+
+def test_row_group_m2l_on_runs_of_empty_rows():
+    """Rows of a real tree with a contiguous half emptied (the shape of fmm_at's target
+    rows, where a run of empty or short rows once fell to one warp): the row-group form
+    through the C ABI against the lane-per-entry form on the same rows, to FP32 accuracy,
+    the same bits every run."""
+    from tree_d_3d_b200 import FlatQuadtree, Quad, _lib, synthetic
+    from tree_d_3d_b200.flat_tree import _m2l_coefficients
+
+    pos, q = synthetic.mixture8(150_000, seed=81)
+    P, Q = torch.tensor(pos, device="cuda"), torch.tensor(q, device="cuda")
+    tree = FlatQuadtree(P, Q, Quad(0, 0, 1), kernel="log", order=12, precision="mixed")
+    lists = tree._lists(0.5)
+    rows = lists["m2l_rows"].cpu().numpy()
+    partners = lists["m2l_partners"].cpu().numpy()
+    n = tree.node_count
+    length = np.diff(rows)
+    length[n // 4: 3 * n // 4] = 0  # half the rows emptied, in one run
+    keep = np.repeat(np.diff(rows) == length, np.diff(rows))
+    new_rows = np.concatenate(([0], np.cumsum(length))).astype(np.int64)
+    new_partners = partners[: rows[-1]][keep]
+    entry_row = np.repeat(np.arange(n, dtype=np.int32), length)
+    dev = tree.device
+    R = torch.tensor(new_rows, device=dev)
+    S = torch.tensor(np.ascontiguousarray(new_partners), device=dev)
+    E = torch.tensor(entry_row, device=dev)
+    coeff = np.ascontiguousarray(_m2l_coefficients(tree.order, tree.symmetric))
+    moments = (tree.moment_re, tree.moment_im)
+    records = tree._source_records(moments)
+    hat = tree._scaled_moments(moments)
+    stream = _lib.stream(dev)
+
+    def run(rows_form):
+        lre = torch.zeros((n, 13), dtype=torch.float64, device=dev)
+        lim = torch.zeros_like(lre)
+        if rows_form:
+            _lib.call("td3_fmm_m2l_mixed_rows", R.data_ptr(), S.data_ptr(), n,
+                      tree.node_center.data_ptr(), tree.node_half.data_ptr(),
+                      records.data_ptr(), 12, coeff.ctypes.data, tree._unit, lre.data_ptr(),
+                      lim.data_ptr(), stream)
+        else:
+            _lib.call("td3_fmm_m2l_mixed", R.data_ptr(), E.data_ptr(), S.data_ptr(), n,
+                      tree.node_center.data_ptr(), tree.node_half.data_ptr(),
+                      tree.node_center.data_ptr(), tree.node_half.data_ptr(), hat.data_ptr(),
+                      12, coeff.ctypes.data, tree._unit, 0, lre.data_ptr(), lim.data_ptr(), 0,
+                      stream)
+        return lre.cpu().numpy(), lim.cpu().numpy()
+
+    a, b, c = run(True), run(True), run(False)
+    for part in (0, 1):
+        assert np.array_equal(a[part], b[part])
+        assert relative(a[part], c[part]) < 1e-6
+        assert not a[part][n // 4: 3 * n // 4].any()  # the emptied rows stay zero
+
